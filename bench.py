@@ -1,0 +1,478 @@
+#!/usr/bin/env python
+"""Benchmark: RK3 steps/s of the KMM channel step at Re_tau 180, 192x129x192.
+
+Headline (BASELINE metric): mixed-precision, graph-captured steps/s on one B200, with the
+plain FP64 GPU path timed beside it and the mixed path's relative L2 error against the FP64
+path after 100 steps.  Workload: Lx = 4 pi, Lz = 4 pi / 3 (LMFx = 2, LMFz = 2/3),
+192 x 129 x 192 modes (288 x 129 x 288 dealiased), order-7 B-splines on the sine map,
+nu = 1/2800, Pr = 0.71, opposition control A = -1 at y+ = 15, fixed dt = 0.01, seeded
+divergence-free random-phase initial condition (synthetic data).
+
+  python bench.py [--gpus N --steps K --warmup W]          our implementation
+  python bench.py --impl reference [...]                    the CPU restatement (oracle port)
+
+Multi-GPU: one independent channel per rank (replicas; the step has no data-path
+collective), weak scaling; value = all ranks' steps / max-over-ranks time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "RK3 steps/s at Re_tau180 192x129x192: mixed vs FP64 GPU at <=1e-5 rel L2 err"
+RE_TAU = 180.0
+SEED = 20261203
+
+
+def workload(nx=192, ny=129, nz=192):
+    return dict(nx=nx, ny=ny, nz=nz, lmfx=2.0, lmfz=2.0 / 3.0, stretch=0.9, nu=1.0 / 2800.0,
+                pr=0.71, fixed_dt=1, control_amp=-1.0, control_yd=-1.0 + 15.0 / RE_TAU)
+
+
+def workload_name(w):
+    return (f"KMM RK3 step {w['nx']}x{w['ny']}x{w['nz']} Re_tau180 (LMFx 2, LMFz 2/3), Pr 0.71 passive "
+            f"scalar, opposition control A=-1 at y+=15, fixed dt 0.01, seeded random-phase IC")
+
+
+# ------------------------------------------------------------------------------------------
+# algorithmic bytes per kernel launch (each kernel's own required HBM traffic)
+# ------------------------------------------------------------------------------------------
+def kernel_bytes(w, s_nl, control=True):
+    nxh = w["nx"] // 2
+    nspec = nxh * w["nz"] * w["ny"]
+    nmid = nxh * (w["nz"] * 3 // 2) * w["ny"]
+    s_st = 16
+    return {
+        "zinv": 4 * nspec * s_st + 4 * nmid * s_nl,
+        "xphys": 4 * nmid * s_nl + 8 * nmid * s_nl,
+        "zfwd": 8 * nmid * s_nl + 8 * nspec * s_nl,
+        "wavespace": 8 * nspec * s_nl + (3 + (1 if control else 0)) * nspec * s_st + 7 * nspec * s_st,
+    }
+
+
+def step_bytes(w, s_nl, control=True):
+    kb = kernel_bytes(w, s_nl, control)
+    return 3 * sum(kb.values())
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def profile_traffic():
+    """DRAM bytes per launch of the dominant kernel from the committed ncu summary, if any."""
+    p = os.path.join(ROOT, "profiles", "traffic.json")
+    try:
+        with open(p) as f:
+            return json.load(f)
+    except Exception:
+        return {}
+
+
+# ------------------------------------------------------------------------------------------
+# clocks during the timed region
+# ------------------------------------------------------------------------------------------
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_id: str):
+        self.gpu_id = gpu_id
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        fd, self.path = tempfile.mkstemp(prefix="clocks_", suffix=".csv")
+        os.close(fd)
+        try:
+            self.fh = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", self.gpu_id, f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=self.fh, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+            self.fh.close()
+
+    def summary(self):
+        rows = []
+        try:
+            with open(self.path) as f:
+                for line in f:
+                    parts = [x.strip() for x in line.split(",")]
+                    if len(parts) >= 9:
+                        rows.append(parts)
+        except Exception:
+            pass
+        finally:
+            try:
+                os.unlink(self.path)
+            except Exception:
+                pass
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        smax = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower().startswith("active")})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+# ------------------------------------------------------------------------------------------
+# distributed plumbing (replicas)
+# ------------------------------------------------------------------------------------------
+def dist_env():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", str(rank)))
+    return world, rank, local
+
+
+def init_dist(world, backend):
+    if world <= 1:
+        return None
+    import datetime
+
+    import torch.distributed as dist
+    os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+    dist.init_process_group(backend=backend, timeout=datetime.timedelta(seconds=120))
+    return dist
+
+
+def max_over_ranks(value: float, dist, device) -> float:
+    """Max of a per-rank float over all ranks (identity without a process group)."""
+    if dist is None:
+        return value
+    import torch
+    t = torch.tensor([value], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(dist, device):
+    if dist is None:
+        return
+    import torch
+    t = torch.zeros(1, device=device)
+    dist.all_reduce(t)
+
+
+# ------------------------------------------------------------------------------------------
+# CPU reference (oracle port), sampled
+# ------------------------------------------------------------------------------------------
+def oracle_sampled_substep(U, RK, ops, p, s, frac, ctrl, frac_w=None):
+    """Time one substep of the oracle port on a sample and scale it to the full substep.
+
+    The transforms (y_to_x, dft_x_realspace, x_to_y) run on the first ny/frac wall-normal
+    planes, the wavespace solves on the first nz/frac_w kz rows (all kx); both phases are
+    linear in the planes / modes they process.  Returns seconds for the full substep.
+    """
+    from oracle import kmm as okmm
+    frac_w = frac_w or frac
+    ny = p.ny
+    ysub = max(1, ny // frac)
+    Usub = np.ascontiguousarray(U[:, :, :, :ysub])
+    t0 = time.perf_counter()
+    Up = np.zeros((10, ysub, p.nz32, p.nxh), dtype=np.complex128)
+    for f in (0, 1, 2, 6):
+        Up[f] = okmm.y_to_x(Usub[f], p.nz32)
+    dyr = okmm.dyr_vector(ops.y, p.dy_factor)[:ysub]
+    okmm.dft_x_realspace(Up, p.nx, s, p.dxr, p.dzr, dyr)
+    for f in (0, 1, 2, 3, 4, 6, 7, 8, 9):
+        okmm.x_to_y(Up[f], p.nz)
+    t_tr = (time.perf_counter() - t0) * (ny / ysub)
+    nsub = max(1, p.nz // frac_w)
+    Us = np.ascontiguousarray(U[:, :nsub]) * p.rescale
+    RKs = np.ascontiguousarray(RK[:, :nsub])
+    t0 = time.perf_counter()
+    _wavespace_block(Us, RKs, ops, p, s, 0.01, ctrl, nsub)
+    t_w = (time.perf_counter() - t0) * (p.nz / nsub)
+    return t_tr + t_w
+
+
+def _wavespace_block(U, RK, ops, p, s, dt, ctrl, nsub):
+    """The oracle's per-mode solves on the modes kz_index < nsub (all kx)."""
+    from oracle import kmm as okmm
+    kxi, kzi = okmm.wavenumbers(p.nx, p.nz)
+    kzi = kzi[:nsub]
+    KZ, KX = np.meshgrid(kzi, kxi, indexing="ij")
+    mask = ~((KX == 0) & (KZ == 0))
+    kx = KX[mask] * (1.0 / p.lmfx)
+    kz = KZ[mask] * (1.0 / p.lmfz)
+
+    def lines(slot, arr=U):
+        return np.ascontiguousarray(arr[slot][mask].T)
+
+    u1, u2, u3, u4, u5, u7, u8, u9, u10 = (lines(i) for i in (0, 1, 2, 3, 4, 6, 7, 8, 9))
+    sg, sp, st = lines(0, RK), lines(1, RK), lines(2, RK)
+    hg, hv, ht = okmm.hvhg(u1, u2, u3, u4, u5, u7, u8, u9, ops, kx, kz)
+    g, sg, Dg = okmm.solve_scalar_helmholtz(hg, sg, ops, kx, kz, (p.nu, None), s, dt)
+    vwall = None
+    if ctrl is not None:
+        w_lo, w_hi, amp, _ = ctrl
+        vwall = np.stack([amp * (w_lo @ u10), amp * (w_hi @ u10)])
+    v, dv, sp = okmm.solve_v_f(hv, sp, u10, ops, Dg, kx, kz, p.nu, s, dt, vwall)
+    okmm.solve_u_w(g, dv, kx, kz)
+    okmm.solve_scalar_helmholtz(ht, st, ops, kx, kz, (p.nu, p.pr), s, dt)
+
+
+def cpu_reference_setup(w):
+    from channel_passive_b200 import ic
+    from oracle import kmm as okmm
+    p = okmm.Params(nx=w["nx"], ny=w["ny"], nz=w["nz"], lmfx=w["lmfx"], lmfz=w["lmfz"],
+                    stretch=w["stretch"], nu=w["nu"], pr=w["pr"], fixed_dt=True,
+                    control_amp=w["control_amp"], control_yplus=15.0, re_tau=RE_TAU)
+    ops = okmm.make_operators(p)
+    U = ic.seeded_ic(p.nx, p.ny, p.nz, ops.y, p.lmfx, p.lmfz, seed=SEED)
+    RK = np.zeros((3, p.nz, p.nxh, p.ny), dtype=np.complex128)
+    RK[:] = U[[0, 1, 6]] * 0.1
+    ctrl = (*okmm.control_weights(ops, p), p.control_amp, None)
+    return p, ops, U, RK, ctrl
+
+
+def run_reference(args):
+    world, rank, local = dist_env()
+    if rank != 0:
+        return 0
+    w = workload()
+    p, ops, U, RK, ctrl = cpu_reference_setup(w)
+    frac, frac_w = args.ref_frac, args.ref_frac_w
+    for i in range(args.warmup):
+        oracle_sampled_substep(U, RK, ops, p, 1 + i % 3, frac, ctrl, frac_w)
+    times = []
+    for i in range(args.steps):
+        # one "step" = a sampled substep, scaled to the full substep; an RK3 step is 3 of them
+        times.append(3.0 * oracle_sampled_substep(U, RK, ops, p, 1 + i % 3, frac, ctrl, frac_w))
+    sec_per_step = float(np.mean(times))
+    value = 1.0 / sec_per_step
+    sample = (f"oracle port (numpy FP64, single thread): each step times one substep with the transforms "
+              f"on 1/{frac} of the y-planes and the wavespace solves on 1/{frac_w} of the kz rows, "
+              f"scaled to a full RK3 step of {w['nx']}x{w['ny']}x{w['nz']}")
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": 0,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": sec_per_step * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded random-phase IC)",
+        "config": {"workload": workload_name(w), "nx": w["nx"], "ny": w["ny"], "nz": w["nz"],
+                   "precision": "fp64", "parallelism": "cpu"},
+        "cpu_baseline": {"value": value, "unit": "steps/s", "cores": 1, "kind": "port", "sample": sample},
+        "e2e": {"value": value, "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ------------------------------------------------------------------------------------------
+# our implementation
+# ------------------------------------------------------------------------------------------
+def cpu_baseline_quick(w):
+    """Rank 0, N = 1: the oracle port timed on a bounded sample (about 10-20 s)."""
+    p, ops, U, RK, ctrl = cpu_reference_setup(w)
+    frac = 4
+    t = min(oracle_sampled_substep(U, RK, ops, p, 2, frac, ctrl, frac) for _ in range(2))
+    return {"value": 1.0 / (3.0 * t), "unit": "steps/s", "cores": 1, "kind": "port",
+            "sample": f"oracle port (numpy FP64, 1 thread), best of 2 substeps on 1/{frac} of the y-planes "
+                      f"and 1/{frac} of the kz rows, scaled to a full RK3 step of {w['nx']}x{w['ny']}x{w['nz']}"}
+
+
+def run_kmm(args):
+    import torch
+
+    from channel_passive_b200 import Channel, Config, ic
+    from channel_passive_b200 import _lib
+
+    world, rank, local = dist_env()
+    torch.cuda.set_device(local)
+    device = torch.device("cuda", local)
+    dist = init_dist(world, "nccl")
+    w = workload(args.nx, args.ny, args.nz)
+    common = dict(nx=w["nx"], ny=w["ny"], nz=w["nz"], lmfx=w["lmfx"], lmfz=w["lmfz"], stretch=w["stretch"],
+                  nu=w["nu"], pr=w["pr"], fixed_dt=1, control_amp=w["control_amp"],
+                  control_yd=w["control_yd"], device=local)
+    mixed = Channel(Config(precision=_lib.KMM_PREC_MIXED, **common))
+    fp64 = Channel(Config(precision=_lib.KMM_PREC_FP64, **common))
+    U0 = ic.seeded_ic(w["nx"], w["ny"], w["nz"], mixed.y, w["lmfx"], w["lmfz"], seed=SEED + rank)
+    dt = 0.01
+    # accuracy: 100 steps from the same IC, mixed vs FP64 (the FP64 GPU path matches the oracle
+    # to 1e-10 in the parity tests)
+    for ch in (mixed, fp64):
+        ch.set_initial_data_uvw(U0, dt)
+        ch.step(args.acc_steps)
+    Um, _ = mixed.download_state()
+    Ud, _ = fp64.download_state()
+    names = {0: "u", 1: "v", 2: "w", 6: "theta"}
+    rel = {names[s]: float(np.linalg.norm(Um[s] - Ud[s]) / np.linalg.norm(Ud[s])) for s in names}
+
+    def timed(ch, k, wmup):
+        ch.step(wmup)
+        stream = torch.cuda.ExternalStream(ch.stream_ptr, device=device)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        barrier(dist, device)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        ch.step_async(k)
+        e1.record(stream)
+        out = ch.sync()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        return max_over_ranks(ms, dist, device), out
+
+    gpu_id = local
+    try:
+        props = torch.cuda.get_device_properties(local)
+        uuid = str(getattr(props, "uuid", "") or "")
+        gpu_id = ("GPU-" + uuid) if uuid and not uuid.startswith("GPU-") else (uuid or str(local))
+    except Exception:
+        gpu_id = str(local)
+    with ClockSampler(str(gpu_id)) as clk:
+        ms_mixed, out_m = timed(mixed, args.steps, args.warmup)
+    clocks = clk.summary()
+    ms_fp64, _ = timed(fp64, args.steps, args.warmup)
+    per_rank_sps = args.steps / (ms_mixed / 1e3)
+    value = world * args.steps / (ms_mixed / 1e3)
+    fp64_value = world * args.steps / (ms_fp64 / 1e3)
+
+    # per-kernel device time (event pairs around every launch) for the roofline
+    prof = mixed.profile_step(args.prof_steps)
+    prof64 = fp64.profile_step(args.prof_steps)
+    kb = kernel_bytes(w, 8)
+    kb64 = kernel_bytes(w, 16)
+    totals = {k: prof[k]["ms"] * prof[k]["launches"] for k in kb}
+    dom = max(totals, key=totals.get)
+    peak, peak_kind = measured_peaks()
+    achieved = kb[dom] / (prof[dom]["ms"] * 1e-3) / 1e9
+    traffic = profile_traffic().get(dom)
+    kernels = {k: {"ms": prof[k]["ms"], "GB_s": kb[k] / (prof[k]["ms"] * 1e-3) / 1e9,
+                   "frac": kb[k] / (prof[k]["ms"] * 1e-3) / 1e9 / peak} for k in kb}
+    kernels64 = {k: {"ms": prof64[k]["ms"], "GB_s": kb64[k] / (prof64[k]["ms"] * 1e-3) / 1e9,
+                     "frac": kb64[k] / (prof64[k]["ms"] * 1e-3) / 1e9 / peak} for k in kb64}
+
+    # end to end: host-resident state in pinned memory, full upload + step + download per step
+    nxh = w["nx"] // 2
+    nspec = nxh * w["nz"] * w["ny"]
+    U_h = torch.zeros((7, w["nz"], nxh, w["ny"]), dtype=torch.complex128).pin_memory()
+    RK_h = torch.zeros((3, w["nz"], nxh, w["ny"]), dtype=torch.complex128).pin_memory()
+    Uc, RKc = mixed.download_state(7)
+    U_h.copy_(torch.from_numpy(Uc))
+    RK_h.copy_(torch.from_numpy(RKc))
+    stream = torch.cuda.ExternalStream(mixed.stream_ptr, device=device)
+    mixed.step_host_ptr(U_h.data_ptr(), 7, RK_h.data_ptr(), 1)
+    barrier(dist, device)
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.e2e_steps):
+        mixed.step_host_ptr(U_h.data_ptr(), 7, RK_h.data_ptr(), 1)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms_e2e = max_over_ranks(e0.elapsed_time(e1), dist, device)
+    e2e_value = world * args.e2e_steps / (ms_e2e / 1e3)
+    io_bytes = 7 * nspec * 16
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline_quick(w)
+
+    launches_per_step = 3 * 5 + 1
+    line = {
+        "metric": METRIC,
+        "value": value,
+        "unit": "steps/s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": ms_mixed / args.steps,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32+f64",
+        "data": "synthetic (seeded divergence-free random-phase IC, seed 20261203 + rank)",
+        "config": {"workload": workload_name(w), "nx": w["nx"], "ny": w["ny"], "nz": w["nz"],
+                   "precision": "mixed (FP32 transforms/products, FP64 state, solves, mean modes)",
+                   "graph": True, "parallelism": f"replicas x{world}",
+                   "l2": "no flush: the resident state and slabs (>1 GB) exceed the 126 MB L2 every step"},
+        "grid_point_steps_per_s": value * w["nx"] * w["ny"] * w["nz"],
+        "fp64": {"value": fp64_value, "ms_per_step": ms_fp64 / args.steps, "kernels": kernels64},
+        "mixed_over_fp64": value / fp64_value,
+        "rel_l2_mixed_vs_fp64": rel,
+        "rel_l2_steps": args.acc_steps,
+        "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "peak_kind": peak_kind,
+                     "traffic": traffic, "algorithmic_bytes": kb[dom],
+                     "step_algorithmic_bytes": step_bytes(w, 8),
+                     "step_frac": step_bytes(w, 8) / (ms_mixed / args.steps * 1e-3) / 1e9 / peak,
+                     "kernels": kernels},
+        "cpu_baseline": cpu,
+        "e2e": {"value": e2e_value, "unit": "steps/s", "h2d_bytes_per_step": io_bytes,
+                "d2h_bytes_per_step": io_bytes,
+                "api": "kmm_step_host: pinned host U/RK_STORE (reference layout) uploaded, one RK3 step, downloaded"},
+        "gpu_launches": launches_per_step * args.steps,
+        "clocks": clocks,
+        "last_step": {"dt": out_m["dt"], "dpdx": out_m["phi_dpdx"][3], "tau_w": out_m["wall_shear_stress"],
+                      "dTdx": out_m["phi_dtdx"][3], "q_w": out_m["wall_theta_stress"]},
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    mixed.close()
+    fp64.close()
+    if dist is not None:
+        dist.destroy_process_group()
+    return 0
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="kmm", choices=["kmm", "reference"])
+    ap.add_argument("--nx", type=int, default=192)
+    ap.add_argument("--ny", type=int, default=129)
+    ap.add_argument("--nz", type=int, default=192)
+    ap.add_argument("--acc-steps", type=int, default=100)
+    ap.add_argument("--prof-steps", type=int, default=5)
+    ap.add_argument("--e2e-steps", type=int, default=20)
+    ap.add_argument("--ref-frac", type=int, default=16)
+    ap.add_argument("--ref-frac-w", type=int, default=8)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args(argv)
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_kmm(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

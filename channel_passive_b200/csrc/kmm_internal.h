@@ -1,0 +1,130 @@
+// kmm_internal.h - handle layout, HBM layout and helpers shared by the libkmm sources.
+//
+// HBM layout (all complex, one plane per wall-normal index y, kx fastest):
+//   S   [4][ny][nz][nxh]    double2   state u, v, w, theta           (fields 1,2,3,7 of U)
+//   RK  [3][ny][nz][nxh]    double2   low-storage RK terms           (RK_STORE 1..3)
+//   P   [8][ny][nz][nxh]    R2        spectral products f1..f5, f7..f9 (fields 1-5, 7-9)
+//   MID [8][ny][nz32][nxh]  R2        x-spectral / z-physical slab = the reference X-pencil
+//                                     Up(nxh, nz32, ny) (dft_x_realspace.f90:31)
+// A (kx, kz) mode m = kz_index * nxh + kx owns the strided line S[f][.][m]: a warp of 32
+// consecutive modes reads one 32-element contiguous run per y, so the per-mode solver is
+// coalesced without any staging.  R2 is double2 (FP64 path) or float2 (mixed path).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "../../include/kmm.h"
+
+namespace kmm {
+
+constexpr int kMaxPass = 8;
+constexpr int kMinBw = 2;
+constexpr int kMaxBw = 7;
+
+// One radix-{2,3,4,5} plan of a length-n complex transform.  pos[i] is where natural index
+// i sits in the decimation-in-time input (and where frequency i sits in the
+// decimation-in-frequency output); tw[t] = exp(-2 pi i t / n).
+struct FftPlan {
+  int n = 0;
+  int npass = 0;
+  int radix[kMaxPass] = {0};
+  const int *pos = nullptr;
+  const double2 *tw64 = nullptr;
+  const float2 *tw32 = nullptr;
+};
+
+// Device-side scalars written by the kernels and read back by the host.
+struct DevScalars {
+  double dt;                    // time step in use
+  double dt_prev;               // dt before the last CFL update
+  unsigned long long velmax_bits;  // max |u|dxr+|v|dyr+|w|dzr as the bits of a non-negative double
+  double phi_dpdx[4];
+  double phi_dtdx[4];
+  double wall_shear_stress;
+  double wall_theta_stress;
+  int err;                      // KMM_ERR_* raised on the device, 0 if none
+  int nonfinite;                // set when a non-finite velocity was seen
+};
+
+// Host-side copy of the wall-normal operators.
+struct HostOps {
+  int ny = 0, k = 0, bw = 0;
+  std::vector<double> y, knots, brk, integ, center;
+  std::vector<double> full[5];   // [point * ny + basis]
+  std::vector<double> band[3];   // (2bw+1, ny) Fortran order
+  std::vector<double> d0_lu;
+  std::vector<double> wlo, whi;  // control weights: v(y_d) = w . v
+};
+
+// Builds the operators (LABS_fill_full + LABS_eval_bw + LABS_full_to_band + LABS_lu(D0)).
+int build_host_ops(int k_order, int ny, double stretch, double ly, int grid, HostOps &ops,
+                   std::string &err);
+// Control weights for the detection planes y_d and -y_d.
+int build_control_weights(HostOps &ops, double yd, std::string &err);
+void host_band_lu(std::vector<double> &a, int bw, int n);
+
+struct Handle {
+  kmm_config cfg{};
+  int nx = 0, ny = 0, nz = 0, nxh = 0, nx32 = 0, nz32 = 0, bw = 0;
+  int64_t nmodes = 0;           // nxh * nz
+  int64_t ns = 0;               // ny * nmodes            (spectral plane stack per field)
+  int64_t nm = 0;               // ny * nz32 * nxh        (mid slab per field)
+  bool mixed = false;
+  double dxr = 0, dzr = 0, cflx = 0, rescale = 0, lmfxr = 0, lmfzr = 0;
+  HostOps ops;
+  std::vector<int> radix_x, radix_z;
+
+  cudaStream_t stream = nullptr;
+  double2 *S = nullptr, *RK = nullptr;
+  void *P = nullptr, *MID = nullptr;       // R2 arrays
+  double2 *wbuf = nullptr;                 // wavespace scratch lines [2][ny][nmodes]
+  double *wband = nullptr;                 // wavespace scratch bands [2bw+1][ny][nmodes]
+  double *dops = nullptr;                  // D0, D1, D2, D0_LU bands, integ, dyr, wlo, whi
+  float *gains = nullptr;                  // control gains per mode
+  double2 *staging = nullptr;              // [7][nz][nxh][ny] reference-layout staging
+  int *fftpos = nullptr;
+  double2 *tw64 = nullptr;
+  float2 *tw32 = nullptr;
+  DevScalars *dsc = nullptr;
+  FftPlan px, pz;
+  int64_t device_bytes = 0;
+
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t gexec = nullptr;
+};
+
+// Offsets of the operator arrays inside dops (doubles).
+struct OpsOffsets {
+  int64_t d0, d1, d2, d0lu, integ, dyr, wlo, whi, total;
+};
+OpsOffsets ops_offsets(int bw, int ny);
+
+// Kernel launchers (transforms.cu / wavespace.cu).
+cudaError_t launch_zinv(Handle &h, const double2 *src_planes, void *mid, int nfield,
+                        cudaStream_t st);
+cudaError_t launch_xphys(Handle &h, void *mid, int substep, cudaStream_t st);
+cudaError_t launch_zfwd(Handle &h, const void *mid, void *dst_planes, int nfield, double scale,
+                        bool dst_fp64, cudaStream_t st);
+cudaError_t launch_update_dt(Handle &h, int substep, cudaStream_t st);
+cudaError_t launch_begin_substep(Handle &h, int substep, cudaStream_t st);
+cudaError_t launch_wavespace(Handle &h, int substep, const double *dt_override,
+                             cudaStream_t st);
+cudaError_t launch_init_stores(Handle &h, cudaStream_t st);
+cudaError_t launch_ref_to_planes(const double2 *src, double2 *dst, int nfield, int64_t nmodes,
+                                 int ny, cudaStream_t st);
+cudaError_t launch_planes_to_ref(const double2 *src, double2 *dst, int nfield, int64_t nmodes,
+                                 int ny, cudaStream_t st);
+cudaError_t launch_labs_lu(Handle &h, double *a, int nmodes, cudaStream_t st);
+cudaError_t launch_labs_bs(Handle &h, const double *a, double2 *b, int nmodes, cudaStream_t st);
+cudaError_t launch_labs_mat_mul(Handle &h, int which, const double2 *x, double2 *b, int nmodes,
+                                cudaStream_t st);
+
+void set_error(const std::string &msg);
+// Sets the dynamic shared-memory limits of every kernel instantiation the handle uses.
+void prepare_kernels(Handle &h);
+void convert_planes_d2f(const double2 *src, float2 *dst, int64_t n, cudaStream_t st);
+
+}  // namespace kmm

@@ -1,0 +1,201 @@
+/*
+ * kmm.h - C ABI of libkmm, a B200 (sm_100a) implementation of one RK3 time step of the
+ * PoongBack Kim-Moin-Moser channel solver with a passive scalar (yaojieuh/CHANNEL_PASSIVE).
+ *
+ * The ABI is plain C: pointers, sizes and int status codes, no C++ or torch types.  It is
+ * what the reference's Fortran driver (main.f90) would bind through ISO_C_BINDING in place of
+ * its own routines; every entry point names the reference routine it replaces.
+ *
+ * Array conventions (shared with the reference):
+ *   complex arrays are interleaved (re, im) doubles, Fortran column-major:
+ *     state   U(ny, nxh, nz, nf)        -> element (y, kx, kz, f) at 2*(y + ny*(kx + nxh*(kz + nz*f)))
+ *     stores  RK_STORE(ny, nxh, nz, 3)
+ *     X-pencil Up(nxh, nz32, ny)        (dft_x_realspace.f90:31)
+ *   band matrices are real (2*bw+1, ny) in the reference's near-boundary packed form
+ *   (module_labs.f90:301-328).
+ * Wavenumber order: kx = 0..nx/2-1; kz = 0..nz/2, -nz/2+1..-1 (module_ppdfftw.f90:347-384).
+ *
+ * Status codes: 0 = success; nonzero = failure with a message from kmm_last_error().  The
+ * reference aborts through mpi_abort on the same conditions (read_input_file.f90:335-343,
+ * dft_x_realspace.f90:494-497); a Fortran shim converts a nonzero status into mpi_abort.
+ */
+#ifndef KMM_H
+#define KMM_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define KMM_OK 0
+#define KMM_ERR_CONFIG 1      /* invalid configuration (read_input_file.f90:251-333 checks) */
+#define KMM_ERR_CUDA 2        /* CUDA runtime error or no device */
+#define KMM_ERR_DT 3          /* dt <= 1e-14 or dt > 1e5 (dft_x_realspace.f90:494-497) */
+#define KMM_ERR_NONFINITE 4   /* NaN / Inf in the velocity maximum or in uploaded state */
+#define KMM_ERR_ARG 5         /* null pointer, bad substep, size mismatch */
+#define KMM_ERR_TIMEOUT 6     /* a bounded device wait gave up */
+
+#define KMM_PREC_FP64 0       /* every kernel in FP64 */
+#define KMM_PREC_MIXED 1      /* FP32 transforms/products, FP64 state, v-influence and mean modes */
+
+#define KMM_GRID_SINE 0       /* the reference's breakpoint map (labs_fill_full.cpp:92) */
+#define KMM_GRID_TANH 1       /* the commented tanh map (labs_fill_full.cpp:89) */
+
+/* Mirrors the positional `input` file read by read_input_file.f90:144-193, plus the
+ * switches this implementation adds (fixed dt, precision, opposition control). */
+typedef struct kmm_config {
+  int32_t nx, ny, nz;         /* modes in x, collocation points in y, modes in z */
+  int32_t no_of_field;        /* must be 10 (fields 1..10 are used, wavespace.f90:29) */
+  int32_t rk_scheme;          /* must be 3 (read_input_file.f90:295-300) */
+  int32_t labs_k;             /* B-spline order minus one (GSL order = labs_k+1) */
+  double lmfx, lmfy, lmfz;    /* Lx = 2 pi lmfx, Ly = 2 lmfy, Lz = 2 pi lmfz */
+  double stretch;             /* breakpoint stretching factor */
+  int32_t grid;               /* KMM_GRID_SINE or KMM_GRID_TANH */
+  double nu, pr;              /* viscosity, Prandtl number */
+  double bulk_vel_u, bulk_vel_w, bulk_t; /* target bulk U, W and theta */
+  double u_gal;               /* Galilean shift of the mean flow */
+  double cfl, dt_factor, dy_factor;      /* CFL number, dt relaxation, dy safety factor */
+  int32_t fixed_dt;           /* 0: dt from the CFL rule each step (reference); 1: dt held */
+  int32_t precision;          /* KMM_PREC_FP64 or KMM_PREC_MIXED */
+  double control_amp;         /* opposition control amplitude A; 0 = no control (reference) */
+  double control_yd;          /* detection plane y_d (-1 < y_d < 0); mirrored at the top wall */
+  int32_t device;             /* CUDA device ordinal */
+  int32_t reserved[7];
+} kmm_config;
+
+/* Per-step diagnostics printed by main.f90:278-280. */
+typedef struct kmm_scalars {
+  double dt;                  /* time step used by the last substep */
+  double velmax;              /* max(|u| dxr + |v| dyr + |w| dzr) of the last substep 1 */
+  double phi_dpdx[4];         /* mean forcing per substep; [3] = sum/dt after a full step */
+  double phi_dtdx[4];         /* scalar forcing per substep; [3] = sum/dt after a full step */
+  double wall_shear_stress;   /* 0.5 nu (dU/dy|bottom - dU/dy|top), substep 3 */
+  double wall_theta_stress;   /* 0.5 nu/pr (dT/dy|bottom - dT/dy|top), substep 3 */
+} kmm_scalars;
+
+typedef struct kmm_info {
+  int32_t bw;                 /* LABS band half-width detected by LABS_eval_bw */
+  int32_t nxh, nx32, nz32;
+  int64_t nmodes;             /* nxh * nz */
+  int64_t device_bytes;       /* HBM held by the handle */
+  int32_t fft_radix_x[8];     /* radix passes of the x transform (0-terminated) */
+  int32_t fft_radix_z[8];
+} kmm_info;
+
+typedef struct kmm_handle kmm_handle;
+
+/* Thread-local text of the last failure. */
+const char *kmm_last_error(void);
+
+/* Fills the reference defaults (single rank, Re_tau 180 style channel). */
+int kmm_config_default(kmm_config *cfg);
+
+/* Parses the positional `input` text file (read_input_file.f90:119-193) into cfg. */
+int kmm_read_input_file(const char *path, kmm_config *cfg);
+
+/* LABS_initialize + RK3_initialize + ppdfftw_initialize (module_labs.f90:77-238,
+ * module_runge_kutta.f90:28-54, module_ppdfftw.f90:499-588): builds the B-spline
+ * operators, allocates the HBM-resident state and plans the transforms. */
+int kmm_create(const kmm_config *cfg, kmm_handle **out);
+int kmm_destroy(kmm_handle *h);
+int kmm_get_info(const kmm_handle *h, kmm_info *info);
+
+/* Host copies of the operators: y(ny), integration weights(ny), bands (2bw+1, ny) each. */
+int kmm_get_operators(const kmm_handle *h, double *y, double *integ, double *d0, double *d1,
+                      double *d2, double *d0_lu);
+
+/* Drop-in for the GSL builder LABS_fill_full (labs_fill_full.cpp:35-195; Fortran interface
+ * module_labs.f90:46-65).  Same arguments, all by reference; K is the GSL order. */
+void kmm_labs_fill_full(double *M0, double *M1, double *M2, double *M3, double *M4, double *yc,
+                        double *yknot, double *int_coeff, double *center_coeff, int *K, int *N,
+                        double *STRETCH, double *Ly);
+
+/* State exchange in the reference layout (module_ppdfftw.f90:298-335 allocations).
+ * U holds nf >= 7 fields; fields 1,2,3,7 (u, v, w, theta) are used.  rk holds the 3 stores.
+ * Host pointers; pinned memory makes the copies asynchronous-capable. */
+int kmm_upload_state(kmm_handle *h, const double *U, int nf, const double *rk, double dt);
+int kmm_download_state(kmm_handle *h, double *U, int nf, double *rk);
+
+/* set_initial_data_uvw (initial_step.f90:139-179): uploads u, v, w, theta and builds the
+ * RK stores on the device. */
+int kmm_set_initial_data_uvw(kmm_handle *h, const double *U, int nf, double dt);
+
+/* time_march (time_march.f90:36-128): one RK3 substep (1..3) on the resident state.
+ * out may be NULL. */
+int kmm_time_march(kmm_handle *h, int rk_substep, kmm_scalars *out);
+
+/* nsteps full RK3 steps (the main.f90:262-321 loop body without I/O), replayed from a
+ * CUDA graph; out receives the diagnostics of the last step. */
+int kmm_step(kmm_handle *h, int nsteps, kmm_scalars *out);
+
+/* Same as kmm_step but only enqueues the work on the handle's stream (no host sync,
+ * no error check); kmm_sync then waits and reports. */
+int kmm_step_async(kmm_handle *h, int nsteps);
+int kmm_sync(kmm_handle *h, kmm_scalars *out);
+
+/* End-to-end drop-in with host-resident state: upload U/RK from host memory, run nsteps
+ * RK3 steps, download U/RK back.  This is time_march with the reference's ownership of
+ * U and RK_STORE (the caller keeps them in host memory). */
+int kmm_step_host(kmm_handle *h, double *U, int nf, double *rk, int nsteps, kmm_scalars *out);
+
+/* The cudaStream_t (as void*) every launch of the handle goes to, for event timing. */
+int kmm_get_stream(const kmm_handle *h, void **stream);
+
+/* Kernel ids reported by kmm_profile_step. */
+#define KMM_NKERNEL 6
+#define KMM_K_BEGIN 0       /* per-substep scalar reset */
+#define KMM_K_ZINV 1        /* y_to_x: z inverse transform of u, v, w, theta */
+#define KMM_K_XPHYS 2       /* dft_x_realspace: x transforms + products + CFL */
+#define KMM_K_DT 3          /* CFL dt update (substep 1) */
+#define KMM_K_ZFWD 4        /* x_to_y: z forward transform of the 8 products (+ rescale) */
+#define KMM_K_WAVESPACE 5   /* wavespace: per-mode solves and the mean modes */
+
+/* Runs nsteps RK3 steps launching kernel by kernel with a CUDA event pair around every
+ * launch on the handle's stream; ms[k] = mean device time per launch of kernel k,
+ * launches[k] = number of launches.  Same numerics as kmm_step. */
+int kmm_profile_step(kmm_handle *h, int nsteps, double *ms, int *launches);
+
+int kmm_get_dt(const kmm_handle *h, double *dt);
+int kmm_set_dt(kmm_handle *h, double dt);
+
+/* Opposition-control gains per mode, (nxh, nz) Fortran order, float; NULL resets to 1. */
+int kmm_set_control_gains(kmm_handle *h, const float *gains);
+
+/* ---- Device-level building blocks (caller device pointers, reference layouts, cudaStream_t
+ * passed as void*).  Complex buffers are interleaved doubles. ---- */
+
+/* y_to_x (y_to_x.f90:21-50) for one field: Y-pencil (ny,nxh,nz) -> X-pencil (nxh,nz32,ny).
+ * xp is double or float complex according to the handle's precision. */
+int kmm_dev_y_to_x(kmm_handle *h, const double *u_ypencil, void *xp, void *stream);
+
+/* x_to_y (x_to_y.f90:21-46) for one field, including rescale_data's 1/(nx32*nz32)
+ * (rescale_data.f90:31-33) when rescale != 0. */
+int kmm_dev_x_to_y(kmm_handle *h, const void *xp, double *u_ypencil, int rescale, void *stream);
+
+/* dft_x_realspace (dft_x_realspace.f90:68-213) on an X-pencil with 10 field slots
+ * (slot stride nxh*nz32*ny complex); reads slots 1,2,3,7 and writes 1-5, 7-9 (slot 10,
+ * the copy of v, is not produced: the v state is used directly).  velmax (substep 1)
+ * is written to *velmax_dev (device double) when not NULL. */
+int kmm_dev_dft_x_realspace(kmm_handle *h, void *xp, int rk_substep, double *velmax_dev,
+                            void *stream);
+
+/* wavespace (wavespace.f90:22-113) on U (ny,nxh,nz,10) and RK_STORE (ny,nxh,nz,3) in the
+ * reference layout, with dt given; slot 10 holds v for the control.  Products in slots
+ * 1-5, 7-9 on entry; u, v, w, theta in slots 1,2,3,7 on exit. */
+int kmm_dev_wavespace(kmm_handle *h, double *U, double *rk, int rk_substep, double dt,
+                      kmm_scalars *out, void *stream);
+
+/* Batched LABS kernels (module_labs.f90) on mode-fastest device arrays, for testing:
+ * a_modes (2bw+1, ny, nmodes) [band element fastest over modes: index ((j*(2bw+1))+r)*nm+m],
+ * b (ny, nmodes) complex. */
+int kmm_dev_labs_lu(kmm_handle *h, double *a_modes, int nmodes, void *stream);
+int kmm_dev_labs_bs(kmm_handle *h, const double *a_modes, double *b, int nmodes, void *stream);
+int kmm_dev_labs_mat_mul(kmm_handle *h, int which, const double *x, double *b, int nmodes,
+                         void *stream); /* which: 0 = D0, 1 = D1, 2 = D2 */
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* KMM_H */
