@@ -456,6 +456,7 @@ int kmm_create(const kmm_config *cfg, kmm_handle **out) {
   if ((rc = dalloc(*h, &h->wband, (size_t)(2 * h->bw + 1) * h->ns))) return fail(rc);
   if ((rc = dalloc(*h, &h->dops, (size_t)off.total))) return fail(rc);
   if ((rc = dalloc(*h, &h->gains, (size_t)h->nmodes))) return fail(rc);
+  if ((rc = dalloc(*h, &h->vwall, 2 * (size_t)h->nmodes))) return fail(rc);
   if ((rc = dalloc(*h, &h->staging, 10 * h->ns))) return fail(rc);
   if ((rc = dalloc(*h, &h->dsc, 1))) return fail(rc);
   if (cudaMemset(h->S, 0, sizeof(double2) * 4 * h->ns) != cudaSuccess ||
@@ -488,7 +489,7 @@ int kmm_destroy(kmm_handle *hh) {
   if (h->gexec) cudaGraphExecDestroy(h->gexec);
   if (h->graph) cudaGraphDestroy(h->graph);
   if (h->stream) cudaStreamSynchronize(h->stream);
-  void *ptrs[] = {h->S, h->RK, h->P, h->MID, h->wbuf, h->wband, h->dops, h->gains, h->staging,
+  void *ptrs[] = {h->S, h->RK, h->P, h->MID, h->wbuf, h->wband, h->dops, h->gains, h->vwall, h->staging,
                   h->fftpos, h->tw64, h->tw32, h->dsc};
   for (void *p : ptrs)
     if (p) cudaFree(p);

@@ -84,6 +84,7 @@ struct Handle {
   double *wband = nullptr;                 // wavespace scratch bands [2bw+1][ny][nmodes]
   double *dops = nullptr;                  // D0, D1, D2, D0_LU bands, integ, dyr, wlo, whi
   float *gains = nullptr;                  // control gains per mode
+  double2 *vwall = nullptr;                // [2][nmodes] control wall velocities
   double2 *staging = nullptr;              // [7][nz][nxh][ny] reference-layout staging
   int *fftpos = nullptr;
   double2 *tw64 = nullptr;

@@ -36,6 +36,7 @@ struct WsArgs {
   double *wband;
   const double *d0, *d1, *d2, *d0lu, *integ, *wlo, *whi;
   const float *gains;
+  double2 *vwall;  // [2][nmodes] control wall velocities (bottom, top)
   double control_amp;
   double nu, pr, lmfxr, lmfzr, bulk_u, bulk_w, bulk_t, u_gal;
   DevScalars *dsc;
@@ -269,18 +270,11 @@ __device__ void mode_step(const WsArgs &a, const Ops<BW> &o, int64_t m) {
   DLine b1 = dline(a.wbuf, 0 * a.ns, m, a.nmodes), b2 = dline(a.wbuf, 1 * a.ns, m, a.nmodes);
   DLine b3 = dline(a.wbuf, 2 * a.ns, m, a.nmodes), hvd = dline(a.wbuf, 3 * a.ns, m, a.nmodes);
   BandM<BW> Dbuf{a.wband + m, a.nmodes};
-  // opposition control: v at the detection planes from the v of this substep's start
+  // opposition-control wall values from k_control_probe (zero without control)
   double2 vlo = z2(0.0, 0.0), vhi = z2(0.0, 0.0);
   if (a.control_amp != 0.0) {
-    double2 sl = z2(0.0, 0.0), sh = z2(0.0, 0.0);
-    for (int i = 1; i <= ny; ++i) {
-      const double2 vi = Sv.ld(i);
-      sl = zadd(sl, zscale(__ldg(a.wlo + i - 1), vi));
-      sh = zadd(sh, zscale(__ldg(a.whi + i - 1), vi));
-    }
-    const double gmul = a.control_amp * (a.gains ? (double)__ldg(a.gains + m) : 1.0);
-    vlo = zscale(gmul, sl);
-    vhi = zscale(gmul, sh);
+    vlo = a.vwall[m];
+    vhi = a.vwall[a.nmodes + m];
   }
   Line<PT> u1 = pline<PT>(a, 0, m), u2 = pline<PT>(a, 1, m), u3 = pline<PT>(a, 2, m),
            u4 = pline<PT>(a, 3, m), u5 = pline<PT>(a, 4, m), u7 = pline<PT>(a, 5, m),
@@ -395,6 +389,44 @@ __device__ void wave00(const WsArgs &a, const Ops<BW> &o) {
   }
 }
 
+// Opposition control, the build's extension at the wall rows of the v Poisson solve
+// (solve_v_f.f90:251-257, where the reference's commented lines read vold).  The reference's
+// vold is field 10, v after the physical round trip (dft_x_realspace.f90:123): x_to_y zeroes
+// the kz Nyquist row and the c2r keeps only the Hermitian part of the kx = 0 plane, so the
+// same projection is applied to the v of the substep's start.  v(y_d) = w . v with the
+// precomputed weights w = D0^{-T} B(y_d); the wall value is A * gain(kx, kz) * v(y_d).
+// Runs before k_wavespace, which overwrites v.
+__global__ void k_control_probe(WsArgs a) {
+  const int64_t m = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (m >= a.nmodes) return;
+  const int kzi = (int)(m / a.nxh), kxi = (int)(m - (int64_t)kzi * a.nxh);
+  double2 sl = z2(0.0, 0.0), sh = z2(0.0, 0.0);
+  if (kzi != a.nz / 2 && m != 0) {
+    auto probe = [&](int64_t mm, double2 &pl, double2 &ph) {
+      DLine line = dline(a.S, 1 * a.ns, mm, a.nmodes);
+      pl = z2(0.0, 0.0);
+      ph = z2(0.0, 0.0);
+      for (int i = 1; i <= a.ny; ++i) {
+        const double2 vi = line.ld(i);
+        pl = zadd(pl, zscale(__ldg(a.wlo + i - 1), vi));
+        ph = zadd(ph, zscale(__ldg(a.whi + i - 1), vi));
+      }
+    };
+    probe(m, sl, sh);
+    if (kxi == 0) {  // (v(kz) + conj v(-kz)) / 2
+      double2 pl, ph;
+      probe((int64_t)((a.nz - kzi) % a.nz) * a.nxh, pl, ph);
+      sl = z2(0.5 * (sl.x + pl.x), 0.5 * (sl.y - pl.y));
+      sh = z2(0.5 * (sh.x + ph.x), 0.5 * (sh.y - ph.y));
+    }
+    const double gmul = a.control_amp * (a.gains ? (double)__ldg(a.gains + m) : 1.0);
+    sl = zscale(gmul, sl);
+    sh = zscale(gmul, sh);
+  }
+  a.vwall[m] = sl;
+  a.vwall[a.nmodes + m] = sh;
+}
+
 template <int BW, typename PT>
 __global__ void __launch_bounds__(128) k_wavespace(WsArgs a) {
   Ops<BW> o{BandS<BW>{a.d0}, BandS<BW>{a.d1}, BandS<BW>{a.d2}, BandS<BW>{a.d0lu}};
@@ -482,6 +514,7 @@ WsArgs make_args(Handle &h, int substep, const double *dt_ptr) {
   a.wlo = h.dops + off.wlo;
   a.whi = h.dops + off.whi;
   a.gains = h.gains;
+  a.vwall = h.vwall;
   a.control_amp = h.cfg.control_amp;
   a.nu = h.cfg.nu;
   a.pr = h.cfg.pr;
@@ -501,6 +534,8 @@ cudaError_t wavespace_bw(Handle &h, int substep, const double *dt_ptr, cudaStrea
   WsArgs a = make_args(h, substep, dt_ptr);
   const int threads = 128;
   const unsigned blocks = (unsigned)((h.nmodes + threads - 1) / threads) + 1;  // +1: wave00 block
+  if (h.cfg.control_amp != 0.0)
+    k_control_probe<<<(unsigned)((h.nmodes + threads - 1) / threads), threads, 0, st>>>(a);
   if (h.mixed) k_wavespace<BW, float2><<<blocks, threads, 0, st>>>(a);
   else k_wavespace<BW, double2><<<blocks, threads, 0, st>>>(a);
   return cudaGetLastError();

@@ -54,7 +54,7 @@ def test_state_roundtrip_bitexact():
         assert ch.dt == 0.01
 
 
-@pytest.mark.parametrize("nx,nz,ny", [(16, 16, 33), (8, 24, 17), (64, 64, 65), (20, 40, 21)])
+@pytest.mark.parametrize("nx,nz,ny", [(16, 16, 33), (8, 24, 21), (64, 64, 65), (20, 40, 21)])
 def test_y_to_x_matches_oracle(nx, nz, ny):
     cfg, p, ops = _setup(nx=nx, ny=ny, nz=nz)
     rng = np.random.default_rng(nx + nz)
@@ -68,7 +68,7 @@ def test_y_to_x_matches_oracle(nx, nz, ny):
     assert rel_l2(got, ref) < 1e-14
 
 
-@pytest.mark.parametrize("nx,nz,ny", [(16, 16, 33), (8, 24, 17), (64, 64, 65)])
+@pytest.mark.parametrize("nx,nz,ny", [(16, 16, 33), (8, 24, 21), (64, 64, 65)])
 def test_x_to_y_matches_oracle_and_masks(nx, nz, ny):
     cfg, p, ops = _setup(nx=nx, ny=ny, nz=nz)
     rng = np.random.default_rng(7)
@@ -152,6 +152,12 @@ def _wavespace_inputs(cfg, rng):
     RK = rng.standard_normal((3, cfg.nz, cfg.nxh, cfg.ny)) + 1j * rng.standard_normal((3, cfg.nz, cfg.nxh, cfg.ny))
     U *= 0.1
     RK *= 0.1
+    # slot 10 is v after the physical round trip: no kz Nyquist row, Hermitian kx = 0 plane
+    nz = cfg.nz
+    U[9, nz // 2] = 0.0
+    for j in range(1, nz // 2):
+        U[9, nz - j, 0] = np.conj(U[9, j, 0])
+    U[9, 0, 0] = U[9, 0, 0].real
     return U, RK
 
 
