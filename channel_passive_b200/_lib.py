@@ -22,6 +22,7 @@ KMM_ERR_TIMEOUT = 6
 
 KMM_PREC_FP64 = 0
 KMM_PREC_MIXED = 1
+KMM_NOALLOC_MAX_DOUBLES = 2097152
 KMM_NKERNEL = 6
 KERNEL_NAMES = ("begin_substep", "zinv", "xphys", "update_dt", "zfwd", "wavespace")
 KMM_GRID_SINE = 0
@@ -97,6 +98,7 @@ SIGNATURES = {
     "kmm_dev_labs_lu": (C.c_int, [_P, _P, C.c_int, _P]),
     "kmm_dev_labs_bs": (C.c_int, [_P, _P, _P, C.c_int, _P]),
     "kmm_dev_labs_mat_mul": (C.c_int, [_P, C.c_int, _P, _P, C.c_int, _P]),
+    "kmm_helmholtz_solve_noalloc": (C.c_int, [C.c_int, C.c_int, C.c_int, _P, _P, _P, _P, _P, _P]),
 }
 
 _lib = None

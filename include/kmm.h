@@ -195,6 +195,25 @@ int kmm_dev_labs_bs(kmm_handle *h, const double *a_modes, double *b, int nmodes,
 int kmm_dev_labs_mat_mul(kmm_handle *h, int which, const double *x, double *b, int nmodes,
                          void *stream); /* which: 0 = D0, 1 = D1, 2 = D2 */
 
+/* Allocation-free batched Helmholtz solve.  No counterpart in the reference: it exists for
+ * callers that may not allocate device memory (code running while a stream is captured into a
+ * CUDA graph, hosts whose device memory is reserved up front by another allocator, loops that
+ * cannot afford cudaMalloc's device-wide synchronisation).  It needs no handle.
+ * For every mode m it builds A_m = a[m] D0 - b[m] D2 with Dirichlet first and last rows (the
+ * left-hand side of solve_g / solve_t), factors it and solves A_m x = rhs_m in place.
+ *   d0_band, d2_band  device, real (2*bw+1, ny) packed bands (module_labs.f90:301-328)
+ *   a, b              device, nmodes doubles
+ *   rhs               device, complex (ny, nmodes), mode fastest; overwritten by x
+ * The per-mode scratch band is a fixed array inside the library of KMM_NOALLOC_MAX_DOUBLES
+ * doubles (16 MiB), held by every GPU that loads the library until exit; calls with
+ * (2*bw+1)*ny*nmodes above it are rejected with KMM_ERR_ARG.  The first call on each device
+ * looks the array up (cudaGetSymbolAddress); make that call before any stream capture.  All
+ * calls share the array: calls that overlap on the GPU race. */
+#define KMM_NOALLOC_MAX_DOUBLES 2097152
+int kmm_helmholtz_solve_noalloc(int ny, int bw, int nmodes, const double *d0_band,
+                                const double *d2_band, const double *a, const double *b,
+                                double *rhs, void *stream);
+
 #ifdef __cplusplus
 }
 #endif
