@@ -34,7 +34,8 @@ OpsOffsets ops_offsets(int bw, int ny) {
   o.dyr = o.integ + ny;
   o.wlo = o.dyr + ny;
   o.whi = o.wlo + ny;
-  o.total = o.whi + ny;
+  o.t0 = o.whi + ny;
+  o.total = o.t0 + (int64_t)ny * (3 * (4 * bw + 1) + (2 * bw + 1) + 2 * bw);
   return o;
 }
 
@@ -129,6 +130,16 @@ int upload_ops(Handle &h) {
     std::memcpy(buf.data() + off.wlo, h.ops.wlo.data(), h.ny * sizeof(double));
     std::memcpy(buf.data() + off.whi, h.ops.whi.data(), h.ny * sizeof(double));
   }
+  {
+    double *t = buf.data() + off.t0;
+    for (int d = 0; d < 3; ++d) {
+      std::memcpy(t, h.ops.off[d].data(), h.ops.off[d].size() * sizeof(double));
+      t += h.ops.off[d].size();
+    }
+    std::memcpy(t, h.ops.l0.data(), h.ops.l0.size() * sizeof(double));
+    t += h.ops.l0.size();
+    std::memcpy(t, h.ops.u0.data(), h.ops.u0.size() * sizeof(double));
+  }
   KMM_CUDA(cudaMemcpy(h.dops, buf.data(), buf.size() * sizeof(double), cudaMemcpyHostToDevice));
   return KMM_OK;
 }
@@ -197,7 +208,7 @@ int enqueue_substep(Handle &h, int s, cudaStream_t st, cudaEvent_t *ev = nullptr
   if (s == 1)
     if ((rc = rec(KMM_K_DT, [&] { return launch_update_dt(h, s, st); }))) return rc;
   if ((rc = rec(KMM_K_ZFWD, [&] { return launch_zfwd(h, h.MID, h.P, 8, h.rescale, !h.mixed, st); }))) return rc;
-  if ((rc = rec(KMM_K_WAVESPACE, [&] { return launch_wavespace(h, s, nullptr, st); }))) return rc;
+  if ((rc = rec(KMM_K_WAVESPACE, [&] { return launch_wavespace2(h, s, nullptr, st); }))) return rc;
   return KMM_OK;
 }
 
@@ -457,6 +468,11 @@ int kmm_create(const kmm_config *cfg, kmm_handle **out) {
   if ((rc = dalloc(*h, &h->dops, (size_t)off.total))) return fail(rc);
   if ((rc = dalloc(*h, &h->gains, (size_t)h->nmodes))) return fail(rc);
   if ((rc = dalloc(*h, &h->vwall, 2 * (size_t)h->nmodes))) return fail(rc);
+  if ((rc = dalloc(*h, &h->zc, 4 * (size_t)h->ns))) return fail(rc);
+  if ((rc = dalloc(*h, &h->ec, 3 * (size_t)h->ns))) return fail(rc);
+  if ((rc = dalloc(*h, &h->xr, 6 * (size_t)h->ns))) return fail(rc);
+  if ((rc = dalloc(*h, &h->ub, (size_t)(2 * h->bw) * h->ns))) return fail(rc);
+  if ((rc = dalloc(*h, &h->w00, 3 * (size_t)h->ny * (8 + 2 * h->bw)))) return fail(rc);
   if ((rc = dalloc(*h, &h->staging, 10 * h->ns))) return fail(rc);
   if ((rc = dalloc(*h, &h->dsc, 1))) return fail(rc);
   if (cudaMemset(h->S, 0, sizeof(double2) * 4 * h->ns) != cudaSuccess ||
@@ -475,6 +491,7 @@ int kmm_create(const kmm_config *cfg, kmm_handle **out) {
   if ((rc = upload_ops(*h))) return fail(rc);
   if ((rc = make_plans(*h))) return fail(rc);
   prepare_kernels(*h);
+  prepare_wavespace2();
   if (cudaGetLastError() != cudaSuccess) {
     set_error("kernel attribute set-up failed");
     return fail(KMM_ERR_CUDA);
@@ -489,7 +506,8 @@ int kmm_destroy(kmm_handle *hh) {
   if (h->gexec) cudaGraphExecDestroy(h->gexec);
   if (h->graph) cudaGraphDestroy(h->graph);
   if (h->stream) cudaStreamSynchronize(h->stream);
-  void *ptrs[] = {h->S, h->RK, h->P, h->MID, h->wbuf, h->wband, h->dops, h->gains, h->vwall, h->staging,
+  void *ptrs[] = {h->S, h->RK, h->P, h->MID, h->wbuf, h->wband, h->dops, h->gains, h->vwall, h->zc,
+                  h->ec, h->xr, h->ub, h->w00, h->staging,
                   h->fftpos, h->tw64, h->tw32, h->dsc};
   for (void *p : ptrs)
     if (p) cudaFree(p);
@@ -736,7 +754,7 @@ int kmm_dev_wavespace(kmm_handle *hh, double *U, double *rk, int s, double dt, k
   KMM_CUDA(cudaStreamSynchronize(st));
   int rc = set_dt_device(h, dt);
   if (rc) return rc;
-  KMM_CUDA(launch_wavespace(h, s, nullptr, st));
+  KMM_CUDA(launch_wavespace2(h, s, nullptr, st));
   const int sslots[4] = {0, 1, 2, 6};
   for (int i = 0; i < 4; ++i)
     KMM_CUDA(launch_planes_to_ref(h.S + i * h.ns, reinterpret_cast<double2 *>(U) + sslots[i] * h.ns, 1, h.nmodes, h.ny, st));

@@ -330,6 +330,47 @@ void host_band_lu(std::vector<double> &a, int bw, int n) {
   }
 }
 
+// Offset-row tables for the per-mode solver: T_d[(r-1)*(4bw+1) + e + 2bw] = D_d(r, r+e) for
+// e in [-2bw, 2bw] (zero outside the matrix), and the profile Crout LU of D0 without pivoting:
+// L0[(r-1)*(2bw+1) + e] = L(r, r-e) for e = 1..2bw with 1/L(r, r) at e = 0, and
+// U0[(r-1)*2bw + e-1] = U(r, r+e) (unit diagonal).  Row r of a collocation matrix spans columns
+// lo(r)..hi(r) with lo = max(1, r-bw) (n-2bw for the last bw rows) and hi = min(r+bw, n)
+// (2bw+1 for the first bw rows), the structure LABS_full_to_band packs (module_labs.f90:301-328);
+// an LU without pivoting keeps L and U inside it.
+static void build_offset_tables(HostOps &ops) {
+  const int n = ops.ny, bw = ops.bw, w = 4 * bw + 1;
+  for (int d = 0; d < 3; ++d) {
+    ops.off[d].assign((size_t)n * w, 0.0);
+    for (int r = 1; r <= n; ++r)
+      for (int e = -2 * bw; e <= 2 * bw; ++e) {
+        const int c = r + e;
+        if (c >= 1 && c <= n) ops.off[d][(size_t)(r - 1) * w + e + 2 * bw] = ops.full[d][(size_t)(r - 1) * n + (c - 1)];
+      }
+  }
+  ops.l0.assign((size_t)n * (2 * bw + 1), 0.0);
+  ops.u0.assign((size_t)n * 2 * bw, 0.0);
+  std::vector<double> L(2 * bw + 1);
+  auto U = [&](int p, int e) { return (e >= 1 && e <= 2 * bw) ? ops.u0[(size_t)(p - 1) * 2 * bw + e - 1] : 0.0; };
+  auto A = [&](int r, int c) { return ops.full[0][(size_t)(r - 1) * n + (c - 1)]; };
+  for (int r = 1; r <= n; ++r) {
+    const int lo = (r <= n - bw) ? std::max(1, r - bw) : n - 2 * bw;
+    const int hi = (r <= bw) ? 2 * bw + 1 : std::min(r + bw, n);
+    for (int c = lo; c <= r; ++c) {
+      double acc = A(r, c);
+      for (int p = lo; p < c; ++p) acc -= L[r - p] * U(p, c - p);
+      L[r - c] = acc;
+    }
+    const double rp = 1.0 / L[0];
+    ops.l0[(size_t)(r - 1) * (2 * bw + 1)] = rp;
+    for (int e = 1; e <= 2 * bw; ++e) ops.l0[(size_t)(r - 1) * (2 * bw + 1) + e] = (r - e >= lo) ? L[e] : 0.0;
+    for (int c = r + 1; c <= hi; ++c) {
+      double acc = A(r, c);
+      for (int p = lo; p < r; ++p) acc -= L[r - p] * U(p, c - p);
+      ops.u0[(size_t)(r - 1) * 2 * bw + (c - r) - 1] = acc * rp;
+    }
+  }
+}
+
 int build_host_ops(int k_order, int ny, double stretch, double ly, int grid, HostOps &ops,
                    std::string &err) {
   if (k_order < 2 || ny <= 2 * (k_order - 1)) {
@@ -353,6 +394,7 @@ int build_host_ops(int k_order, int ny, double stretch, double ly, int grid, Hos
   for (int d = 0; d < 3; ++d) full_to_band(ops.full[d], ops.bw, ny, ops.band[d]);
   ops.d0_lu = ops.band[0];
   host_band_lu(ops.d0_lu, ops.bw, ny);
+  build_offset_tables(ops);
   return KMM_OK;
 }
 

@@ -56,6 +56,8 @@ struct HostOps {
   std::vector<double> full[5];   // [point * ny + basis]
   std::vector<double> band[3];   // (2bw+1, ny) Fortran order
   std::vector<double> d0_lu;
+  std::vector<double> off[3];    // offset rows of D0, D1, D2: [(r-1)*(4bw+1) + e + 2bw]
+  std::vector<double> l0, u0;    // profile LU of D0 (see build_offset_tables)
   std::vector<double> wlo, whi;  // control weights: v(y_d) = w . v
 };
 
@@ -85,6 +87,11 @@ struct Handle {
   double *dops = nullptr;                  // D0, D1, D2, D0_LU bands, integ, dyr, wlo, whi
   float *gains = nullptr;                  // control gains per mode
   double2 *vwall = nullptr;                // [2][nmodes] control wall velocities
+  double2 *zc = nullptr;                   // per-mode solver: complex lines [4][ny][nmodes]
+  double2 *ec = nullptr;                   //                  complex lines [3][ny][nmodes]
+  double *xr = nullptr;                    //                  real lines    [6][ny][nmodes]
+  double *ub = nullptr;                    //                  U factor      [2bw][ny][nmodes]
+  double *w00 = nullptr;                   // mean-mode lines (3 threads)
   double2 *staging = nullptr;              // [7][nz][nxh][ny] reference-layout staging
   int *fftpos = nullptr;
   double2 *tw64 = nullptr;
@@ -99,7 +106,9 @@ struct Handle {
 
 // Offsets of the operator arrays inside dops (doubles).
 struct OpsOffsets {
-  int64_t d0, d1, d2, d0lu, integ, dyr, wlo, whi, total;
+  int64_t d0, d1, d2, d0lu, integ, dyr, wlo, whi;
+  int64_t t0;  // offset tables T0, T1, T2 [ny][4bw+1], then the D0 profile LU L0 [ny][2bw+1], U0 [ny][2bw]
+  int64_t total;
 };
 OpsOffsets ops_offsets(int bw, int ny);
 
@@ -127,5 +136,8 @@ void set_error(const std::string &msg);
 // Sets the dynamic shared-memory limits of every kernel instantiation the handle uses.
 void prepare_kernels(Handle &h);
 void convert_planes_d2f(const double2 *src, float2 *dst, int64_t n, cudaStream_t st);
+void prepare_wavespace2();
+cudaError_t launch_control_probe(Handle &h, cudaStream_t st);
+cudaError_t launch_wavespace2(Handle &h, int substep, const double *dt_override, cudaStream_t st);
 
 }  // namespace kmm

@@ -1,0 +1,255 @@
+// sweeps.cuh - register-window sweeps for one (kx, kz) system per thread.
+//
+// The wall-normal operators are held in "offset rows": T(r, e) = D(r, r+e) for e in [-2BW, 2BW]
+// (zero outside the matrix).  A collocation matrix row r spans columns lo(r)..hi(r):
+//   lo = max(1, r-BW) for r <= n-BW, n-2BW for the last BW rows,
+//   hi = min(r+BW, n) for r > BW,    2BW+1 for the first BW rows,
+// which is the near-boundary packing of LABS_full_to_band (module_labs.f90:301-328).  An LU
+// without pivoting keeps L and U inside that profile, so the Crout factorisation of
+// fixed_bandec (module_labs.f90:3487-3636: L carries the pivots, U has a unit diagonal) is
+// computed here row by row:
+//   L(r, c) = A(r, c) - sum_{p=lo..c-1} L(r, p) U(p, c),     c = lo..r
+//   U(r, c) = (A(r, c) - sum_{p=lo..r-1} L(r, p) U(p, c)) / L(r, r),   c = r+1..hi
+// and fused with the forward substitution of every right-hand side that is ready, so L is
+// never stored.  The solution windows live in registers:
+//   forward  z_r = (b_r - sum_e L(r, r-e) z_{r-e}) / L(r, r)        window z_{r-2BW..r-1}
+//   backward x_r = z_r - sum_e U(r, r+e) x_{r+e}                     window x_{r..r+2BW}
+// and a band mat-vec (M x)_q = sum_e M(q, q+e) x_{q+e} of the solution is emitted from the
+// backward window as soon as its inputs exist: row q = r+BW at step r (r <= n-2BW), the last
+// BW rows at step n-2BW and the first BW rows at step 1.  All loops over e have compile-time
+// trip counts, so the windows stay in registers.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "labs.cuh"
+
+namespace kmm {
+
+struct RLine {
+  double *p;
+  int64_t s;
+  __device__ __forceinline__ double ld(int i) const { return p[(int64_t)(i - 1) * s]; }
+  __device__ __forceinline__ void st(int i, double v) const { p[(int64_t)(i - 1) * s] = v; }
+};
+
+// Per-mode unit-upper factor: U(p, e) = U(p, p+e), e = 1..2BW, layout [e][y][mode].
+template <int BW>
+struct UBand {
+  double *p;
+  int64_t s;   // stride between rows (number of modes)
+  int64_t es;  // stride between offsets (ny * number of modes)
+  __device__ __forceinline__ double get(int r, int e) const { return p[(int64_t)(e - 1) * es + (int64_t)(r - 1) * s]; }
+  __device__ __forceinline__ void set(int r, int e, double v) const { p[(int64_t)(e - 1) * es + (int64_t)(r - 1) * s] = v; }
+};
+
+template <int BW>
+__device__ __forceinline__ int row_lo(int r, int n) { return (r <= n - BW) ? (r - BW > 1 ? r - BW : 1) : n - 2 * BW; }
+template <int BW>
+__device__ __forceinline__ int row_hi(int r, int n) { return (r <= BW) ? 2 * BW + 1 : (r + BW < n ? r + BW : n); }
+
+// Offset-row tables shared by all modes.
+template <int BW>
+struct Tabs {
+  const double *t0, *t1, *t2;  // [(r-1)*(4BW+1) + e + 2BW]
+  const double *l0;            // D0 profile LU: [(r-1)*(2BW+1) + e] = L(r, r-e), e=0 -> 1/L(r,r)
+  const double *u0;            // [(r-1)*2BW + e-1] = U(r, r+e)
+};
+
+template <int BW>
+__device__ __forceinline__ const double *trow(const double *t, int r) { return t + (r - 1) * (4 * BW + 1) + 2 * BW; }
+
+// (M x)_q from the backward window w[j] = x_{r+j}: sum_j M(q, r+j-q) w[j].
+template <int BW, typename WT>
+__device__ __forceinline__ double2 mvc(const double *t, int q, int r, const WT &w) {
+  const double *row = trow<BW>(t, q) + (r - q);
+  double2 acc = z2(0.0, 0.0);
+#pragma unroll
+  for (int j = 0; j <= 2 * BW; ++j) {
+    const double m = row[j];
+    acc.x += m * w[j].x;
+    acc.y += m * w[j].y;
+  }
+  return acc;
+}
+template <int BW, typename WT>
+__device__ __forceinline__ double mvr(const double *t, int q, int r, const WT &w) {
+  const double *row = trow<BW>(t, q) + (r - q);
+  double acc = 0.0;
+#pragma unroll
+  for (int j = 0; j <= 2 * BW; ++j) acc += row[j] * w[j];
+  return acc;
+}
+
+// Forward substitution with the fixed D0 factor for NC complex chains, ascending.
+// in(r, b[NC]) supplies the right-hand sides of row r; out(r, z[NC]) receives the results.
+template <int BW, int NC, typename In, typename Out>
+__device__ __forceinline__ void fwd_fixed(const Tabs<BW> &tb, int n, In in, Out out) {
+  constexpr int W = 2 * BW;
+  double2 w[NC][W];
+#pragma unroll
+  for (int c = 0; c < NC; ++c)
+#pragma unroll
+    for (int k = 0; k < W; ++k) w[c][k] = z2(0.0, 0.0);
+  for (int r = 1; r <= n; ++r) {
+    double2 b[NC];
+    in(r, b);
+    const double *L = tb.l0 + (r - 1) * (W + 1);
+    const double rp = L[0];
+    double2 z[NC];
+#pragma unroll
+    for (int c = 0; c < NC; ++c) {
+      double2 acc = b[c];
+#pragma unroll
+      for (int e = 1; e <= W; ++e) {
+        const double l = L[e];
+        acc.x -= l * w[c][W - e].x;
+        acc.y -= l * w[c][W - e].y;
+      }
+      z[c] = z2(acc.x * rp, acc.y * rp);
+#pragma unroll
+      for (int k = 0; k < W - 1; ++k) w[c][k] = w[c][k + 1];
+      w[c][W - 1] = z[c];
+    }
+    out(r, z);
+  }
+}
+
+// Backward substitution (unit U given by ufn(r, e)) for NC complex and NR real chains,
+// descending, with mat-vec emission: emit(q, r, wc, wr) where wc[c][j] = x_{r+j}.
+template <int BW, int NC, int NR, typename UF, typename Zin, typename Emit>
+__device__ __forceinline__ void bwd_emit(int n, UF ufn, Zin zin, Emit emit) {
+  constexpr int W = 2 * BW + 1;
+  constexpr int NCc = NC > 0 ? NC : 1, NRr = NR > 0 ? NR : 1;
+  double2 wc[NCc][W];
+  double wr[NRr][W];
+#pragma unroll
+  for (int j = 0; j < W; ++j) {
+#pragma unroll
+    for (int c = 0; c < NCc; ++c) wc[c][j] = z2(0.0, 0.0);
+#pragma unroll
+    for (int c = 0; c < NRr; ++c) wr[c][j] = 0.0;
+  }
+  for (int r = n; r >= 1; --r) {
+#pragma unroll
+    for (int j = W - 1; j >= 1; --j) {
+#pragma unroll
+      for (int c = 0; c < NCc; ++c) wc[c][j] = wc[c][j - 1];
+#pragma unroll
+      for (int c = 0; c < NRr; ++c) wr[c][j] = wr[c][j - 1];
+    }
+    double u[2 * BW];
+#pragma unroll
+    for (int e = 1; e <= 2 * BW; ++e) u[e - 1] = ufn(r, e);
+    double2 zc[NCc];
+    double zr[NRr];
+    zin(r, zc, zr);
+#pragma unroll
+    for (int c = 0; c < NC; ++c) {
+      double2 acc = zc[c];
+#pragma unroll
+      for (int e = 1; e <= 2 * BW; ++e) {
+        acc.x -= u[e - 1] * wc[c][e].x;
+        acc.y -= u[e - 1] * wc[c][e].y;
+      }
+      wc[c][0] = acc;
+    }
+#pragma unroll
+    for (int c = 0; c < NR; ++c) {
+      double acc = zr[c];
+#pragma unroll
+      for (int e = 1; e <= 2 * BW; ++e) acc -= u[e - 1] * wr[c][e];
+      wr[c][0] = acc;
+    }
+    if (r <= n - 2 * BW) emit(r + BW, r, wc, wr);
+    if (r == n - 2 * BW)
+      for (int q = n - BW + 1; q <= n; ++q) emit(q, r, wc, wr);
+    if (r == 1)
+      for (int q = 1; q <= BW; ++q) emit(q, r, wc, wr);
+  }
+}
+
+// Profile Crout LU of a per-mode matrix fused with the forward substitution of NC complex and
+// NR real chains, ascending.  rowA(r, a) fills a[e + 2BW] = A(r, r+e); in(r, bc, br) gives the
+// right-hand sides of row r; out(r, zc, zr) receives the forward results; U goes to ust.
+// Returns L(1, 1), the first pivot.
+template <int BW, int NC, int NR, typename RowA, typename In, typename Out>
+__device__ __forceinline__ double lu_fwd(int n, RowA rowA, In in, Out out, UBand<BW> ust) {
+  constexpr int W = 2 * BW;
+  constexpr int NCc = NC > 0 ? NC : 1, NRr = NR > 0 ? NR : 1;
+  double2 wc[NCc][W];
+  double wr[NRr][W];
+#pragma unroll
+  for (int k = 0; k < W; ++k) {
+#pragma unroll
+    for (int c = 0; c < NCc; ++c) wc[c][k] = z2(0.0, 0.0);
+#pragma unroll
+    for (int c = 0; c < NRr; ++c) wr[c][k] = 0.0;
+  }
+  double piv1 = 0.0;
+  for (int r = 1; r <= n; ++r) {
+    const int lo = row_lo<BW>(r, n), hi = row_hi<BW>(r, n);
+    double a[4 * BW + 1];
+    rowA(r, a);
+    double L[W + 1];  // L[d] = L(r, r-d)
+#pragma unroll
+    for (int d = W; d >= 0; --d) {
+      double acc = 0.0;
+      if (r - d >= lo) {
+        acc = a[2 * BW - d];
+#pragma unroll
+        for (int dp = W; dp > d; --dp)
+          if (r - dp >= lo) acc -= L[dp] * ust.get(r - dp, dp - d);
+      }
+      L[d] = acc;
+    }
+    if (r == 1) piv1 = L[0];
+    const double rp = 1.0 / L[0];
+#pragma unroll
+    for (int e = 1; e <= W; ++e) {
+      double v = 0.0;
+      if (r + e <= hi) {
+        double acc = a[2 * BW + e];
+#pragma unroll
+        for (int dp = W; dp >= 1; --dp)
+          if (r - dp >= lo && e + dp <= W) acc -= L[dp] * ust.get(r - dp, e + dp);
+        v = acc * rp;
+      }
+      ust.set(r, e, v);
+    }
+    double2 bc[NCc];
+    double br[NRr];
+    in(r, bc, br);
+    double2 zc[NCc];
+    double zr[NRr];
+#pragma unroll
+    for (int c = 0; c < NC; ++c) {
+      double2 acc = bc[c];
+#pragma unroll
+      for (int d = 1; d <= W; ++d) {
+        acc.x -= L[d] * wc[c][W - d].x;
+        acc.y -= L[d] * wc[c][W - d].y;
+      }
+      zc[c] = z2(acc.x * rp, acc.y * rp);
+#pragma unroll
+      for (int k = 0; k < W - 1; ++k) wc[c][k] = wc[c][k + 1];
+      wc[c][W - 1] = zc[c];
+    }
+#pragma unroll
+    for (int c = 0; c < NR; ++c) {
+      double acc = br[c];
+#pragma unroll
+      for (int d = 1; d <= W; ++d) acc -= L[d] * wr[c][W - d];
+      zr[c] = acc * rp;
+#pragma unroll
+      for (int k = 0; k < W - 1; ++k) wr[c][k] = wr[c][k + 1];
+      wr[c][W - 1] = zr[c];
+    }
+    out(r, zc, zr);
+  }
+  return piv1;
+}
+
+}  // namespace kmm

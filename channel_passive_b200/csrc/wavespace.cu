@@ -589,6 +589,13 @@ template <int BW> struct MmRun {
 
 }  // namespace
 
+cudaError_t launch_control_probe(Handle &h, cudaStream_t st) {
+  WsArgs a = make_args(h, 1, nullptr);
+  const int threads = 128;
+  k_control_probe<<<(unsigned)((h.nmodes + threads - 1) / threads), threads, 0, st>>>(a);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_wavespace(Handle &h, int substep, const double *dt_ptr, cudaStream_t st) {
   return dispatch_bw<WsRun>(h.bw, h, substep, dt_ptr, st);
 }
