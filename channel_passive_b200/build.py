@@ -44,7 +44,7 @@ def build(force: bool = False, verbose: bool = False, extra=None) -> Path:
     objdir = PKG / "_build"
     objdir.mkdir(exist_ok=True)
     cc = nvcc()
-    common = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr",
+    common = ["-O3", "-std=c++20", "-lineinfo", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr",
               "-I", str(PKG.parent / "include")] + ARCH + list(extra or [])
     objs = []
     procs = []

@@ -492,6 +492,13 @@ int kmm_create(const kmm_config *cfg, kmm_handle **out) {
   if ((rc = make_plans(*h))) return fail(rc);
   prepare_kernels(*h);
   prepare_wavespace2();
+  {
+    const cudaError_t e = prepare_transforms2();
+    if (e != cudaSuccess) {
+      set_error(std::string("transform set-up failed: ") + cudaGetErrorString(e));
+      return fail(KMM_ERR_CUDA);
+    }
+  }
   if (cudaGetLastError() != cudaSuccess) {
     set_error("kernel attribute set-up failed");
     return fail(KMM_ERR_CUDA);

@@ -137,6 +137,12 @@ void set_error(const std::string &msg);
 void prepare_kernels(Handle &h);
 void convert_planes_d2f(const double2 *src, float2 *dst, int64_t n, cudaStream_t st);
 void prepare_wavespace2();
+cudaError_t prepare_transforms2();
+// Four-step transforms (transforms2.cu); return cudaErrorNotSupported for other lengths.
+cudaError_t launch_zinv2(Handle &h, const double2 *src_planes, void *mid, int nfield, cudaStream_t st);
+cudaError_t launch_xphys2(Handle &h, void *mid, int substep, cudaStream_t st);
+cudaError_t launch_zfwd2(Handle &h, const void *mid, void *dst_planes, int nfield, double scale,
+                         bool dst_fp64, cudaStream_t st);
 cudaError_t launch_control_probe(Handle &h, cudaStream_t st);
 cudaError_t launch_wavespace2(Handle &h, int substep, const double *dt_override, cudaStream_t st);
 

@@ -293,6 +293,8 @@ static cudaError_t zinv_impl(Handle &h, const double2 *src, void *mid, int nfiel
 }
 
 cudaError_t launch_zinv(Handle &h, const double2 *src, void *mid, int nfield, cudaStream_t st) {
+  const cudaError_t e = launch_zinv2(h, src, mid, nfield, st);
+  if (e != cudaErrorNotSupported) return e;
   return h.mixed ? zinv_impl<float>(h, src, mid, nfield, st)
                  : zinv_impl<double>(h, src, mid, nfield, st);
 }
@@ -312,6 +314,8 @@ static cudaError_t zfwd_impl(Handle &h, const void *mid, void *dst, int nfield, 
 
 cudaError_t launch_zfwd(Handle &h, const void *mid, void *dst, int nfield, double scale,
                         bool dst_fp64, cudaStream_t st) {
+  const cudaError_t e = launch_zfwd2(h, mid, dst, nfield, scale, dst_fp64, st);
+  if (e != cudaErrorNotSupported) return e;
   if (h.mixed)
     return dst_fp64 ? zfwd_impl<float, double2>(h, mid, dst, nfield, scale, st)
                     : zfwd_impl<float, float2>(h, mid, dst, nfield, scale, st);
@@ -350,6 +354,8 @@ static cudaError_t xphys_impl(Handle &h, void *mid, int substep, cudaStream_t st
 }
 
 cudaError_t launch_xphys(Handle &h, void *mid, int substep, cudaStream_t st) {
+  const cudaError_t e = launch_xphys2(h, mid, substep, st);
+  if (e != cudaErrorNotSupported) return e;
   return h.mixed ? xphys_impl<float>(h, mid, substep, st) : xphys_impl<double>(h, mid, substep, st);
 }
 
