@@ -208,7 +208,7 @@ int enqueue_substep(Handle &h, int s, cudaStream_t st, cudaEvent_t *ev = nullptr
   if (s == 1)
     if ((rc = rec(KMM_K_DT, [&] { return launch_update_dt(h, s, st); }))) return rc;
   if ((rc = rec(KMM_K_ZFWD, [&] { return launch_zfwd(h, h.MID, h.P, 8, h.rescale, !h.mixed, st); }))) return rc;
-  if ((rc = rec(KMM_K_WAVESPACE, [&] { return launch_wavespace2(h, s, nullptr, st); }))) return rc;
+  if ((rc = rec(KMM_K_WAVESPACE, [&] { return launch_wavespace_split(h, s, nullptr, st); }))) return rc;
   return KMM_OK;
 }
 
@@ -452,10 +452,12 @@ int kmm_create(const kmm_config *cfg, kmm_handle **out) {
     delete h;
     return KMM_ERR_CUDA;
   }
-  if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess) {
+  if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaStreamCreateWithFlags(&h->side, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaEventCreateWithFlags(&h->ev_fork, cudaEventDisableTiming) != cudaSuccess ||
+      cudaEventCreateWithFlags(&h->ev_join, cudaEventDisableTiming) != cudaSuccess) {
     set_error("cudaStreamCreate failed");
-    delete h;
-    return KMM_ERR_CUDA;
+    return fail(KMM_ERR_CUDA);
   }
   const size_t r2 = h->mixed ? sizeof(float2) : sizeof(double2);
   OpsOffsets off = ops_offsets(h->bw, h->ny);
@@ -468,10 +470,11 @@ int kmm_create(const kmm_config *cfg, kmm_handle **out) {
   if ((rc = dalloc(*h, &h->dops, (size_t)off.total))) return fail(rc);
   if ((rc = dalloc(*h, &h->gains, (size_t)h->nmodes))) return fail(rc);
   if ((rc = dalloc(*h, &h->vwall, 2 * (size_t)h->nmodes))) return fail(rc);
-  if ((rc = dalloc(*h, &h->zc, 4 * (size_t)h->ns))) return fail(rc);
-  if ((rc = dalloc(*h, &h->ec, 3 * (size_t)h->ns))) return fail(rc);
+  if ((rc = dalloc(*h, &h->zc, 8 * (size_t)h->ns))) return fail(rc);
+  if ((rc = dalloc(*h, &h->ec, 9 * (size_t)h->ns))) return fail(rc);
   if ((rc = dalloc(*h, &h->xr, 6 * (size_t)h->ns))) return fail(rc);
-  if ((rc = dalloc(*h, &h->ub, (size_t)(2 * h->bw) * h->ns))) return fail(rc);
+  if ((rc = dalloc(*h, &h->ub, 4 * (size_t)split_ub_role(*h)))) return fail(rc);
+  if ((rc = dalloc(*h, &h->dvw, 3 * (size_t)h->nmodes))) return fail(rc);
   if ((rc = dalloc(*h, &h->w00, 3 * (size_t)h->ny * (8 + 2 * h->bw)))) return fail(rc);
   if ((rc = dalloc(*h, &h->staging, 10 * h->ns))) return fail(rc);
   if ((rc = dalloc(*h, &h->dsc, 1))) return fail(rc);
@@ -491,7 +494,6 @@ int kmm_create(const kmm_config *cfg, kmm_handle **out) {
   if ((rc = upload_ops(*h))) return fail(rc);
   if ((rc = make_plans(*h))) return fail(rc);
   prepare_kernels(*h);
-  prepare_wavespace2();
   {
     const cudaError_t e = prepare_transforms2();
     if (e != cudaSuccess) {
@@ -513,11 +515,15 @@ int kmm_destroy(kmm_handle *hh) {
   if (h->gexec) cudaGraphExecDestroy(h->gexec);
   if (h->graph) cudaGraphDestroy(h->graph);
   if (h->stream) cudaStreamSynchronize(h->stream);
+  if (h->side) cudaStreamSynchronize(h->side);
   void *ptrs[] = {h->S, h->RK, h->P, h->MID, h->wbuf, h->wband, h->dops, h->gains, h->vwall, h->zc,
-                  h->ec, h->xr, h->ub, h->w00, h->staging,
+                  h->ec, h->xr, h->ub, h->dvw, h->w00, h->staging,
                   h->fftpos, h->tw64, h->tw32, h->dsc};
   for (void *p : ptrs)
     if (p) cudaFree(p);
+  if (h->ev_fork) cudaEventDestroy(h->ev_fork);
+  if (h->ev_join) cudaEventDestroy(h->ev_join);
+  if (h->side) cudaStreamDestroy(h->side);
   if (h->stream) cudaStreamDestroy(h->stream);
   delete h;
   return KMM_OK;
@@ -761,7 +767,7 @@ int kmm_dev_wavespace(kmm_handle *hh, double *U, double *rk, int s, double dt, k
   KMM_CUDA(cudaStreamSynchronize(st));
   int rc = set_dt_device(h, dt);
   if (rc) return rc;
-  KMM_CUDA(launch_wavespace2(h, s, nullptr, st));
+  KMM_CUDA(launch_wavespace_split(h, s, nullptr, st));
   const int sslots[4] = {0, 1, 2, 6};
   for (int i = 0; i < 4; ++i)
     KMM_CUDA(launch_planes_to_ref(h.S + i * h.ns, reinterpret_cast<double2 *>(U) + sslots[i] * h.ns, 1, h.nmodes, h.ny, st));

@@ -87,11 +87,14 @@ struct Handle {
   double *dops = nullptr;                  // D0, D1, D2, D0_LU bands, integ, dyr, wlo, whi
   float *gains = nullptr;                  // control gains per mode
   double2 *vwall = nullptr;                // [2][nmodes] control wall velocities
-  double2 *zc = nullptr;                   // per-mode solver: complex lines [4][ny][nmodes]
-  double2 *ec = nullptr;                   //                  complex lines [3][ny][nmodes]
-  double *xr = nullptr;                    //                  real lines    [6][ny][nmodes]
-  double *ub = nullptr;                    //                  U factor      [2bw][ny][nmodes]
+  double2 *zc = nullptr;                   // per-mode solver: forward lines  [8][ny][nmodes]
+  double2 *ec = nullptr;                   //                  hvhg outputs   [9][ny][nmodes]
+  double *xr = nullptr;                    //                  real lines     [6][ny][nmodes]
+  double *ub = nullptr;                    //                  U factors, 4 roles (split_ub_role each)
+  double2 *dvw = nullptr;                  //                  wall derivatives [3][nmodes]
   double *w00 = nullptr;                   // mean-mode lines (3 threads)
+  cudaStream_t side = nullptr;             // mean-mode lines run here, forked from / joined to stream
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   double2 *staging = nullptr;              // [7][nz][nxh][ny] reference-layout staging
   int *fftpos = nullptr;
   double2 *tw64 = nullptr;
@@ -136,7 +139,6 @@ void set_error(const std::string &msg);
 // Sets the dynamic shared-memory limits of every kernel instantiation the handle uses.
 void prepare_kernels(Handle &h);
 void convert_planes_d2f(const double2 *src, float2 *dst, int64_t n, cudaStream_t st);
-void prepare_wavespace2();
 cudaError_t prepare_transforms2();
 // Four-step transforms (transforms2.cu); return cudaErrorNotSupported for other lengths.
 cudaError_t launch_zinv2(Handle &h, const double2 *src_planes, void *mid, int nfield, cudaStream_t st);
@@ -144,6 +146,10 @@ cudaError_t launch_xphys2(Handle &h, void *mid, int substep, cudaStream_t st);
 cudaError_t launch_zfwd2(Handle &h, const void *mid, void *dst_planes, int nfield, double scale,
                          bool dst_fp64, cudaStream_t st);
 cudaError_t launch_control_probe(Handle &h, cudaStream_t st);
-cudaError_t launch_wavespace2(Handle &h, int substep, const double *dt_override, cudaStream_t st);
+// Per-mode solves of one substep (wavespace_split.cu): hvhg, Helmholtz and assembly kernels on
+// st, the mean lines on h.side (joined back to st before return).
+cudaError_t launch_wavespace_split(Handle &h, int substep, const double *dt_override, cudaStream_t st);
+// Doubles of U factor storage per solver role.
+int64_t split_ub_role(const Handle &h);
 
 }  // namespace kmm

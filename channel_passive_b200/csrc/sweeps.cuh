@@ -28,6 +28,13 @@
 
 namespace kmm {
 
+// Rows of look-ahead for the L1 prefetches issued by the sweeps: the per-row loads of a thread
+// are independent of its recurrence, so fetching them a few rows early hides the memory latency
+// that would otherwise stall every row (one warp per scheduler has nothing else to run).
+constexpr int kPrefetchRows = 6;
+
+__device__ __forceinline__ void pf_l1(const void *p) { asm volatile("prefetch.global.L1 [%0];" ::"l"(p)); }
+
 struct RLine {
   double *p;
   int64_t s;
@@ -35,15 +42,30 @@ struct RLine {
   __device__ __forceinline__ void st(int i, double v) const { p[(int64_t)(i - 1) * s] = v; }
 };
 
-// Per-mode unit-upper factor: U(p, e) = U(p, p+e), e = 1..2BW, layout [e][y][mode].
+// Per-mode unit-upper factor U(r, r+e), e = 1..2BW.  Inside the profile only the first BW rows
+// reach past e = BW (their last column is 2BW+1), so U is kept as [e = 1..BW][y][mode] plus
+// [r = 1..BW][e = BW+1..2BW][mode] for those rows; every other entry is zero and not stored.
+// A region for one mode set holds BW * es + BW * BW * s doubles.
 template <int BW>
 struct UBand {
-  double *p;
+  double *p;   // [BW][ny][s]
+  double *px;  // [BW][BW][s]
   int64_t s;   // stride between rows (number of modes)
   int64_t es;  // stride between offsets (ny * number of modes)
-  __device__ __forceinline__ double get(int r, int e) const { return p[(int64_t)(e - 1) * es + (int64_t)(r - 1) * s]; }
-  __device__ __forceinline__ void set(int r, int e, double v) const { p[(int64_t)(e - 1) * es + (int64_t)(r - 1) * s] = v; }
+  __device__ __forceinline__ double get(int r, int e) const {
+    if (e <= BW) return p[(int64_t)(e - 1) * es + (int64_t)(r - 1) * s];
+    return r <= BW ? px[(int64_t)((r - 1) * BW + e - BW - 1) * s] : 0.0;
+  }
+  __device__ __forceinline__ void set(int r, int e, double v) const {
+    if (e <= BW) p[(int64_t)(e - 1) * es + (int64_t)(r - 1) * s] = v;
+    else if (r <= BW) px[(int64_t)((r - 1) * BW + e - BW - 1) * s] = v;
+  }
+  __device__ __forceinline__ const double *row_ptr(int r) const { return p + (int64_t)(r - 1) * s; }
 };
+template <int BW>
+__device__ __forceinline__ UBand<BW> make_uband(double *base, int64_t s, int64_t es) {
+  return UBand<BW>{base, base + BW * es, s, es};
+}
 
 template <int BW>
 __device__ __forceinline__ int row_lo(int r, int n) { return (r <= n - BW) ? (r - BW > 1 ? r - BW : 1) : n - 2 * BW; }
@@ -85,15 +107,21 @@ __device__ __forceinline__ double mvr(const double *t, int q, int r, const WT &w
 
 // Forward substitution with the fixed D0 factor for NC complex chains, ascending.
 // in(r, b[NC]) supplies the right-hand sides of row r; out(r, z[NC]) receives the results.
-template <int BW, int NC, typename In, typename Out>
-__device__ __forceinline__ void fwd_fixed(const Tabs<BW> &tb, int n, In in, Out out) {
+struct NoPf {
+  __device__ __forceinline__ void operator()(int) const {}
+};
+
+template <int BW, int NC, typename In, typename Out, typename Pf = NoPf>
+__device__ __forceinline__ void fwd_fixed(const Tabs<BW> &tb, int n, In in, Out out, Pf pf = Pf()) {
   constexpr int W = 2 * BW;
   double2 w[NC][W];
 #pragma unroll
   for (int c = 0; c < NC; ++c)
 #pragma unroll
     for (int k = 0; k < W; ++k) w[c][k] = z2(0.0, 0.0);
+  for (int r = 1; r <= kPrefetchRows && r <= n; ++r) pf(r);
   for (int r = 1; r <= n; ++r) {
+    if (r + kPrefetchRows <= n) pf(r + kPrefetchRows);
     double2 b[NC];
     in(r, b);
     const double *L = tb.l0 + (r - 1) * (W + 1);
@@ -119,8 +147,8 @@ __device__ __forceinline__ void fwd_fixed(const Tabs<BW> &tb, int n, In in, Out 
 
 // Backward substitution (unit U given by ufn(r, e)) for NC complex and NR real chains,
 // descending, with mat-vec emission: emit(q, r, wc, wr) where wc[c][j] = x_{r+j}.
-template <int BW, int NC, int NR, typename UF, typename Zin, typename Emit>
-__device__ __forceinline__ void bwd_emit(int n, UF ufn, Zin zin, Emit emit) {
+template <int BW, int NC, int NR, typename UF, typename Zin, typename Emit, typename Pf = NoPf>
+__device__ __forceinline__ void bwd_emit(int n, UF ufn, Zin zin, Emit emit, Pf pf = Pf()) {
   constexpr int W = 2 * BW + 1;
   constexpr int NCc = NC > 0 ? NC : 1, NRr = NR > 0 ? NR : 1;
   double2 wc[NCc][W];
@@ -132,7 +160,9 @@ __device__ __forceinline__ void bwd_emit(int n, UF ufn, Zin zin, Emit emit) {
 #pragma unroll
     for (int c = 0; c < NRr; ++c) wr[c][j] = 0.0;
   }
+  for (int r = n; r > n - kPrefetchRows && r >= 1; --r) pf(r);
   for (int r = n; r >= 1; --r) {
+    if (r - kPrefetchRows >= 1) pf(r - kPrefetchRows);
 #pragma unroll
     for (int j = W - 1; j >= 1; --j) {
 #pragma unroll
@@ -173,14 +203,16 @@ __device__ __forceinline__ void bwd_emit(int n, UF ufn, Zin zin, Emit emit) {
 
 // Profile Crout LU of a per-mode matrix fused with the forward substitution of NC complex and
 // NR real chains, ascending.  rowA(r, a) fills a[e + 2BW] = A(r, r+e); in(r, bc, br) gives the
-// right-hand sides of row r; out(r, zc, zr) receives the forward results; U goes to ust.
-// Returns L(1, 1), the first pivot.
-template <int BW, int NC, int NR, typename RowA, typename In, typename Out>
-__device__ __forceinline__ double lu_fwd(int n, RowA rowA, In in, Out out, UBand<BW> ust) {
+// right-hand sides of row r; out(r, zc, zr) receives the forward results; U goes to ust (for
+// the backward sweep).  Rows 2BW+1..n-BW only touch U(p, p+e) with e <= BW of the last BW rows,
+// which stay in a register window; the first 2BW and last BW rows read U back from ust.
+template <int BW, int NC, int NR, typename RowA, typename In, typename Out, typename Pf = NoPf>
+__device__ __forceinline__ void lu_fwd(int n, RowA rowA, In in, Out out, UBand<BW> ust, Pf pf = Pf()) {
   constexpr int W = 2 * BW;
   constexpr int NCc = NC > 0 ? NC : 1, NRr = NR > 0 ? NR : 1;
   double2 wc[NCc][W];
   double wr[NRr][W];
+  double Uw[BW][BW];  // Uw[dp-1][e-1] = U(r-dp, r-dp+e)
 #pragma unroll
   for (int k = 0; k < W; ++k) {
 #pragma unroll
@@ -188,37 +220,79 @@ __device__ __forceinline__ double lu_fwd(int n, RowA rowA, In in, Out out, UBand
 #pragma unroll
     for (int c = 0; c < NRr; ++c) wr[c][k] = 0.0;
   }
-  double piv1 = 0.0;
+#pragma unroll
+  for (int i = 0; i < BW; ++i)
+#pragma unroll
+    for (int e = 0; e < BW; ++e) Uw[i][e] = 0.0;
+  for (int r = 1; r <= kPrefetchRows && r <= n; ++r) pf(r);
   for (int r = 1; r <= n; ++r) {
-    const int lo = row_lo<BW>(r, n), hi = row_hi<BW>(r, n);
+    if (r + kPrefetchRows <= n) pf(r + kPrefetchRows);
     double a[4 * BW + 1];
     rowA(r, a);
     double L[W + 1];  // L[d] = L(r, r-d)
+    double Ur[W];     // U(r, r+e), e = 1..W
+    if (r > 2 * BW && r <= n - BW) {
+      // centre row: lo = r - BW, hi = r + BW; U of rows r-BW..r-1 from the register window
 #pragma unroll
-    for (int d = W; d >= 0; --d) {
-      double acc = 0.0;
-      if (r - d >= lo) {
-        acc = a[2 * BW - d];
+      for (int d = W; d > BW; --d) L[d] = 0.0;
 #pragma unroll
-        for (int dp = W; dp > d; --dp)
-          if (r - dp >= lo) acc -= L[dp] * ust.get(r - dp, dp - d);
+      for (int d = BW; d >= 0; --d) {
+        double acc = a[2 * BW - d];
+#pragma unroll
+        for (int dp = BW; dp > d; --dp) acc -= L[dp] * Uw[dp - 1][dp - d - 1];
+        L[d] = acc;
       }
-      L[d] = acc;
-    }
-    if (r == 1) piv1 = L[0];
-    const double rp = 1.0 / L[0];
+      const double rp = 1.0 / L[0];
 #pragma unroll
-    for (int e = 1; e <= W; ++e) {
-      double v = 0.0;
-      if (r + e <= hi) {
-        double acc = a[2 * BW + e];
+      for (int e = 1; e <= W; ++e) {
+        double v = 0.0;
+        if (e <= BW) {
+          double acc = a[2 * BW + e];
 #pragma unroll
-        for (int dp = W; dp >= 1; --dp)
-          if (r - dp >= lo && e + dp <= W) acc -= L[dp] * ust.get(r - dp, e + dp);
-        v = acc * rp;
+          for (int dp = BW; dp >= 1; --dp)
+            if (e + dp <= BW) acc -= L[dp] * Uw[dp - 1][e + dp - 1];
+          v = acc * rp;
+        }
+        Ur[e - 1] = v;
       }
-      ust.set(r, e, v);
+      L[0] = rp;  // from here on L[0] holds the reciprocal pivot
+    } else {
+      const int lo = row_lo<BW>(r, n), hi = row_hi<BW>(r, n);
+#pragma unroll
+      for (int d = W; d >= 0; --d) {
+        double acc = 0.0;
+        if (r - d >= lo) {
+          acc = a[2 * BW - d];
+#pragma unroll
+          for (int dp = W; dp > d; --dp)
+            if (r - dp >= lo) acc -= L[dp] * ust.get(r - dp, dp - d);
+        }
+        L[d] = acc;
+      }
+      const double rp = 1.0 / L[0];
+#pragma unroll
+      for (int e = 1; e <= W; ++e) {
+        double v = 0.0;
+        if (r + e <= hi) {
+          double acc = a[2 * BW + e];
+#pragma unroll
+          for (int dp = W; dp >= 1; --dp)
+            if (r - dp >= lo && e + dp <= W) acc -= L[dp] * ust.get(r - dp, e + dp);
+          v = acc * rp;
+        }
+        Ur[e - 1] = v;
+      }
+      L[0] = rp;
     }
+#pragma unroll
+    for (int e = 1; e <= W; ++e) ust.set(r, e, Ur[e - 1]);
+#pragma unroll
+    for (int i = BW - 1; i >= 1; --i)
+#pragma unroll
+      for (int e = 0; e < BW; ++e) Uw[i][e] = Uw[i - 1][e];
+#pragma unroll
+    for (int e = 0; e < BW; ++e) Uw[0][e] = Ur[e];
+    const double rp = L[0];
     double2 bc[NCc];
     double br[NRr];
     in(r, bc, br);
@@ -249,7 +323,6 @@ __device__ __forceinline__ double lu_fwd(int n, RowA rowA, In in, Out out, UBand
     }
     out(r, zc, zr);
   }
-  return piv1;
 }
 
 }  // namespace kmm

@@ -1,0 +1,635 @@
+// wavespace_split.cu - the per-(kx, kz) wall-normal solves of one substep (wavespace.f90:22-113)
+// as three kernels with several threads per mode.
+//
+// One thread per mode leaves about four warps on each SM (nxh * nz modes), too few to cover the
+// memory latency of the row recurrences.  The solves of one mode are independent chains, so each
+// kernel gives every chain its own warp ("role"); lane t of a warp owns mode 32 * block + t, so
+// every line access of a warp stays one contiguous run.
+//
+// k_hvhg (hvhg.f90:56-159), one D0 solve per role, ascending then descending:
+//   role 0  a3 = -kx^2 f1 - 2 kx kz f5 - kz^2 f3   -> HV0 = i(kx^3+kx kz^2) f2 + i(kx^2 kz+kz^3) f4 + D1 c(a3)
+//   role 1  f8                                      -> HT  = -(i kx f7 + i kz f9 + D1 c(f8))
+//   role 2  f2                                      -> G2  = a1 - i kz D1 c(f2),  V2 = i kx D2 c(f2)
+//   role 3  f4                                      -> G3  = i kx D1 c(f4),       V3 = i kz D2 c(f4)
+//   so hg = G2 + G3, hv = HV0 + (V2 + V3), ht = HT.  At substep 1 roles 0-2 also solve D0 for the
+//   store they feed (RK_STORE 2, 3, 1) and emit D2 of it (DP, DT, DG; solve_g.f90:84-111).
+// k_helmholtz, one profile LU per role (solve_t.f90:28-201, solve_g.f90, solve_v_f.f90:95-298):
+//   role 0  (alpha D0 - beta_t D2) theta = rhs_t      -> St, new RK_STORE 3
+//   role 1  (alpha D0 - beta D2) g = rhs_g             -> Su (g), new RK_STORE 1
+//   role 2  (alpha D0 - beta D2) phi_p = rhs_phi       -> new RK_STORE 2 (partial), then
+//           (D2 - k^2 D0) v_p = phi_p, v_p = vwall     -> Sv = v_p, Sw = D1 v_p
+//   role 3  (alpha D0 - beta D2) phi_h = (p0, 0, ..)   -> phi_h, D2 phi_h, then
+//           (D2 - k^2 D0) v_h = phi_h, v_h = 0 at walls -> v_h, D1 v_h
+//   phi_h and v_h have equal real and imaginary parts (the unit wall vector is (p0, p0),
+//   solve_v_f.f90:142), so role 3 carries one real chain.
+// k_assemble, one thread per (y, mode): C1, C2 from the wall derivatives (solve_v_f.f90:293-298),
+//   v, dv/dy, RK_STORE 2 completion, then u and w (solve_u_w.f90:27-38).
+// k_mean, three threads on a forked stream: wave00.f90:41-714 for U, W and Theta.
+#include <cuda_runtime.h>
+
+#include "kmm_internal.h"
+#include "sweeps.cuh"
+
+namespace kmm {
+
+namespace {
+
+constexpr int kLanes = 32;  // modes per block; one warp per role
+constexpr int kRoles = 4;
+
+enum HLine { H_HV0 = 0, H_HT, H_G2, H_V2, H_G3, H_V3, H_DP, H_DT, H_DG, H_COUNT };
+
+// Low-storage RK3 coefficients alpha, beta, gamma, zeta of substeps 1-3
+// (RK3_initialize, module_runge_kutta.f90:34-45).
+__constant__ double c_rk[4][3] = {{29.0 / 96.0, -3.0 / 40.0, 1.0 / 6.0},
+                                  {37.0 / 160.0, 5.0 / 24.0, 1.0 / 6.0},
+                                  {8.0 / 15.0, 5.0 / 12.0, 3.0 / 4.0},
+                                  {0.0, -17.0 / 60.0, -5.0 / 12.0}};
+__device__ __forceinline__ double rkc(int c, int s) { return c_rk[c - 1][s - 1]; }
+
+struct SplitArgs {
+  int ny, nxh, nz, substep;
+  int64_t nmodes, ns;
+  double2 *S, *RK;
+  const void *P;
+  double2 *zl;       // [8][ny][nm] role-private forward lines
+  double2 *hl;       // [H_COUNT][ny][nm] hvhg outputs
+  double *xr;        // [6][ny][nm] real lines of role 3
+  double *ub;        // [4][ub_role] per-role U factors
+  int64_t ub_role;   // doubles per role
+  double2 *dv;       // [3][nm] dv_p(1), dv_p(n), (dv_h(1), dv_h(n))
+  const double *tabs;   // t0, t1, t2, l0, u0
+  const double2 *vwall;
+  double control_amp;
+  double nu, pr, lmfxr, lmfzr;
+  DevScalars *dsc;
+  const double *dt_ptr;
+};
+
+template <int BW>
+__device__ __forceinline__ Tabs<BW> tabs_at(const double *base, int ny) {
+  const int64_t tw = (int64_t)ny * (4 * BW + 1);
+  Tabs<BW> t;
+  t.t0 = base;
+  t.t1 = base + tw;
+  t.t2 = base + 2 * tw;
+  t.l0 = base + 3 * tw;
+  t.u0 = t.l0 + (int64_t)ny * (2 * BW + 1);
+  return t;
+}
+
+template <typename PT> __device__ __forceinline__ double2 ldp(const PT *p);
+template <> __device__ __forceinline__ double2 ldp<double2>(const double2 *p) { return *p; }
+template <> __device__ __forceinline__ double2 ldp<float2>(const float2 *p) {
+  const float2 v = *p;
+  return make_double2((double)v.x, (double)v.y);
+}
+
+struct ModeK {
+  double kx, kz, k2;
+};
+__device__ __forceinline__ ModeK mode_k(const SplitArgs &a, int64_t m) {
+  const int kzi = (int)(m / a.nxh), kxi = (int)(m - (int64_t)kzi * a.nxh);
+  const int kzint = (kzi <= a.nz / 2) ? kzi : kzi - a.nz;  // set_waveno
+  ModeK k;
+  k.kx = kxi * a.lmfxr;                                   // wavespace.f90:69
+  k.kz = kzint * a.lmfzr;
+  k.k2 = k.kx * k.kx + k.kz * k.kz;
+  return k;
+}
+
+// A = ca D0 - cb D2 with the Dirichlet first / last rows, as an offset row.
+template <int BW>
+__device__ __forceinline__ void helm_row(const Tabs<BW> &tb, int r, int n, double ca, double cb, double *out) {
+  const double *r0 = trow<BW>(tb.t0, r), *r2 = trow<BW>(tb.t2, r);
+  if (r == 1 || r == n) {
+#pragma unroll
+    for (int e = -2 * BW; e <= 2 * BW; ++e) out[e + 2 * BW] = 0.0;
+    out[2 * BW] = ca * r0[0] - cb * r2[0];
+    return;
+  }
+#pragma unroll
+  for (int e = -2 * BW; e <= 2 * BW; ++e) out[e + 2 * BW] = ca * r0[e] - cb * r2[e];
+}
+
+// (D2 - k^2 D0) with the wall rows replaced by D0 (v given there), solve_v_f.f90:95-140.
+template <int BW>
+__device__ __forceinline__ void vrow(const Tabs<BW> &tb, int r, int n, double k2, double *row) {
+  const double *r0 = trow<BW>(tb.t0, r), *r2 = trow<BW>(tb.t2, r);
+  if (r == 1 || r == n) {
+#pragma unroll
+    for (int e = -2 * BW; e <= 2 * BW; ++e) row[e + 2 * BW] = 0.0;
+    row[2 * BW] = r0[0];
+    return;
+  }
+#pragma unroll
+  for (int e = -2 * BW; e <= 2 * BW; ++e) row[e + 2 * BW] = -k2 * r0[e] + r2[e];
+}
+
+// ------------------------------------------------------------------------------------------
+// k_hvhg: role ROLE of mode m; NC = 2 adds the store's D0 solve at substep 1.
+template <int BW, typename PT, int ROLE, int NC>
+__device__ __forceinline__ void hvhg_role(const SplitArgs &a, const Tabs<BW> &tb, int64_t m) {
+  const int n = a.ny;
+  const int64_t nm = a.nmodes, ns = a.ns;
+  const ModeK k = mode_k(a, m);
+  const double kx = k.kx, kz = k.kz;
+  const double kxkz = kx * kz, kx2 = kx * kx, kz2 = kz * kz;
+  const PT *P = reinterpret_cast<const PT *>(a.P) + m;
+  auto prod = [&](int slot, int r) { return ldp<PT>(P + slot * ns + (int64_t)(r - 1) * nm); };
+  auto pfp = [&](int slot, int r) { pf_l1(P + slot * ns + (int64_t)(r - 1) * nm); };
+  const DLine Z0{a.zl + (2 * ROLE) * ns + m, nm}, Z1{a.zl + (2 * ROLE + 1) * ns + m, nm};
+  constexpr int store_slot = ROLE == 0 ? 1 : ROLE == 1 ? 2 : 0;  // RK_STORE 2, 3, 1
+  constexpr int d2_line = ROLE == 0 ? H_DP : ROLE == 1 ? H_DT : H_DG;
+  const DLine Rs{a.RK + store_slot * ns + m, nm};
+  auto hl = [&](int i) { return DLine{a.hl + i * ns + m, nm}; };
+  auto ufix = [&](int r, int e) { return tb.u0[(r - 1) * 2 * BW + e - 1]; };
+
+  fwd_fixed<BW, NC>(tb, n,
+      [&](int r, double2 *b) {
+        if constexpr (ROLE == 0) {
+          const double2 f1 = prod(0, r), f3 = prod(2, r), f5 = prod(4, r);
+          b[0] = zsub(zsub(zscale(-kx2, f1), zscale(2.0 * kxkz, f5)), zscale(kz2, f3));
+        } else if constexpr (ROLE == 1) {
+          b[0] = prod(6, r);
+        } else if constexpr (ROLE == 2) {
+          b[0] = prod(1, r);
+        } else {
+          b[0] = prod(3, r);
+        }
+        if constexpr (NC == 2) b[1] = Rs.ld(r);
+      },
+      [&](int r, const double2 *z) {
+        Z0.st(r, z[0]);
+        if constexpr (NC == 2) Z1.st(r, z[1]);
+      },
+      [&](int r) {
+        if constexpr (ROLE == 0) { pfp(0, r); pfp(2, r); pfp(4, r); }
+        else pfp(ROLE == 1 ? 6 : ROLE == 2 ? 1 : 3, r);
+        if constexpr (NC == 2) pf_l1(Rs.p + (int64_t)(r - 1) * nm);
+      });
+
+  bwd_emit<BW, NC, 0>(n, ufix,
+      [&](int r, double2 *zc, double *) {
+        zc[0] = Z0.ld(r);
+        if constexpr (NC == 2) zc[1] = Z1.ld(r);
+      },
+      [&](int q, int r, const double2 (&wc)[NC][2 * BW + 1], const double (&)[1][2 * BW + 1]) {
+        if constexpr (ROLE == 0) {
+          const double c2i = kx * kx * kx + kx * (kz * kz), c4i = (kx * kx) * kz + kz * kz * kz;
+          const double2 f2 = prod(1, q), f4 = prod(3, q);
+          const double2 ehv = z2(-c2i * f2.y - c4i * f4.y, c2i * f2.x + c4i * f4.x);
+          hl(H_HV0).st(q, zadd(ehv, mvc<BW>(tb.t1, q, r, wc[0])));
+        } else if constexpr (ROLE == 1) {
+          const double2 f7 = prod(5, q), f9 = prod(7, q);
+          const double2 t7 = z2(-kx * f7.y - kz * f9.y, kx * f7.x + kz * f9.x);
+          const double2 t = zadd(t7, mvc<BW>(tb.t1, q, r, wc[0]));
+          hl(H_HT).st(q, z2(-t.x, -t.y));
+        } else if constexpr (ROLE == 2) {
+          const double2 f1 = prod(0, q), f3 = prod(2, q), f5 = prod(4, q);
+          const double2 a1 = zadd(zscale(kxkz, zsub(f1, f3)), zscale(kz2 - kx2, f5));
+          const double2 d1 = mvc<BW>(tb.t1, q, r, wc[0]), d2 = mvc<BW>(tb.t2, q, r, wc[0]);
+          hl(H_G2).st(q, zadd(a1, z2(kz * d1.y, -kz * d1.x)));
+          hl(H_V2).st(q, z2(-kx * d2.y, kx * d2.x));
+        } else {
+          const double2 d1 = mvc<BW>(tb.t1, q, r, wc[0]), d2 = mvc<BW>(tb.t2, q, r, wc[0]);
+          hl(H_G3).st(q, z2(-kx * d1.y, kx * d1.x));
+          hl(H_V3).st(q, z2(-kz * d2.y, kz * d2.x));
+        }
+        if constexpr (NC == 2) hl(d2_line).st(q, mvc<BW>(tb.t2, q, r, wc[NC - 1]));
+      },
+      [&](int r) {
+        pf_l1(Z0.p + (int64_t)(r - 1) * nm);
+        if constexpr (NC == 2) pf_l1(Z1.p + (int64_t)(r - 1) * nm);
+        if (r <= n - 2 * BW) {
+          const int q = r + BW;
+          if constexpr (ROLE == 0) { pfp(1, q); pfp(3, q); }
+          else if constexpr (ROLE == 1) { pfp(5, q); pfp(7, q); }
+          else if constexpr (ROLE == 2) { pfp(0, q); pfp(2, q); pfp(4, q); }
+        }
+      });
+}
+
+template <int BW, typename PT>
+__global__ void __launch_bounds__(kLanes * kRoles, 4) k_hvhg(SplitArgs a) {
+  if (a.dsc->err) return;
+  const int role = threadIdx.x / kLanes;
+  const int64_t m = (int64_t)blockIdx.x * kLanes + (threadIdx.x % kLanes);
+  if (m == 0 || m >= a.nmodes) return;
+  const Tabs<BW> tb = tabs_at<BW>(a.tabs, a.ny);
+  const bool s1 = a.substep == 1;
+  switch (role) {
+    case 0: s1 ? hvhg_role<BW, PT, 0, 2>(a, tb, m) : hvhg_role<BW, PT, 0, 1>(a, tb, m); break;
+    case 1: s1 ? hvhg_role<BW, PT, 1, 2>(a, tb, m) : hvhg_role<BW, PT, 1, 1>(a, tb, m); break;
+    case 2: s1 ? hvhg_role<BW, PT, 2, 2>(a, tb, m) : hvhg_role<BW, PT, 2, 1>(a, tb, m); break;
+    default: hvhg_role<BW, PT, 3, 1>(a, tb, m); break;
+  }
+}
+
+// ------------------------------------------------------------------------------------------
+// k_helmholtz
+template <int BW, int ROLE>
+__device__ __forceinline__ void helmholtz_role(const SplitArgs &a, const Tabs<BW> &tb, int64_t m) {
+  const int n = a.ny, s = a.substep;
+  const int64_t nm = a.nmodes, ns = a.ns;
+  const double dt = *a.dt_ptr, nu = a.nu;
+  const double k2 = mode_k(a, m).k2;
+  auto hl = [&](int i) { return DLine{a.hl + i * ns + m, nm}; };
+  auto pfl = [&](const void *base, int r) {
+    pf_l1(reinterpret_cast<const char *>(base) + (int64_t)(r - 1) * nm * sizeof(double2));
+  };
+  const UBand<BW> ub = make_uband<BW>(a.ub + ROLE * a.ub_role + m, nm, ns);
+  auto uper = [&](int r, int e) { return ub.get(r, e); };
+  const DLine Zr{a.zl + ROLE * ns + m, nm};
+
+  // RK right-hand side (solve_g.f90:84-123): rows 1 and n are the Dirichlet rows (zero)
+  auto rhs = [&](double2 store, double2 h, double2 d2, double visc, int r) {
+    if (r == 1 || r == n) return z2(0.0, 0.0);
+    if (s == 1) {
+      const double alpha = dt * rkc(1, s) * visc, gamma = dt * rkc(3, s);
+      return zadd(zadd(zscale(1.0 - alpha * k2, store), zscale(gamma, h)), zscale(alpha, d2));
+    }
+    return zadd(store, zscale(dt * rkc(3, s), h));
+  };
+  // new store (solve_g.f90:138-185): zeta' h + (1 - alpha' k2) f + alpha' D2 f, or f at s = 3
+  auto store_new = [&](double2 h, double2 f, double2 d2f, double visc) {
+    if (s == 3) return f;
+    const double alpha = dt * rkc(1, s + 1) * visc, zeta = dt * rkc(4, s + 1);
+    return zadd(zadd(zscale(zeta, h), zscale(1.0 - alpha * k2, f)), zscale(alpha, d2f));
+  };
+
+  if constexpr (ROLE <= 2) {
+    // one complex Helmholtz solve: theta (role 0), g (role 1), phi_p (role 2)
+    const double visc = ROLE == 0 ? nu / a.pr : nu;
+    const double beta = dt * rkc(2, s) * visc;
+    const double dummy = 1.0 + beta * k2;
+    const int sslot = ROLE == 0 ? 2 : ROLE == 1 ? 0 : 1;
+    const DLine store{a.RK + sslot * ns + m, nm};
+    const DLine d2l = hl(ROLE == 0 ? H_DT : ROLE == 1 ? H_DG : H_DP);
+    auto hsum = [&](int r) {
+      if constexpr (ROLE == 0) return hl(H_HT).ld(r);
+      if (ROLE == 1) return zadd(hl(H_G2).ld(r), hl(H_G3).ld(r));
+      return zadd(hl(H_HV0).ld(r), zadd(hl(H_V2).ld(r), hl(H_V3).ld(r)));
+    };
+    auto pfh = [&](int r) {
+      if constexpr (ROLE == 0) pfl(hl(H_HT).p, r);
+      else if constexpr (ROLE == 1) { pfl(hl(H_G2).p, r); pfl(hl(H_G3).p, r); }
+      else { pfl(hl(H_HV0).p, r); pfl(hl(H_V2).p, r); pfl(hl(H_V3).p, r); }
+    };
+    lu_fwd<BW, 1, 0>(n, [&](int r, double *row) { helm_row<BW>(tb, r, n, dummy, beta, row); },
+        [&](int r, double2 *bc, double *) {
+          bc[0] = rhs(store.ld(r), hsum(r), s == 1 ? d2l.ld(r) : z2(0.0, 0.0), visc, r);
+        },
+        [&](int r, const double2 *zc, const double *) { Zr.st(r, zc[0]); }, ub,
+        [&](int r) {
+          pfl(store.p, r);
+          pfh(r);
+          if (s == 1) pfl(d2l.p, r);
+        });
+    const DLine out{ROLE == 0 ? a.S + 3 * ns + m : ROLE == 1 ? a.S + m : a.zl + 4 * ns + m, nm};
+    bwd_emit<BW, 1, 0>(n, uper, [&](int r, double2 *zc, double *) { zc[0] = Zr.ld(r); },
+        [&](int q, int r, const double2 (&wc)[1][2 * BW + 1], const double (&)[1][2 * BW + 1]) {
+          const double2 f = mvc<BW>(tb.t0, q, r, wc[0]), d2f = mvc<BW>(tb.t2, q, r, wc[0]);
+          out.st(q, f);
+          store.st(q, store_new(hsum(q), f, d2f, visc));
+        },
+        [&](int r) {
+          pfl(Zr.p, r);
+          const int q = r + BW;
+          if (r <= n - 2 * BW) pfh(q);
+        });
+    if constexpr (ROLE != 2) return;
+    // (D2 - k^2 D0) v_p = phi_p with v_p = the wall velocity at rows 1 and n
+    double2 vlo = z2(0.0, 0.0), vhi = z2(0.0, 0.0);
+    if (a.control_amp != 0.0) {
+      vlo = a.vwall[m];
+      vhi = a.vwall[nm + m];
+    }
+    lu_fwd<BW, 1, 0>(n, [&](int r, double *row) { vrow<BW>(tb, r, n, k2, row); },
+        [&](int r, double2 *bc, double *) { bc[0] = (r == 1) ? vlo : (r == n) ? vhi : out.ld(r); },
+        [&](int r, const double2 *zc, const double *) { Zr.st(r, zc[0]); }, ub,
+        [&](int r) { pfl(out.p, r); });
+    const DLine Sv{a.S + ns + m, nm}, Sw{a.S + 2 * ns + m, nm};
+    bwd_emit<BW, 1, 0>(n, uper, [&](int r, double2 *zc, double *) { zc[0] = Zr.ld(r); },
+        [&](int q, int r, const double2 (&wc)[1][2 * BW + 1], const double (&)[1][2 * BW + 1]) {
+          const double2 vp = mvc<BW>(tb.t0, q, r, wc[0]), dvp = mvc<BW>(tb.t1, q, r, wc[0]);
+          Sv.st(q, vp);
+          Sw.st(q, dvp);
+          if (q == 1) a.dv[m] = dvp;
+          if (q == n) a.dv[nm + m] = dvp;
+        },
+        [&](int r) { pfl(Zr.p, r); });
+  } else {
+    // phi_h: (alpha D0 - beta D2) phi_h = unit wall vector, then v_h (real chains)
+    const double beta = dt * rkc(2, s) * nu;
+    const double dummy = 1.0 + beta * k2;
+    const double p0 = dummy * trow<BW>(tb.t0, 1)[0] - beta * trow<BW>(tb.t2, 1)[0];  // A_g(1,1)
+    const RLine Xz{a.xr + m, nm}, X1{a.xr + ns + m, nm}, X2{a.xr + 2 * ns + m, nm};
+    const RLine X4{a.xr + 3 * ns + m, nm}, X5{a.xr + 4 * ns + m, nm};
+    auto pfr = [&](const double *base, int r) { pf_l1(base + (int64_t)(r - 1) * nm); };
+    lu_fwd<BW, 0, 1>(n, [&](int r, double *row) { helm_row<BW>(tb, r, n, dummy, beta, row); },
+        [&](int r, double2 *, double *br) { br[0] = (r == 1) ? p0 : 0.0; },
+        [&](int r, const double2 *, const double *zr) { Xz.st(r, zr[0]); }, ub);
+    bwd_emit<BW, 0, 1>(n, uper, [&](int r, double2 *, double *zr) { zr[0] = Xz.ld(r); },
+        [&](int q, int r, const double2 (&)[1][2 * BW + 1], const double (&wr)[1][2 * BW + 1]) {
+          X1.st(q, mvr<BW>(tb.t0, q, r, wr[0]));  // phi_h (real part = imaginary part)
+          X2.st(q, mvr<BW>(tb.t2, q, r, wr[0]));  // D2 phi_h
+        },
+        [&](int r) { pfr(Xz.p, r); });
+    lu_fwd<BW, 0, 1>(n, [&](int r, double *row) { vrow<BW>(tb, r, n, k2, row); },
+        [&](int r, double2 *, double *br) { br[0] = (r == 1 || r == n) ? 0.0 : X1.ld(r); },
+        [&](int r, const double2 *, const double *zr) { Xz.st(r, zr[0]); }, ub,
+        [&](int r) { pfr(X1.p, r); });
+    double dh1 = 0.0, dhn = 0.0;
+    bwd_emit<BW, 0, 1>(n, uper, [&](int r, double2 *, double *zr) { zr[0] = Xz.ld(r); },
+        [&](int q, int r, const double2 (&)[1][2 * BW + 1], const double (&wr)[1][2 * BW + 1]) {
+          const double vh = mvr<BW>(tb.t0, q, r, wr[0]), dvh = mvr<BW>(tb.t1, q, r, wr[0]);
+          X4.st(q, vh);
+          X5.st(q, dvh);
+          if (q == 1) dh1 = dvh;
+          if (q == n) dhn = dvh;
+        },
+        [&](int r) { pfr(Xz.p, r); });
+    a.dv[2 * nm + m] = z2(dh1, dhn);
+  }
+}
+
+template <int BW>
+__global__ void __launch_bounds__(kLanes * kRoles, 4) k_helmholtz(SplitArgs a) {
+  if (a.dsc->err) return;  // a failed dt update leaves the state untouched
+  const int role = threadIdx.x / kLanes;
+  const int64_t m = (int64_t)blockIdx.x * kLanes + (threadIdx.x % kLanes);
+  if (m == 0 || m >= a.nmodes) return;
+  const Tabs<BW> tb = tabs_at<BW>(a.tabs, a.ny);
+  switch (role) {
+    case 0: helmholtz_role<BW, 0>(a, tb, m); break;
+    case 1: helmholtz_role<BW, 1>(a, tb, m); break;
+    case 2: helmholtz_role<BW, 2>(a, tb, m); break;
+    default: helmholtz_role<BW, 3>(a, tb, m); break;
+  }
+}
+
+// ------------------------------------------------------------------------------------------
+// k_assemble: one thread per (y, mode), mode fastest.
+__global__ void __launch_bounds__(256) k_assemble(SplitArgs a) {
+  if (a.dsc->err) return;
+  const int64_t nm = a.nmodes, ns = a.ns;
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= ns) return;
+  const int r = (int)(t / nm) + 1;
+  const int64_t m = t - (int64_t)(r - 1) * nm;
+  if (m == 0) return;
+  const int n = a.ny, s = a.substep, rr = n + 1 - r;
+  const ModeK k = mode_k(a, m);
+  // C1, C2 (solve_v_f.f90:293-294); the homogeneous derivative is dvh * (1 + i)
+  const double2 dvh = a.dv[2 * nm + m];
+  const double2 h1 = z2(dvh.x, dvh.x), hn = z2(dvh.y, dvh.y);
+  const double2 d1 = a.dv[m], dn = a.dv[nm + m];
+  const double2 den = zsub(zmul(h1, h1), zmul(hn, hn));
+  const double2 C1 = zdiv(zsub(zmul(hn, dn), zmul(h1, d1)), den);
+  const double2 C2 = zdiv(zsub(zmul(h1, dn), zmul(hn, d1)), den);
+  const double2 C1c = z2(C1.x - C1.y, C1.x + C1.y), C2c = z2(C2.x - C2.y, C2.x + C2.y);  // C * (1 + i)
+  double cd = 1.0, ca = 0.0;
+  if (s != 3) {
+    const double alpha = *a.dt_ptr * a.nu * rkc(1, s + 1);
+    cd = 1.0 - alpha * k.k2;
+    ca = alpha;
+  }
+  const double *xr = a.xr + m;
+  auto X = [&](int i, int row) { return xr[i * ns + (int64_t)(row - 1) * nm]; };
+  const int64_t o = (int64_t)(r - 1) * nm + m;
+  double2 *S = a.S, *Rp = a.RK + ns;
+  const double2 v = zadd(zadd(S[ns + o], zscale(X(3, r), C1c)), zscale(X(3, rr), C2c));
+  const double2 dv = zsub(zadd(S[2 * ns + o], zscale(X(4, r), C1c)), zscale(X(4, rr), C2c));
+  double2 sp = Rp[o];
+  sp = zadd(sp, zscale(cd * X(1, r), C1c));
+  sp = zadd(sp, zscale(cd * X(1, rr), C2c));
+  if (s != 3) {
+    sp = zadd(sp, zscale(ca * X(2, r), C1c));
+    sp = zadd(sp, zscale(ca * X(2, rr), C2c));
+  }
+  Rp[o] = sp;
+  const double2 kxx = z2(0.0, k.kx / k.k2), kzz = z2(0.0, k.kz / k.k2);
+  const double2 g = S[o];
+  S[o] = zsub(zmul(kxx, dv), zmul(kzz, g));  // solve_u_w.f90:27-38
+  S[ns + o] = v;
+  S[2 * ns + o] = zadd(zmul(kxx, g), zmul(kzz, dv));
+}
+
+// ------------------------------------------------------------------------------------------
+// k_mean: wave00.f90 for one mean line per thread: U (line 0: forced, Galilean shift),
+// W (line 1: phi = 0), Theta (line 2: nu/pr, forced to the bulk value).
+struct MeanArgs {
+  int ny, substep;
+  int64_t nmodes, ns;
+  double2 *S, *RK;
+  const void *P;
+  double *w00;
+  const double *tabs, *integ;
+  double nu, pr, bulk_u, bulk_w, bulk_t, u_gal;
+  DevScalars *dsc;
+  const double *dt_ptr;
+};
+
+template <int BW, typename PT>
+__global__ void k_mean(MeanArgs a) {
+  const int line = threadIdx.x;
+  if (line >= 3 || a.dsc->err) return;
+  const Tabs<BW> tb = tabs_at<BW>(a.tabs, a.ny);
+  const int n = a.ny, s = a.substep;
+  const int64_t ns = a.ns;
+  const double dt = *a.dt_ptr;
+  const double visc = (line == 2) ? a.nu / a.pr : a.nu;
+  const double gal = (line == 0) ? a.u_gal : 0.0;
+  const double bulk = (line == 0) ? a.bulk_u : (line == 1) ? a.bulk_w : a.bulk_t;
+  const int pslot = (line == 0) ? 1 : (line == 1) ? 3 : 6;  // uv, vw, v theta
+  const PT *P = reinterpret_cast<const PT *>(a.P) + pslot * ns;
+  const DLine store{a.RK + line * ns, a.nmodes};
+  const DLine out{a.S + (line == 0 ? 0 : line == 1 ? 2 : 3) * ns, a.nmodes};
+  const int64_t per = 8 * (int64_t)n + 2 * BW * (int64_t)n;  // doubles per line thread
+  double *base = a.w00 + line * per;
+  const DLine Zf{reinterpret_cast<double2 *>(base), 1}, Zs{reinterpret_cast<double2 *>(base) + n, 1};
+  const DLine R{reinterpret_cast<double2 *>(base) + 2 * n, 1}, DF{reinterpret_cast<double2 *>(base) + 3 * n, 1};
+  const UBand<BW> ub = make_uband<BW>(base + 8 * (int64_t)n, 1, n);
+  auto ufix = [&](int r, int e) { return tb.u0[(r - 1) * 2 * BW + e - 1]; };
+  // D0 solves: the flux product (and the store at substep 1)
+  fwd_fixed<BW, 2>(tb, n,
+      [&](int r, double2 *b) {
+        b[0] = ldp<PT>(P + (int64_t)(r - 1) * a.nmodes);
+        b[1] = (s == 1) ? store.ld(r) : z2(0.0, 0.0);
+      },
+      [&](int r, const double2 *z) { Zf.st(r, z[0]); Zs.st(r, z[1]); },
+      [&](int r) {
+        pf_l1(P + (int64_t)(r - 1) * a.nmodes);
+        pf_l1(store.p + (int64_t)(r - 1) * a.nmodes);
+      });
+  bwd_emit<BW, 2, 0>(n, ufix,
+      [&](int r, double2 *zc, double *) { zc[0] = Zf.ld(r); zc[1] = Zs.ld(r); },
+      [&](int q, int r, const double2 (&wc)[2][2 * BW + 1], const double (&)[1][2 * BW + 1]) {
+        const double2 d = mvc<BW>(tb.t1, q, r, wc[0]);  // d/dy of the flux
+        DF.st(q, d);
+        double2 b;
+        const double gamma = dt * rkc(3, s);
+        if (s == 1) {
+          const double alpha = dt * rkc(1, s) * visc;
+          b = zsub(zadd(store.ld(q), zscale(alpha, mvc<BW>(tb.t2, q, r, wc[1]))), zscale(gamma, d));
+        } else {
+          b = zsub(store.ld(q), zscale(gamma, d));
+        }
+        // wave00.f90:169-173: zero wall rows, interior real part + u_gal, imaginary part 1
+        R.st(q, (q == 1 || q == n) ? z2(0.0, 0.0) : z2(b.x + gal, 1.0));
+      });
+  // (D0 - beta D2) c = rhs, Dirichlet rows
+  const double beta = dt * rkc(2, s) * visc;
+  lu_fwd<BW, 1, 0>(n, [&](int r, double *row) { helm_row<BW>(tb, r, n, 1.0, beta, row); },
+      [&](int r, double2 *bc, double *) { bc[0] = R.ld(r); },
+      [&](int r, const double2 *zc, const double *) { R.st(r, zc[0]); }, ub);
+  {  // backward substitution storing the coefficients (the integral needs all of them)
+    double2 w[2 * BW + 1];
+#pragma unroll
+    for (int j = 0; j <= 2 * BW; ++j) w[j] = z2(0.0, 0.0);
+    for (int r = n; r >= 1; --r) {
+#pragma unroll
+      for (int j = 2 * BW; j >= 1; --j) w[j] = w[j - 1];
+      double2 acc = R.ld(r);
+#pragma unroll
+      for (int e = 1; e <= 2 * BW; ++e) {
+        const double u = ub.get(r, e);
+        acc.x -= u * w[e].x;
+        acc.y -= u * w[e].y;
+      }
+      w[0] = acc;
+      R.st(r, acc);
+    }
+  }
+  double2 integral = z2(0.0, 0.0);
+  for (int i = 1; i <= n; ++i) integral = zadd(integral, zscale(__ldg(a.integ + i - 1), R.ld(i)));  // LABS_integration
+  double phi = (bulk - 0.5 * integral.x) / (0.5 * integral.y);  // calculate_phi
+  if (line == 1) phi = 0.0;                                       // wave00.f90:396
+  // c = Re c + phi Im c (real); mean profile D0 c, store alpha' D2 c + profile - zeta' d
+  for (int r = 1; r <= n; ++r) {
+    const double2 c = R.ld(r);
+    Zf.st(r, z2(c.x + phi * c.y, 0.0));
+  }
+  if (s == 3) {
+    const double *r1 = trow<BW>(tb.t1, 1), *rn = trow<BW>(tb.t1, n);
+    const double wall = r1[0] * Zf.ld(1).x + r1[1] * Zf.ld(2).x - rn[-1] * Zf.ld(n - 1).x - rn[0] * Zf.ld(n).x;
+    if (line == 0) a.dsc->wall_shear_stress = 0.5 * a.nu * wall;
+    if (line == 2) a.dsc->wall_theta_stress = 0.5 * a.nu / a.pr * wall;
+  }
+  if (line == 0) a.dsc->phi_dpdx[s - 1] = phi;
+  if (line == 2) a.dsc->phi_dtdx[s - 1] = phi;
+  bwd_emit<BW, 1, 0>(n, [&](int, int) { return 0.0; },
+      [&](int r, double2 *zc, double *) { zc[0] = Zf.ld(r); },
+      [&](int q, int r, const double2 (&wc)[1][2 * BW + 1], const double (&)[1][2 * BW + 1]) {
+        double2 prof = mvc<BW>(tb.t0, q, r, wc[0]);
+        prof.x -= gal;
+        out.st(q, prof);
+        if (s != 3) {
+          const double alpha = dt * rkc(1, s + 1) * visc, zeta = dt * rkc(4, s + 1);
+          store.st(q, zsub(zadd(zscale(alpha, mvc<BW>(tb.t2, q, r, wc[0])), prof), zscale(zeta, DF.ld(q))));
+        } else {
+          store.st(q, prof);
+        }
+      },
+      [&](int r) { pf_l1(store.p + (int64_t)(r - 1) * a.nmodes); });
+  if (line == 1) {  // v mean = 0 (wave00.f90:462)
+    const DLine Sv{a.S + ns, a.nmodes};
+    for (int r = 1; r <= n; ++r) Sv.st(r, z2(0.0, 0.0));
+  }
+}
+
+template <int BW>
+cudaError_t split_bw(Handle &h, int substep, const double *dt_ptr, cudaStream_t st) {
+  const OpsOffsets off = ops_offsets(h.bw, h.ny);
+  const double *dtp = dt_ptr ? dt_ptr : &h.dsc->dt;
+  SplitArgs a;
+  a.ny = h.ny;
+  a.nxh = h.nxh;
+  a.nz = h.nz;
+  a.substep = substep;
+  a.nmodes = h.nmodes;
+  a.ns = h.ns;
+  a.S = h.S;
+  a.RK = h.RK;
+  a.P = h.P;
+  a.zl = h.zc;
+  a.hl = h.ec;
+  a.xr = h.xr;
+  a.ub = h.ub;
+  a.ub_role = split_ub_role(h);
+  a.dv = h.dvw;
+  a.tabs = h.dops + off.t0;
+  a.vwall = h.vwall;
+  a.control_amp = h.cfg.control_amp;
+  a.nu = h.cfg.nu;
+  a.pr = h.cfg.pr;
+  a.lmfxr = h.lmfxr;
+  a.lmfzr = h.lmfzr;
+  a.dsc = h.dsc;
+  a.dt_ptr = dtp;
+
+  MeanArgs ma;
+  ma.ny = h.ny;
+  ma.substep = substep;
+  ma.nmodes = h.nmodes;
+  ma.ns = h.ns;
+  ma.S = h.S;
+  ma.RK = h.RK;
+  ma.P = h.P;
+  ma.w00 = h.w00;
+  ma.tabs = a.tabs;
+  ma.integ = h.dops + off.integ;
+  ma.nu = h.cfg.nu;
+  ma.pr = h.cfg.pr;
+  ma.bulk_u = h.cfg.bulk_vel_u;
+  ma.bulk_w = h.cfg.bulk_vel_w;
+  ma.bulk_t = h.cfg.bulk_t;
+  ma.u_gal = h.cfg.u_gal;
+  ma.dsc = h.dsc;
+  ma.dt_ptr = dtp;
+
+  // the mean lines touch only mode 0, which the split kernels skip: run them beside those
+  cudaError_t e = cudaEventRecord(h.ev_fork, st);
+  if (e != cudaSuccess) return e;
+  if ((e = cudaStreamWaitEvent(h.side, h.ev_fork, 0)) != cudaSuccess) return e;
+  if (h.mixed) k_mean<BW, float2><<<1, 32, 0, h.side>>>(ma);
+  else k_mean<BW, double2><<<1, 32, 0, h.side>>>(ma);
+  if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  if ((e = cudaEventRecord(h.ev_join, h.side)) != cudaSuccess) return e;
+
+  const unsigned blocks = (unsigned)((h.nmodes + kLanes - 1) / kLanes);
+  if (h.mixed) k_hvhg<BW, float2><<<blocks, kLanes * kRoles, 0, st>>>(a);
+  else k_hvhg<BW, double2><<<blocks, kLanes * kRoles, 0, st>>>(a);
+  if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  k_helmholtz<BW><<<blocks, kLanes * kRoles, 0, st>>>(a);
+  if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  const unsigned ablocks = (unsigned)((h.ns + 255) / 256);
+  k_assemble<<<ablocks, 256, 0, st>>>(a);
+  if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  return cudaStreamWaitEvent(st, h.ev_join, 0);
+}
+
+}  // namespace
+
+int64_t split_ub_role(const Handle &h) {
+  return (int64_t)h.bw * h.ns + (int64_t)h.bw * h.bw * h.nmodes;
+}
+
+cudaError_t launch_wavespace_split(Handle &h, int substep, const double *dt_ptr, cudaStream_t st) {
+  if (h.cfg.control_amp != 0.0) {
+    cudaError_t e = launch_control_probe(h, st);
+    if (e != cudaSuccess) return e;
+  }
+  switch (h.bw) {
+    case 2: return split_bw<2>(h, substep, dt_ptr, st);
+    case 3: return split_bw<3>(h, substep, dt_ptr, st);
+    case 4: return split_bw<4>(h, substep, dt_ptr, st);
+    case 5: return split_bw<5>(h, substep, dt_ptr, st);
+    case 6: return split_bw<6>(h, substep, dt_ptr, st);
+    case 7: return split_bw<7>(h, substep, dt_ptr, st);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+}  // namespace kmm
