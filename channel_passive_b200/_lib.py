@@ -23,8 +23,8 @@ KMM_ERR_TIMEOUT = 6
 KMM_PREC_FP64 = 0
 KMM_PREC_MIXED = 1
 KMM_NOALLOC_MAX_DOUBLES = 2097152
-KMM_NKERNEL = 6
-KERNEL_NAMES = ("begin_substep", "zinv", "xphys", "update_dt", "zfwd", "wavespace")
+KMM_NKERNEL = 8
+KERNEL_NAMES = ("begin_substep", "zinv", "xphys", "update_dt", "zfwd", "hvhg", "helmholtz", "assemble")
 KMM_GRID_SINE = 0
 KMM_GRID_TANH = 1
 

@@ -208,7 +208,9 @@ int enqueue_substep(Handle &h, int s, cudaStream_t st, cudaEvent_t *ev = nullptr
   if (s == 1)
     if ((rc = rec(KMM_K_DT, [&] { return launch_update_dt(h, s, st); }))) return rc;
   if ((rc = rec(KMM_K_ZFWD, [&] { return launch_zfwd(h, h.MID, h.P, 8, h.rescale, !h.mixed, st); }))) return rc;
-  if ((rc = rec(KMM_K_WAVESPACE, [&] { return launch_wavespace_split(h, s, nullptr, st); }))) return rc;
+  if ((rc = rec(KMM_K_HVHG, [&] { return launch_ws_hvhg(h, s, nullptr, st); }))) return rc;
+  if ((rc = rec(KMM_K_HELMHOLTZ, [&] { return launch_ws_helmholtz(h, s, nullptr, st); }))) return rc;
+  if ((rc = rec(KMM_K_ASSEMBLE, [&] { return launch_ws_assemble(h, s, nullptr, st); }))) return rc;
   return KMM_OK;
 }
 
@@ -465,8 +467,6 @@ int kmm_create(const kmm_config *cfg, kmm_handle **out) {
   if ((rc = dalloc(*h, &h->RK, 3 * h->ns))) return fail(rc);
   if ((rc = dalloc(*h, reinterpret_cast<char **>(&h->P), 8 * h->ns * r2))) return fail(rc);
   if ((rc = dalloc(*h, reinterpret_cast<char **>(&h->MID), 8 * h->nm * r2))) return fail(rc);
-  if ((rc = dalloc(*h, &h->wbuf, 4 * h->ns + 6 * h->ny))) return fail(rc);
-  if ((rc = dalloc(*h, &h->wband, (size_t)(2 * h->bw + 1) * h->ns))) return fail(rc);
   if ((rc = dalloc(*h, &h->dops, (size_t)off.total))) return fail(rc);
   if ((rc = dalloc(*h, &h->gains, (size_t)h->nmodes))) return fail(rc);
   if ((rc = dalloc(*h, &h->vwall, 2 * (size_t)h->nmodes))) return fail(rc);
@@ -516,7 +516,7 @@ int kmm_destroy(kmm_handle *hh) {
   if (h->graph) cudaGraphDestroy(h->graph);
   if (h->stream) cudaStreamSynchronize(h->stream);
   if (h->side) cudaStreamSynchronize(h->side);
-  void *ptrs[] = {h->S, h->RK, h->P, h->MID, h->wbuf, h->wband, h->dops, h->gains, h->vwall, h->zc,
+  void *ptrs[] = {h->S, h->RK, h->P, h->MID, h->dops, h->gains, h->vwall, h->zc,
                   h->ec, h->xr, h->ub, h->dvw, h->w00, h->staging,
                   h->fftpos, h->tw64, h->tw32, h->dsc};
   for (void *p : ptrs)
@@ -656,7 +656,7 @@ int kmm_get_stream(const kmm_handle *hh, void **stream) {
 int kmm_profile_step(kmm_handle *hh, int nsteps, double *ms, int *launches) {
   if (!hh || nsteps <= 0 || !ms || !launches) return KMM_ERR_ARG;
   Handle &h = *reinterpret_cast<Handle *>(hh);
-  const int per_step = 3 * 6;
+  const int per_step = 3 * KMM_NKERNEL;
   const int nmax = per_step * nsteps;
   std::vector<cudaEvent_t> ev(2 * nmax, nullptr);
   std::vector<int> ids(nmax, -1);

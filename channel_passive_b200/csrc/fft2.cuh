@@ -152,4 +152,78 @@ __device__ __forceinline__ void fft4(typename Cpx<R>::T *a, int lda, typename Cp
   __syncthreads();
 }
 
+// The same transform in place: NL lines at a + l*lda with lda >= (N1+1)*N2, launched with NT
+// threads.  Every thread keeps its step-1 (and step-2) work items in registers across a
+// barrier before it overwrites the line, so no second buffer is needed.
+template <int N1, int N2>
+constexpr int ip_lda() {
+  return ((N1 + 1) * N2) | 1;
+}
+
+template <typename R, int N1, int N2, int NL, int NT>
+__device__ __forceinline__ void fft4_ip(typename Cpx<R>::T *a, int lda, const typename Cpx<R>::T *tw, int sign) {
+  using C = typename Cpx<R>::T;
+  constexpr int I1 = (NL * N1 + NT - 1) / NT, I2 = (NL * N2 + NT - 1) / NT;
+  {
+    C v[I1][N2];
+#pragma unroll
+    for (int i = 0; i < I1; ++i) {
+      const int it = threadIdx.x + i * NT;
+      if (I1 * NT == NL * N1 || it < NL * N1) {
+        const int l = it / N1, n1 = it - l * N1;
+        const C *x = a + l * lda;
+#pragma unroll
+        for (int n2 = 0; n2 < N2; ++n2) v[i][n2] = x[n1 + N1 * n2];
+        reg_dft<C, N2>(v[i], sign);
+        if (n1 > 0) {
+#pragma unroll
+          for (int k2 = 1; k2 < N2; ++k2) {
+            C w = tw[n1 * k2];
+            if (sign > 0) w.y = -w.y;
+            v[i][k2] = cmul(v[i][k2], w);
+          }
+        }
+      }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int i = 0; i < I1; ++i) {
+      const int it = threadIdx.x + i * NT;
+      if (I1 * NT == NL * N1 || it < NL * N1) {
+        const int l = it / N1, n1 = it - l * N1;
+        C *y = a + l * lda;
+#pragma unroll
+        for (int k2 = 0; k2 < N2; ++k2) y[n1 + (N1 + 1) * k2] = v[i][k2];
+      }
+    }
+    __syncthreads();
+  }
+  {
+    C v[I2][N1];
+#pragma unroll
+    for (int i = 0; i < I2; ++i) {
+      const int it = threadIdx.x + i * NT;
+      if (I2 * NT == NL * N2 || it < NL * N2) {
+        const int l = it / N2, k2 = it - l * N2;
+        const C *y = a + l * lda;
+#pragma unroll
+        for (int n1 = 0; n1 < N1; ++n1) v[i][n1] = y[n1 + (N1 + 1) * k2];
+        reg_dft<C, N1>(v[i], sign);
+      }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int i = 0; i < I2; ++i) {
+      const int it = threadIdx.x + i * NT;
+      if (I2 * NT == NL * N2 || it < NL * N2) {
+        const int l = it / N2, k2 = it - l * N2;
+        C *X = a + l * lda;
+#pragma unroll
+        for (int k1 = 0; k1 < N1; ++k1) X[k2 + N2 * k1] = v[i][k1];
+      }
+    }
+    __syncthreads();
+  }
+}
+
 }  // namespace kmm

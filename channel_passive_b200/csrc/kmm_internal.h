@@ -82,8 +82,6 @@ struct Handle {
   cudaStream_t stream = nullptr;
   double2 *S = nullptr, *RK = nullptr;
   void *P = nullptr, *MID = nullptr;       // R2 arrays
-  double2 *wbuf = nullptr;                 // wavespace scratch lines [2][ny][nmodes]
-  double *wband = nullptr;                 // wavespace scratch bands [2bw+1][ny][nmodes]
   double *dops = nullptr;                  // D0, D1, D2, D0_LU bands, integ, dyr, wlo, whi
   float *gains = nullptr;                  // control gains per mode
   double2 *vwall = nullptr;                // [2][nmodes] control wall velocities
@@ -115,7 +113,7 @@ struct OpsOffsets {
 };
 OpsOffsets ops_offsets(int bw, int ny);
 
-// Kernel launchers (transforms.cu / wavespace.cu).
+// Kernel launchers (transforms.cu, labs_kernels.cu).
 cudaError_t launch_zinv(Handle &h, const double2 *src_planes, void *mid, int nfield,
                         cudaStream_t st);
 cudaError_t launch_xphys(Handle &h, void *mid, int substep, cudaStream_t st);
@@ -123,8 +121,6 @@ cudaError_t launch_zfwd(Handle &h, const void *mid, void *dst_planes, int nfield
                         bool dst_fp64, cudaStream_t st);
 cudaError_t launch_update_dt(Handle &h, int substep, cudaStream_t st);
 cudaError_t launch_begin_substep(Handle &h, int substep, cudaStream_t st);
-cudaError_t launch_wavespace(Handle &h, int substep, const double *dt_override,
-                             cudaStream_t st);
 cudaError_t launch_init_stores(Handle &h, cudaStream_t st);
 cudaError_t launch_ref_to_planes(const double2 *src, double2 *dst, int nfield, int64_t nmodes,
                                  int ny, cudaStream_t st);
@@ -145,10 +141,14 @@ cudaError_t launch_zinv2(Handle &h, const double2 *src_planes, void *mid, int nf
 cudaError_t launch_xphys2(Handle &h, void *mid, int substep, cudaStream_t st);
 cudaError_t launch_zfwd2(Handle &h, const void *mid, void *dst_planes, int nfield, double scale,
                          bool dst_fp64, cudaStream_t st);
-cudaError_t launch_control_probe(Handle &h, cudaStream_t st);
 // Per-mode solves of one substep (wavespace_split.cu): hvhg, Helmholtz and assembly kernels on
 // st, the mean lines on h.side (joined back to st before return).
 cudaError_t launch_wavespace_split(Handle &h, int substep, const double *dt_override, cudaStream_t st);
+// The three parts of launch_wavespace_split (control probe + mean fork + hvhg; Helmholtz;
+// assembly + mean join), for per-kernel timing.
+cudaError_t launch_ws_hvhg(Handle &h, int substep, const double *dt_override, cudaStream_t st);
+cudaError_t launch_ws_helmholtz(Handle &h, int substep, const double *dt_override, cudaStream_t st);
+cudaError_t launch_ws_assemble(Handle &h, int substep, const double *dt_override, cudaStream_t st);
 // Doubles of U factor storage per solver role.
 int64_t split_ub_role(const Handle &h);
 

@@ -127,16 +127,24 @@ __device__ __forceinline__ void fwd_fixed(const Tabs<BW> &tb, int n, In in, Out 
     const double *L = tb.l0 + (r - 1) * (W + 1);
     const double rp = L[0];
     double2 z[NC];
+    // L(r, r-e) vanishes for e > BW above the last BW rows
+    auto chain = [&]<int E>() {
+#pragma unroll
+      for (int c = 0; c < NC; ++c) {
+        double2 acc = b[c];
+#pragma unroll
+        for (int e = 1; e <= E; ++e) {
+          const double l = L[e];
+          acc.x -= l * w[c][W - e].x;
+          acc.y -= l * w[c][W - e].y;
+        }
+        z[c] = z2(acc.x * rp, acc.y * rp);
+      }
+    };
+    if (r <= n - BW) chain.template operator()<BW>();
+    else chain.template operator()<W>();
 #pragma unroll
     for (int c = 0; c < NC; ++c) {
-      double2 acc = b[c];
-#pragma unroll
-      for (int e = 1; e <= W; ++e) {
-        const double l = L[e];
-        acc.x -= l * w[c][W - e].x;
-        acc.y -= l * w[c][W - e].y;
-      }
-      z[c] = z2(acc.x * rp, acc.y * rp);
 #pragma unroll
       for (int k = 0; k < W - 1; ++k) w[c][k] = w[c][k + 1];
       w[c][W - 1] = z[c];
@@ -170,29 +178,34 @@ __device__ __forceinline__ void bwd_emit(int n, UF ufn, Zin zin, Emit emit, Pf p
 #pragma unroll
       for (int c = 0; c < NRr; ++c) wr[c][j] = wr[c][j - 1];
     }
-    double u[2 * BW];
-#pragma unroll
-    for (int e = 1; e <= 2 * BW; ++e) u[e - 1] = ufn(r, e);
     double2 zc[NCc];
     double zr[NRr];
     zin(r, zc, zr);
+    // U(r, r+e) vanishes for e > BW below the first BW rows
+    auto chain = [&]<int E>() {
+      double u[E];
 #pragma unroll
-    for (int c = 0; c < NC; ++c) {
-      double2 acc = zc[c];
+      for (int e = 1; e <= E; ++e) u[e - 1] = ufn(r, e);
 #pragma unroll
-      for (int e = 1; e <= 2 * BW; ++e) {
-        acc.x -= u[e - 1] * wc[c][e].x;
-        acc.y -= u[e - 1] * wc[c][e].y;
+      for (int c = 0; c < NC; ++c) {
+        double2 acc = zc[c];
+#pragma unroll
+        for (int e = 1; e <= E; ++e) {
+          acc.x -= u[e - 1] * wc[c][e].x;
+          acc.y -= u[e - 1] * wc[c][e].y;
+        }
+        wc[c][0] = acc;
       }
-      wc[c][0] = acc;
-    }
 #pragma unroll
-    for (int c = 0; c < NR; ++c) {
-      double acc = zr[c];
+      for (int c = 0; c < NR; ++c) {
+        double acc = zr[c];
 #pragma unroll
-      for (int e = 1; e <= 2 * BW; ++e) acc -= u[e - 1] * wr[c][e];
-      wr[c][0] = acc;
-    }
+        for (int e = 1; e <= E; ++e) acc -= u[e - 1] * wr[c][e];
+        wr[c][0] = acc;
+      }
+    };
+    if (r > BW) chain.template operator()<BW>();
+    else chain.template operator()<2 * BW>();
     if (r <= n - 2 * BW) emit(r + BW, r, wc, wr);
     if (r == n - 2 * BW)
       for (int q = n - BW + 1; q <= n; ++q) emit(q, r, wc, wr);
@@ -202,7 +215,8 @@ __device__ __forceinline__ void bwd_emit(int n, UF ufn, Zin zin, Emit emit, Pf p
 }
 
 // Profile Crout LU of a per-mode matrix fused with the forward substitution of NC complex and
-// NR real chains, ascending.  rowA(r, a) fills a[e + 2BW] = A(r, r+e); in(r, bc, br) gives the
+// NR real chains, ascending.  rowA(r, a, centre) fills a[e + 2BW] = A(r, r+e) (for centre rows
+// only |e| <= BW, the entries they use); in(r, bc, br) gives the
 // right-hand sides of row r; out(r, zc, zr) receives the forward results; U goes to ust (for
 // the backward sweep).  Rows 2BW+1..n-BW only touch U(p, p+e) with e <= BW of the last BW rows,
 // which stay in a register window; the first 2BW and last BW rows read U back from ust.
@@ -228,10 +242,10 @@ __device__ __forceinline__ void lu_fwd(int n, RowA rowA, In in, Out out, UBand<B
   for (int r = 1; r <= n; ++r) {
     if (r + kPrefetchRows <= n) pf(r + kPrefetchRows);
     double a[4 * BW + 1];
-    rowA(r, a);
     double L[W + 1];  // L[d] = L(r, r-d)
     double Ur[W];     // U(r, r+e), e = 1..W
     if (r > 2 * BW && r <= n - BW) {
+      rowA(r, a, true);
       // centre row: lo = r - BW, hi = r + BW; U of rows r-BW..r-1 from the register window
 #pragma unroll
       for (int d = W; d > BW; --d) L[d] = 0.0;
@@ -257,6 +271,7 @@ __device__ __forceinline__ void lu_fwd(int n, RowA rowA, In in, Out out, UBand<B
       }
       L[0] = rp;  // from here on L[0] holds the reciprocal pivot
     } else {
+      rowA(r, a, false);
       const int lo = row_lo<BW>(r, n), hi = row_hi<BW>(r, n);
 #pragma unroll
       for (int d = W; d >= 0; --d) {
@@ -298,25 +313,36 @@ __device__ __forceinline__ void lu_fwd(int n, RowA rowA, In in, Out out, UBand<B
     in(r, bc, br);
     double2 zc[NCc];
     double zr[NRr];
+    // L(r, r-d) vanishes for d > BW above the last BW rows
+    auto chain = [&]<int D>() {
+#pragma unroll
+      for (int c = 0; c < NC; ++c) {
+        double2 acc = bc[c];
+#pragma unroll
+        for (int d = 1; d <= D; ++d) {
+          acc.x -= L[d] * wc[c][W - d].x;
+          acc.y -= L[d] * wc[c][W - d].y;
+        }
+        zc[c] = z2(acc.x * rp, acc.y * rp);
+      }
+#pragma unroll
+      for (int c = 0; c < NR; ++c) {
+        double acc = br[c];
+#pragma unroll
+        for (int d = 1; d <= D; ++d) acc -= L[d] * wr[c][W - d];
+        zr[c] = acc * rp;
+      }
+    };
+    if (r <= n - BW) chain.template operator()<BW>();
+    else chain.template operator()<W>();
 #pragma unroll
     for (int c = 0; c < NC; ++c) {
-      double2 acc = bc[c];
-#pragma unroll
-      for (int d = 1; d <= W; ++d) {
-        acc.x -= L[d] * wc[c][W - d].x;
-        acc.y -= L[d] * wc[c][W - d].y;
-      }
-      zc[c] = z2(acc.x * rp, acc.y * rp);
 #pragma unroll
       for (int k = 0; k < W - 1; ++k) wc[c][k] = wc[c][k + 1];
       wc[c][W - 1] = zc[c];
     }
 #pragma unroll
     for (int c = 0; c < NR; ++c) {
-      double acc = br[c];
-#pragma unroll
-      for (int d = 1; d <= W; ++d) acc -= L[d] * wr[c][W - d];
-      zr[c] = acc * rp;
 #pragma unroll
       for (int k = 0; k < W - 1; ++k) wr[c][k] = wr[c][k + 1];
       wr[c][W - 1] = zr[c];

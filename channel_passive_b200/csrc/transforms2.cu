@@ -1,10 +1,11 @@
 // transforms2.cu - the substep's transforms with compile-time four-step FFTs (fft2.cuh).
 //
 // Same contracts as transforms.cu (k_zinv / k_xphys / k_zfwd: y_to_x, dft_x_realspace and
-// x_to_y with rescale_data folded in) for the line lengths N = N1 * N2 listed in fft4_shape;
+// x_to_y with rescale_data folded in) for the line lengths N = N1 * N2 listed in with_shape;
 // the launchers fall back to the generic kernels of transforms.cu for other lengths.  Lines
-// are line-major in shared memory with an odd leading dimension, natural order in and out, so
-// the 3/2 padding and truncation read and write plain positions k and N - k.
+// are line-major in shared memory with the odd leading dimension (N1+1)*N2 | 1 and are
+// transformed in place (fft4_ip), natural order in and out, so the 3/2 padding and truncation
+// read and write plain positions k and N - k.
 #include <cuda_runtime.h>
 
 #include "fft2.cuh"
@@ -14,8 +15,6 @@ namespace kmm {
 
 namespace {
 
-constexpr int kT2 = 256;
-
 template <typename C> __device__ __forceinline__ C ld_as(const double2 *p) {
   const double2 v = *p;
   return cmake<C>(v.x, v.y);
@@ -24,59 +23,54 @@ template <typename R> __device__ __forceinline__ const typename Cpx<R>::T *tw_of
 template <> __device__ __forceinline__ const double2 *tw_of<double>(const FftPlan &pl) { return pl.tw64; }
 template <> __device__ __forceinline__ const float2 *tw_of<float>(const FftPlan &pl) { return pl.tw32; }
 
-constexpr int lda_of(int N) { return N | 1; }
-constexpr int ldb_of(int N1, int N2) { return ((N1 + 1) * N2) | 1; }
-
-// y_to_x: grid (ceil(nxh/KB), ny, nfield)
-template <typename R, int N1, int N2, int KB>
-__global__ void __launch_bounds__(kT2) k_zinv2(const double2 *__restrict__ src, typename Cpx<R>::T *__restrict__ dst,
-                                               FftPlan pl, int nz, int nxh, int64_t ns, int64_t nm) {
+// y_to_x: grid (ceil(nxh/KB), ny, nfield), NT threads
+template <typename R, int N1, int N2, int KB, int NT>
+__global__ void __launch_bounds__(NT) k_zinv2(const double2 *__restrict__ src, typename Cpx<R>::T *__restrict__ dst,
+                                              FftPlan pl, int nz, int nxh, int64_t ns, int64_t nm) {
   using C = typename Cpx<R>::T;
-  constexpr int N = N1 * N2, LDA = lda_of(N), LDB = ldb_of(N1, N2);
+  constexpr int N = N1 * N2, LD = ip_lda<N1, N2>();
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C *a = reinterpret_cast<C *>(smem_raw);
-  C *b = a + KB * LDA;
   const int nh = nz / 2;
   const int kx0 = blockIdx.x * KB, y = blockIdx.y, f = blockIdx.z;
   const double2 *sp = src + f * ns + (int64_t)y * nz * nxh;
-  for (int w = threadIdx.x; w < N * KB; w += blockDim.x) {
+  for (int w = threadIdx.x; w < N * KB; w += NT) {
     const int l = w % KB, p = w / KB;
     int kzi = -1;
     if (p < nh) kzi = p;
     else if (p > 2 * nh) kzi = p - nh;
     C v = cmake<C>(0.0, 0.0);
     if (kzi >= 0 && kx0 + l < nxh) v = ld_as<C>(sp + (int64_t)kzi * nxh + kx0 + l);
-    a[l * LDA + p] = v;
+    a[l * LD + p] = v;
   }
   __syncthreads();
-  fft4<R, N1, N2>(a, LDA, b, LDB, KB, tw_of<R>(pl), +1);
+  fft4_ip<R, N1, N2, KB, NT>(a, LD, tw_of<R>(pl), +1);
   C *dp = dst + f * nm + (int64_t)y * N * nxh;
-  for (int w = threadIdx.x; w < N * KB; w += blockDim.x) {
+  for (int w = threadIdx.x; w < N * KB; w += NT) {
     const int l = w % KB, z = w / KB;
-    if (kx0 + l < nxh) dp[(int64_t)z * nxh + kx0 + l] = a[l * LDA + z];
+    if (kx0 + l < nxh) dp[(int64_t)z * nxh + kx0 + l] = a[l * LD + z];
   }
 }
 
-// x_to_y: grid (ceil(nxh/KB), ny, nfield)
-template <typename R, int N1, int N2, int KB, typename D>
-__global__ void __launch_bounds__(kT2) k_zfwd2(const typename Cpx<R>::T *__restrict__ src, D *__restrict__ dst,
-                                               FftPlan pl, int nz, int nxh, int64_t ns, int64_t nm, double scale) {
+// x_to_y: grid (ceil(nxh/KB), ny, nfield), NT threads
+template <typename R, int N1, int N2, int KB, int NT, typename D>
+__global__ void __launch_bounds__(NT) k_zfwd2(const typename Cpx<R>::T *__restrict__ src, D *__restrict__ dst,
+                                              FftPlan pl, int nz, int nxh, int64_t ns, int64_t nm, double scale) {
   using C = typename Cpx<R>::T;
-  constexpr int N = N1 * N2, LDA = lda_of(N), LDB = ldb_of(N1, N2);
+  constexpr int N = N1 * N2, LD = ip_lda<N1, N2>();
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C *a = reinterpret_cast<C *>(smem_raw);
-  C *b = a + KB * LDA;
   const int nh = nz / 2;
   const int kx0 = blockIdx.x * KB, y = blockIdx.y, f = blockIdx.z;
   const C *sp = src + f * nm + (int64_t)y * N * nxh;
-  for (int w = threadIdx.x; w < N * KB; w += blockDim.x) {
+  for (int w = threadIdx.x; w < N * KB; w += NT) {
     const int l = w % KB, z = w / KB;
-    a[l * LDA + z] = (kx0 + l < nxh) ? sp[(int64_t)z * nxh + kx0 + l] : cmake<C>(0.0, 0.0);
+    a[l * LD + z] = (kx0 + l < nxh) ? sp[(int64_t)z * nxh + kx0 + l] : cmake<C>(0.0, 0.0);
   }
   __syncthreads();
-  fft4<R, N1, N2>(a, LDA, b, LDB, KB, tw_of<R>(pl), -1);
+  fft4_ip<R, N1, N2, KB, NT>(a, LD, tw_of<R>(pl), -1);
   D *dp = dst + f * ns + (int64_t)y * nz * nxh;
-  for (int w = threadIdx.x; w < nz * KB; w += blockDim.x) {
+  for (int w = threadIdx.x; w < nz * KB; w += NT) {
     const int l = w % KB, kzi = w / KB;
     if (kx0 + l >= nxh) continue;
     const int k = (kzi < nh) ? kzi : (kzi == nh ? -1 : kzi + nh);
@@ -85,7 +79,7 @@ __global__ void __launch_bounds__(kT2) k_zfwd2(const typename Cpx<R>::T *__restr
       out.x = 0;
       out.y = 0;
     } else {
-      const C v = a[l * LDA + k];
+      const C v = a[l * LD + k];
       out.x = (decltype(out.x))(scale * (double)v.x);
       out.y = (decltype(out.y))(scale * (double)v.y);
     }
@@ -102,31 +96,30 @@ struct X2Args {
   DevScalars *dsc;
 };
 
-// dft_x_realspace: grid (ceil(nz32/ZB), ny); MID slots 0..3 = u, v, w, theta in,
+// dft_x_realspace: grid (ceil(nz32/ZB), ny), NT threads; MID slots 0..3 = u, v, w, theta in,
 // slots 0..7 = f1, f2, f3, f4, f5, f7, f8, f9 out (a block owns its rows).
-template <typename R, int N1, int N2, int ZB>
-__global__ void __launch_bounds__(kT2) k_xphys2(typename Cpx<R>::T *__restrict__ mid, FftPlan pl, X2Args a_) {
+template <typename R, int N1, int N2, int ZB, int NT>
+__global__ void __launch_bounds__(NT) k_xphys2(typename Cpx<R>::T *__restrict__ mid, FftPlan pl, X2Args a_) {
   using C = typename Cpx<R>::T;
-  constexpr int N = N1 * N2, LDA = lda_of(N), LDB = ldb_of(N1, N2);
+  constexpr int N = N1 * N2, LD = ip_lda<N1, N2>();
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C *a = reinterpret_cast<C *>(smem_raw);  // 4*ZB lines: (u,v) ZB, (w,theta) ZB, then f57, f89
-  C *b = a + 4 * ZB * LDA;
   const int nxh = a_.nxh;
   const int z0 = blockIdx.x * ZB, y = blockIdx.y;
   const int64_t row0 = ((int64_t)y * a_.nz32 + z0) * nxh;
-  for (int w = threadIdx.x; w < 2 * ZB * N; w += blockDim.x) {
+  for (int w = threadIdx.x; w < 2 * ZB * N; w += NT) {
     const int L = w / N, p = w - L * N;
-    a[L * LDA + p] = cmake<C>(0.0, 0.0);
+    a[L * LD + p] = cmake<C>(0.0, 0.0);
   }
   __syncthreads();
   // Z_k = X1_k + i X2_k and its Hermitian mirror at N - k; DC imaginary parts dropped (c2r)
-  for (int w = threadIdx.x; w < 2 * ZB * nxh; w += blockDim.x) {
+  for (int w = threadIdx.x; w < 2 * ZB * nxh; w += NT) {
     const int k = w % nxh, t = w / nxh, l = t % ZB, bsel = t / ZB;
     if (z0 + l >= a_.nz32) continue;
     const int64_t off = row0 + (int64_t)l * nxh + k;
     const int fa = bsel ? 2 : 0, fb = bsel ? 3 : 1;
     const C x1 = mid[fa * a_.nm + off], x2 = mid[fb * a_.nm + off];
-    C *line = a + (bsel * ZB + l) * LDA;
+    C *line = a + (bsel * ZB + l) * LD;
     if (k == 0) {
       line[0] = cmake<C>(x1.x, x2.x);
     } else {
@@ -138,13 +131,13 @@ __global__ void __launch_bounds__(kT2) k_xphys2(typename Cpx<R>::T *__restrict__
     }
   }
   __syncthreads();
-  fft4<R, N1, N2>(a, LDA, b, LDB, 2 * ZB, tw_of<R>(pl), +1);
+  fft4_ip<R, N1, N2, 2 * ZB, NT>(a, LD, tw_of<R>(pl), +1);
   const double dyr = a_.dyr[y];
   double vmax = 0.0;
   int bad = 0;
-  for (int w = threadIdx.x; w < ZB * N; w += blockDim.x) {
+  for (int w = threadIdx.x; w < ZB * N; w += NT) {
     const int l = w / N, p = w - l * N;
-    const C uv = a[l * LDA + p], wt = a[(ZB + l) * LDA + p];
+    const C uv = a[l * LD + p], wt = a[(ZB + l) * LD + p];
     const R u = uv.x, v = uv.y, ww = wt.x, t = wt.y;
     const R bv2 = v * v;
     C f12, f34, f57, f89;
@@ -152,10 +145,10 @@ __global__ void __launch_bounds__(kT2) k_xphys2(typename Cpx<R>::T *__restrict__
     f34.x = ww * ww - bv2; f34.y = v * ww;
     f57.x = u * ww; f57.y = u * t;
     f89.x = v * t; f89.y = ww * t;
-    a[l * LDA + p] = f12;
-    a[(ZB + l) * LDA + p] = f34;
-    a[(2 * ZB + l) * LDA + p] = f57;
-    a[(3 * ZB + l) * LDA + p] = f89;
+    a[l * LD + p] = f12;
+    a[(ZB + l) * LD + p] = f34;
+    a[(2 * ZB + l) * LD + p] = f57;
+    a[(3 * ZB + l) * LD + p] = f89;
     if (a_.substep == 1 && z0 + l < a_.nz32) {
       const double vel = (fabs((double)u) * a_.dxr) + (fabs((double)v) * dyr) + (fabs((double)ww) * a_.dzr);
       if (!isfinite(vel)) bad = 1;
@@ -163,11 +156,11 @@ __global__ void __launch_bounds__(kT2) k_xphys2(typename Cpx<R>::T *__restrict__
     }
   }
   __syncthreads();
-  fft4<R, N1, N2>(a, LDA, b, LDB, 4 * ZB, tw_of<R>(pl), -1);
-  for (int w = threadIdx.x; w < 4 * ZB * nxh; w += blockDim.x) {
+  fft4_ip<R, N1, N2, 4 * ZB, NT>(a, LD, tw_of<R>(pl), -1);
+  for (int w = threadIdx.x; w < 4 * ZB * nxh; w += NT) {
     const int k = w % nxh, t = w / nxh, l = t % ZB, bsel = t / ZB;
     if (z0 + l >= a_.nz32) continue;
-    const C *line = a + (bsel * ZB + l) * LDA;
+    const C *line = a + (bsel * ZB + l) * LD;
     const C zk = line[k], zm = line[k == 0 ? 0 : N - k];
     C A, B;
     A.x = (R)0.5 * (zk.x + zm.x); A.y = (R)0.5 * (zk.y - zm.y);
@@ -177,7 +170,7 @@ __global__ void __launch_bounds__(kT2) k_xphys2(typename Cpx<R>::T *__restrict__
     mid[(2 * bsel + 1) * a_.nm + off] = B;
   }
   if (a_.substep == 1) {
-    __shared__ double red[kT2 / 32];
+    __shared__ double red[NT / 32];
     __shared__ int redbad;
     if (threadIdx.x == 0) redbad = 0;
     __syncthreads();
@@ -187,7 +180,7 @@ __global__ void __launch_bounds__(kT2) k_xphys2(typename Cpx<R>::T *__restrict__
     __syncthreads();
     if (threadIdx.x == 0) {
       double m = 0.0;
-      for (int i = 0; i < (int)(blockDim.x >> 5); ++i) m = fmax(m, red[i]);
+      for (int i = 0; i < NT / 32; ++i) m = fmax(m, red[i]);
       atomicMax(&a_.dsc->velmax_bits, (unsigned long long)__double_as_longlong(m));
       if (redbad) atomicOr(&a_.dsc->nonfinite, 1);
     }
@@ -218,12 +211,24 @@ template <typename K> void set_smem(K kern, int optin) {
   cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, optin - (int)fa.sharedSizeBytes);
 }
 
-template <typename R> constexpr int zkb() { return sizeof(R) == 8 ? 8 : 16; }
+// Lines per block and threads (KB, KT: z transforms; ZB, ZT: x pass), tuned at N = 288 on B200
+// for occupancy: the in-place four-step needs (N1+1)*N2 | 1 complex values of shared memory per
+// line, so these choices keep 39 KB or less per block.
+template <typename R> struct TCfg;
+template <> struct TCfg<float> {
+  static constexpr int KB = 16, KT = 128, ZB = 2, ZT = 128;
+};
+template <> struct TCfg<double> {
+  static constexpr int KB = 4, KT = 128, ZB = 1, ZT = 64;
+};
 
 template <typename R, int N1, int N2>
-size_t xphys_zb_bytes(int zb) {
-  using C = typename Cpx<R>::T;
-  return sizeof(C) * (size_t)4 * zb * (lda_of(N1 * N2) + ldb_of(N1, N2));
+constexpr size_t z_smem() {
+  return sizeof(typename Cpx<R>::T) * (size_t)TCfg<R>::KB * ip_lda<N1, N2>();
+}
+template <typename R, int N1, int N2>
+constexpr size_t x_smem() {
+  return sizeof(typename Cpx<R>::T) * (size_t)4 * TCfg<R>::ZB * ip_lda<N1, N2>();
 }
 
 }  // namespace
@@ -254,18 +259,15 @@ cudaError_t prepare_transforms2() {
   if (e != cudaSuccess) return e;
   for (int N : {12, 24, 36, 48, 72, 96, 144, 192, 288, 384, 576}) {
     with_shape(N, [&]<int N1, int N2>() {
-      set_smem(k_zinv2<double, N1, N2, 8>, optin);
-      set_smem(k_zinv2<float, N1, N2, 16>, optin);
-      set_smem(k_zfwd2<double, N1, N2, 8, double2>, optin);
-      set_smem(k_zfwd2<float, N1, N2, 16, float2>, optin);
-      set_smem(k_zfwd2<float, N1, N2, 16, double2>, optin);
-      set_smem(k_xphys2<double, N1, N2, 4>, optin);
-      set_smem(k_xphys2<double, N1, N2, 2>, optin);
-      set_smem(k_xphys2<double, N1, N2, 1>, optin);
-      set_smem(k_xphys2<float, N1, N2, 8>, optin);
-      set_smem(k_xphys2<float, N1, N2, 4>, optin);
-      set_smem(k_xphys2<float, N1, N2, 2>, optin);
-      set_smem(k_xphys2<float, N1, N2, 1>, optin);
+      using F = TCfg<float>;
+      using D = TCfg<double>;
+      set_smem(k_zinv2<double, N1, N2, D::KB, D::KT>, optin);
+      set_smem(k_zinv2<float, N1, N2, F::KB, F::KT>, optin);
+      set_smem(k_zfwd2<double, N1, N2, D::KB, D::KT, double2>, optin);
+      set_smem(k_zfwd2<float, N1, N2, F::KB, F::KT, float2>, optin);
+      set_smem(k_zfwd2<float, N1, N2, F::KB, F::KT, double2>, optin);
+      set_smem(k_xphys2<double, N1, N2, D::ZB, D::ZT>, optin);
+      set_smem(k_xphys2<float, N1, N2, F::ZB, F::ZT>, optin);
     });
   }
   return cudaSuccess;
@@ -274,14 +276,13 @@ cudaError_t prepare_transforms2() {
 // Returns cudaErrorNotSupported when the length has no four-step shape (caller falls back).
 cudaError_t launch_zinv2(Handle &h, const double2 *src, void *mid, int nfield, cudaStream_t st) {
   cudaError_t err = cudaErrorNotSupported;
-  const int N = h.nz32;
   auto go = [&]<typename R>() {
-    with_shape(N, [&]<int N1, int N2>() {
+    with_shape(h.nz32, [&]<int N1, int N2>() {
       using C = typename Cpx<R>::T;
-      constexpr int KB = zkb<R>();
-      const size_t smem = sizeof(C) * (size_t)KB * (lda_of(N1 * N2) + ldb_of(N1, N2));
-      dim3 grid((unsigned)((h.nxh + KB - 1) / KB), (unsigned)h.ny, (unsigned)nfield);
-      k_zinv2<R, N1, N2, KB><<<grid, kT2, smem, st>>>(src, reinterpret_cast<C *>(mid), h.pz, h.nz, h.nxh, h.ns, h.nm);
+      using T = TCfg<R>;
+      dim3 grid((unsigned)((h.nxh + T::KB - 1) / T::KB), (unsigned)h.ny, (unsigned)nfield);
+      k_zinv2<R, N1, N2, T::KB, T::KT><<<grid, T::KT, z_smem<R, N1, N2>(), st>>>(
+          src, reinterpret_cast<C *>(mid), h.pz, h.nz, h.nxh, h.ns, h.nm);
       err = cudaGetLastError();
     });
   };
@@ -293,15 +294,13 @@ cudaError_t launch_zinv2(Handle &h, const double2 *src, void *mid, int nfield, c
 cudaError_t launch_zfwd2(Handle &h, const void *mid, void *dst, int nfield, double scale, bool dst_fp64,
                          cudaStream_t st) {
   cudaError_t err = cudaErrorNotSupported;
-  const int N = h.nz32;
   auto go = [&]<typename R, typename D>() {
-    with_shape(N, [&]<int N1, int N2>() {
+    with_shape(h.nz32, [&]<int N1, int N2>() {
       using C = typename Cpx<R>::T;
-      constexpr int KB = zkb<R>();
-      const size_t smem = sizeof(C) * (size_t)KB * (lda_of(N1 * N2) + ldb_of(N1, N2));
-      dim3 grid((unsigned)((h.nxh + KB - 1) / KB), (unsigned)h.ny, (unsigned)nfield);
-      k_zfwd2<R, N1, N2, KB, D><<<grid, kT2, smem, st>>>(reinterpret_cast<const C *>(mid), reinterpret_cast<D *>(dst),
-                                                         h.pz, h.nz, h.nxh, h.ns, h.nm, scale);
+      using T = TCfg<R>;
+      dim3 grid((unsigned)((h.nxh + T::KB - 1) / T::KB), (unsigned)h.ny, (unsigned)nfield);
+      k_zfwd2<R, N1, N2, T::KB, T::KT, D><<<grid, T::KT, z_smem<R, N1, N2>(), st>>>(
+          reinterpret_cast<const C *>(mid), reinterpret_cast<D *>(dst), h.pz, h.nz, h.nxh, h.ns, h.nm, scale);
       err = cudaGetLastError();
     });
   };
@@ -316,7 +315,6 @@ cudaError_t launch_zfwd2(Handle &h, const void *mid, void *dst, int nfield, doub
 
 cudaError_t launch_xphys2(Handle &h, void *mid, int substep, cudaStream_t st) {
   cudaError_t err = cudaErrorNotSupported;
-  const int N = h.nx32;
   X2Args a;
   a.ny = h.ny;
   a.nz32 = h.nz32;
@@ -328,19 +326,12 @@ cudaError_t launch_xphys2(Handle &h, void *mid, int substep, cudaStream_t st) {
   a.substep = substep;
   a.dsc = h.dsc;
   auto go = [&]<typename R>() {
-    with_shape(N, [&]<int N1, int N2>() {
+    with_shape(h.nx32, [&]<int N1, int N2>() {
       using C = typename Cpx<R>::T;
-      const size_t lim = 200 * 1024;
-      auto launch = [&]<int ZB>() {
-        const size_t smem = xphys_zb_bytes<R, N1, N2>(ZB);
-        dim3 grid((unsigned)((h.nz32 + ZB - 1) / ZB), (unsigned)h.ny);
-        k_xphys2<R, N1, N2, ZB><<<grid, kT2, smem, st>>>(reinterpret_cast<C *>(mid), h.px, a);
-        err = cudaGetLastError();
-      };
-      if (sizeof(R) == 4 && xphys_zb_bytes<R, N1, N2>(8) <= lim) launch.template operator()<8>();
-      else if (xphys_zb_bytes<R, N1, N2>(4) <= lim) launch.template operator()<4>();
-      else if (xphys_zb_bytes<R, N1, N2>(2) <= lim) launch.template operator()<2>();
-      else launch.template operator()<1>();
+      using T = TCfg<R>;
+      dim3 grid((unsigned)((h.nz32 + T::ZB - 1) / T::ZB), (unsigned)h.ny);
+      k_xphys2<R, N1, N2, T::ZB, T::ZT><<<grid, T::ZT, x_smem<R, N1, N2>(), st>>>(reinterpret_cast<C *>(mid), h.px, a);
+      err = cudaGetLastError();
     });
   };
   if (h.mixed) go.template operator()<float>();

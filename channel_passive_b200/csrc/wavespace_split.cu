@@ -11,6 +11,7 @@
 //   role 1  f8                                      -> HT  = -(i kx f7 + i kz f9 + D1 c(f8))
 //   role 2  f2                                      -> G2  = a1 - i kz D1 c(f2),  V2 = i kx D2 c(f2)
 //   role 3  f4                                      -> G3  = i kx D1 c(f4),       V3 = i kz D2 c(f4)
+//           and, with opposition control, the probes v(+-y_d) of the starting v
 //   so hg = G2 + G3, hv = HV0 + (V2 + V3), ht = HT.  At substep 1 roles 0-2 also solve D0 for the
 //   store they feed (RK_STORE 2, 3, 1) and emit D2 of it (DP, DT, DG; solve_g.f90:84-111).
 // k_helmholtz, one profile LU per role (solve_t.f90:28-201, solve_g.f90, solve_v_f.f90:95-298):
@@ -59,7 +60,9 @@ struct SplitArgs {
   int64_t ub_role;   // doubles per role
   double2 *dv;       // [3][nm] dv_p(1), dv_p(n), (dv_h(1), dv_h(n))
   const double *tabs;   // t0, t1, t2, l0, u0
-  const double2 *vwall;
+  double2 *vwall;          // [2][nm] control probes v(y_d), v(-y_d) of each mode
+  const double *wlo, *whi;  // control weights: v(y_d) = w . v
+  const float *gains;       // control gain per mode
   double control_amp;
   double nu, pr, lmfxr, lmfzr;
   DevScalars *dsc;
@@ -98,10 +101,17 @@ __device__ __forceinline__ ModeK mode_k(const SplitArgs &a, int64_t m) {
   return k;
 }
 
-// A = ca D0 - cb D2 with the Dirichlet first / last rows, as an offset row.
+// A = ca D0 - cb D2 with the Dirichlet first / last rows, as an offset row (|e| <= BW only
+// for a centre row, which is never a wall row).
 template <int BW>
-__device__ __forceinline__ void helm_row(const Tabs<BW> &tb, int r, int n, double ca, double cb, double *out) {
+__device__ __forceinline__ void helm_row(const Tabs<BW> &tb, int r, int n, double ca, double cb, double *out,
+                                         bool centre) {
   const double *r0 = trow<BW>(tb.t0, r), *r2 = trow<BW>(tb.t2, r);
+  if (centre) {
+#pragma unroll
+    for (int e = -BW; e <= BW; ++e) out[e + 2 * BW] = ca * r0[e] - cb * r2[e];
+    return;
+  }
   if (r == 1 || r == n) {
 #pragma unroll
     for (int e = -2 * BW; e <= 2 * BW; ++e) out[e + 2 * BW] = 0.0;
@@ -114,8 +124,13 @@ __device__ __forceinline__ void helm_row(const Tabs<BW> &tb, int r, int n, doubl
 
 // (D2 - k^2 D0) with the wall rows replaced by D0 (v given there), solve_v_f.f90:95-140.
 template <int BW>
-__device__ __forceinline__ void vrow(const Tabs<BW> &tb, int r, int n, double k2, double *row) {
+__device__ __forceinline__ void vrow(const Tabs<BW> &tb, int r, int n, double k2, double *row, bool centre) {
   const double *r0 = trow<BW>(tb.t0, r), *r2 = trow<BW>(tb.t2, r);
+  if (centre) {
+#pragma unroll
+    for (int e = -BW; e <= BW; ++e) row[e + 2 * BW] = -k2 * r0[e] + r2[e];
+    return;
+  }
   if (r == 1 || r == n) {
 #pragma unroll
     for (int e = -2 * BW; e <= 2 * BW; ++e) row[e + 2 * BW] = 0.0;
@@ -144,6 +159,12 @@ __device__ __forceinline__ void hvhg_role(const SplitArgs &a, const Tabs<BW> &tb
   const DLine Rs{a.RK + store_slot * ns + m, nm};
   auto hl = [&](int i) { return DLine{a.hl + i * ns + m, nm}; };
   auto ufix = [&](int r, int e) { return tb.u0[(r - 1) * 2 * BW + e - 1]; };
+  // Role 3 also probes the wall-normal velocity at the detection planes for opposition
+  // control: v(+-y_d) = w . v over the substep's starting v, with the precomputed weights
+  // w = D0^{-T} B(+-y_d).
+  const bool probe = ROLE == 3 && a.control_amp != 0.0;
+  const DLine Sv{a.S + ns + m, nm};
+  double2 plo = z2(0.0, 0.0), phi = z2(0.0, 0.0);
 
   fwd_fixed<BW, NC>(tb, n,
       [&](int r, double2 *b) {
@@ -156,6 +177,11 @@ __device__ __forceinline__ void hvhg_role(const SplitArgs &a, const Tabs<BW> &tb
           b[0] = prod(1, r);
         } else {
           b[0] = prod(3, r);
+          if (probe) {
+            const double2 v = Sv.ld(r);
+            plo = zadd(plo, zscale(__ldg(a.wlo + r - 1), v));
+            phi = zadd(phi, zscale(__ldg(a.whi + r - 1), v));
+          }
         }
         if constexpr (NC == 2) b[1] = Rs.ld(r);
       },
@@ -167,7 +193,12 @@ __device__ __forceinline__ void hvhg_role(const SplitArgs &a, const Tabs<BW> &tb
         if constexpr (ROLE == 0) { pfp(0, r); pfp(2, r); pfp(4, r); }
         else pfp(ROLE == 1 ? 6 : ROLE == 2 ? 1 : 3, r);
         if constexpr (NC == 2) pf_l1(Rs.p + (int64_t)(r - 1) * nm);
+        if (probe) pf_l1(Sv.p + (int64_t)(r - 1) * nm);
       });
+  if (probe) {
+    a.vwall[m] = plo;
+    a.vwall[nm + m] = phi;
+  }
 
   bwd_emit<BW, NC, 0>(n, ufix,
       [&](int r, double2 *zc, double *) {
@@ -240,6 +271,10 @@ __device__ __forceinline__ void helmholtz_role(const SplitArgs &a, const Tabs<BW
   };
   const UBand<BW> ub = make_uband<BW>(a.ub + ROLE * a.ub_role + m, nm, ns);
   auto uper = [&](int r, int e) { return ub.get(r, e); };
+  auto pfu = [&](int r) {  // the U row a backward step reads
+#pragma unroll
+    for (int e = 1; e <= BW; ++e) pf_l1(ub.p + (int64_t)(e - 1) * ns + (int64_t)(r - 1) * nm);
+  };
   const DLine Zr{a.zl + ROLE * ns + m, nm};
 
   // RK right-hand side (solve_g.f90:84-123): rows 1 and n are the Dirichlet rows (zero)
@@ -276,7 +311,7 @@ __device__ __forceinline__ void helmholtz_role(const SplitArgs &a, const Tabs<BW
       else if constexpr (ROLE == 1) { pfl(hl(H_G2).p, r); pfl(hl(H_G3).p, r); }
       else { pfl(hl(H_HV0).p, r); pfl(hl(H_V2).p, r); pfl(hl(H_V3).p, r); }
     };
-    lu_fwd<BW, 1, 0>(n, [&](int r, double *row) { helm_row<BW>(tb, r, n, dummy, beta, row); },
+    lu_fwd<BW, 1, 0>(n, [&](int r, double *row, bool c) { helm_row<BW>(tb, r, n, dummy, beta, row, c); },
         [&](int r, double2 *bc, double *) {
           bc[0] = rhs(store.ld(r), hsum(r), s == 1 ? d2l.ld(r) : z2(0.0, 0.0), visc, r);
         },
@@ -295,17 +330,37 @@ __device__ __forceinline__ void helmholtz_role(const SplitArgs &a, const Tabs<BW
         },
         [&](int r) {
           pfl(Zr.p, r);
+          pfu(r);
           const int q = r + BW;
-          if (r <= n - 2 * BW) pfh(q);
+          if (r <= n - 2 * BW) {
+            pfh(q);
+            pfl(store.p, q);
+          }
         });
     if constexpr (ROLE != 2) return;
     // (D2 - k^2 D0) v_p = phi_p with v_p = the wall velocity at rows 1 and n
+    // Opposition control, the extension at the wall rows of the v solve (solve_v_f.f90:251-257,
+    // whose commented lines read vold): v at the walls = A * gain * v(+-y_d).  vold is field 10,
+    // v after the physical round trip (dft_x_realspace.f90:123), which has no kz Nyquist mode
+    // and, at kx = 0, only the Hermitian part (v(kz) + conj v(-kz)) / 2.
     double2 vlo = z2(0.0, 0.0), vhi = z2(0.0, 0.0);
     if (a.control_amp != 0.0) {
-      vlo = a.vwall[m];
-      vhi = a.vwall[nm + m];
+      const int kzi = (int)(m / a.nxh), kxi = (int)(m - (int64_t)kzi * a.nxh);
+      if (kzi != a.nz / 2) {
+        vlo = a.vwall[m];
+        vhi = a.vwall[nm + m];
+        if (kxi == 0) {
+          const int64_t mp = (int64_t)((a.nz - kzi) % a.nz) * a.nxh;
+          const double2 pl = a.vwall[mp], ph = a.vwall[nm + mp];
+          vlo = z2(0.5 * (vlo.x + pl.x), 0.5 * (vlo.y - pl.y));
+          vhi = z2(0.5 * (vhi.x + ph.x), 0.5 * (vhi.y - ph.y));
+        }
+        const double gmul = a.control_amp * (double)__ldg(a.gains + m);
+        vlo = zscale(gmul, vlo);
+        vhi = zscale(gmul, vhi);
+      }
     }
-    lu_fwd<BW, 1, 0>(n, [&](int r, double *row) { vrow<BW>(tb, r, n, k2, row); },
+    lu_fwd<BW, 1, 0>(n, [&](int r, double *row, bool c) { vrow<BW>(tb, r, n, k2, row, c); },
         [&](int r, double2 *bc, double *) { bc[0] = (r == 1) ? vlo : (r == n) ? vhi : out.ld(r); },
         [&](int r, const double2 *zc, const double *) { Zr.st(r, zc[0]); }, ub,
         [&](int r) { pfl(out.p, r); });
@@ -318,7 +373,10 @@ __device__ __forceinline__ void helmholtz_role(const SplitArgs &a, const Tabs<BW
           if (q == 1) a.dv[m] = dvp;
           if (q == n) a.dv[nm + m] = dvp;
         },
-        [&](int r) { pfl(Zr.p, r); });
+        [&](int r) {
+          pfl(Zr.p, r);
+          pfu(r);
+        });
   } else {
     // phi_h: (alpha D0 - beta D2) phi_h = unit wall vector, then v_h (real chains)
     const double beta = dt * rkc(2, s) * nu;
@@ -327,7 +385,7 @@ __device__ __forceinline__ void helmholtz_role(const SplitArgs &a, const Tabs<BW
     const RLine Xz{a.xr + m, nm}, X1{a.xr + ns + m, nm}, X2{a.xr + 2 * ns + m, nm};
     const RLine X4{a.xr + 3 * ns + m, nm}, X5{a.xr + 4 * ns + m, nm};
     auto pfr = [&](const double *base, int r) { pf_l1(base + (int64_t)(r - 1) * nm); };
-    lu_fwd<BW, 0, 1>(n, [&](int r, double *row) { helm_row<BW>(tb, r, n, dummy, beta, row); },
+    lu_fwd<BW, 0, 1>(n, [&](int r, double *row, bool c) { helm_row<BW>(tb, r, n, dummy, beta, row, c); },
         [&](int r, double2 *, double *br) { br[0] = (r == 1) ? p0 : 0.0; },
         [&](int r, const double2 *, const double *zr) { Xz.st(r, zr[0]); }, ub);
     bwd_emit<BW, 0, 1>(n, uper, [&](int r, double2 *, double *zr) { zr[0] = Xz.ld(r); },
@@ -335,8 +393,11 @@ __device__ __forceinline__ void helmholtz_role(const SplitArgs &a, const Tabs<BW
           X1.st(q, mvr<BW>(tb.t0, q, r, wr[0]));  // phi_h (real part = imaginary part)
           X2.st(q, mvr<BW>(tb.t2, q, r, wr[0]));  // D2 phi_h
         },
-        [&](int r) { pfr(Xz.p, r); });
-    lu_fwd<BW, 0, 1>(n, [&](int r, double *row) { vrow<BW>(tb, r, n, k2, row); },
+        [&](int r) {
+          pfr(Xz.p, r);
+          pfu(r);
+        });
+    lu_fwd<BW, 0, 1>(n, [&](int r, double *row, bool c) { vrow<BW>(tb, r, n, k2, row, c); },
         [&](int r, double2 *, double *br) { br[0] = (r == 1 || r == n) ? 0.0 : X1.ld(r); },
         [&](int r, const double2 *, const double *zr) { Xz.st(r, zr[0]); }, ub,
         [&](int r) { pfr(X1.p, r); });
@@ -349,7 +410,10 @@ __device__ __forceinline__ void helmholtz_role(const SplitArgs &a, const Tabs<BW
           if (q == 1) dh1 = dvh;
           if (q == n) dhn = dvh;
         },
-        [&](int r) { pfr(Xz.p, r); });
+        [&](int r) {
+          pfr(Xz.p, r);
+          pfu(r);
+        });
     a.dv[2 * nm + m] = z2(dh1, dhn);
   }
 }
@@ -481,7 +545,7 @@ __global__ void k_mean(MeanArgs a) {
       });
   // (D0 - beta D2) c = rhs, Dirichlet rows
   const double beta = dt * rkc(2, s) * visc;
-  lu_fwd<BW, 1, 0>(n, [&](int r, double *row) { helm_row<BW>(tb, r, n, 1.0, beta, row); },
+  lu_fwd<BW, 1, 0>(n, [&](int r, double *row, bool c) { helm_row<BW>(tb, r, n, 1.0, beta, row, c); },
       [&](int r, double2 *bc, double *) { bc[0] = R.ld(r); },
       [&](int r, const double2 *zc, const double *) { R.st(r, zc[0]); }, ub);
   {  // backward substitution storing the coefficients (the integral needs all of them)
@@ -539,8 +603,10 @@ __global__ void k_mean(MeanArgs a) {
   }
 }
 
+// part 0: fork the mean lines to h.side, then k_hvhg; part 1: k_helmholtz; part 2: k_assemble,
+// then join h.side back to st.
 template <int BW>
-cudaError_t split_bw(Handle &h, int substep, const double *dt_ptr, cudaStream_t st) {
+cudaError_t split_bw(Handle &h, int part, int substep, const double *dt_ptr, cudaStream_t st) {
   const OpsOffsets off = ops_offsets(h.bw, h.ny);
   const double *dtp = dt_ptr ? dt_ptr : &h.dsc->dt;
   SplitArgs a;
@@ -561,6 +627,9 @@ cudaError_t split_bw(Handle &h, int substep, const double *dt_ptr, cudaStream_t 
   a.dv = h.dvw;
   a.tabs = h.dops + off.t0;
   a.vwall = h.vwall;
+  a.wlo = h.dops + off.wlo;
+  a.whi = h.dops + off.whi;
+  a.gains = h.gains;
   a.control_amp = h.cfg.control_amp;
   a.nu = h.cfg.nu;
   a.pr = h.cfg.pr;
@@ -589,25 +658,40 @@ cudaError_t split_bw(Handle &h, int substep, const double *dt_ptr, cudaStream_t 
   ma.dsc = h.dsc;
   ma.dt_ptr = dtp;
 
-  // the mean lines touch only mode 0, which the split kernels skip: run them beside those
-  cudaError_t e = cudaEventRecord(h.ev_fork, st);
-  if (e != cudaSuccess) return e;
-  if ((e = cudaStreamWaitEvent(h.side, h.ev_fork, 0)) != cudaSuccess) return e;
-  if (h.mixed) k_mean<BW, float2><<<1, 32, 0, h.side>>>(ma);
-  else k_mean<BW, double2><<<1, 32, 0, h.side>>>(ma);
-  if ((e = cudaGetLastError()) != cudaSuccess) return e;
-  if ((e = cudaEventRecord(h.ev_join, h.side)) != cudaSuccess) return e;
-
+  cudaError_t e;
   const unsigned blocks = (unsigned)((h.nmodes + kLanes - 1) / kLanes);
-  if (h.mixed) k_hvhg<BW, float2><<<blocks, kLanes * kRoles, 0, st>>>(a);
-  else k_hvhg<BW, double2><<<blocks, kLanes * kRoles, 0, st>>>(a);
-  if ((e = cudaGetLastError()) != cudaSuccess) return e;
-  k_helmholtz<BW><<<blocks, kLanes * kRoles, 0, st>>>(a);
-  if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  if (part == 0) {
+    // the mean lines touch only mode 0, which the split kernels skip: run them beside those
+    if ((e = cudaEventRecord(h.ev_fork, st)) != cudaSuccess) return e;
+    if ((e = cudaStreamWaitEvent(h.side, h.ev_fork, 0)) != cudaSuccess) return e;
+    if (h.mixed) k_mean<BW, float2><<<1, 32, 0, h.side>>>(ma);
+    else k_mean<BW, double2><<<1, 32, 0, h.side>>>(ma);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    if ((e = cudaEventRecord(h.ev_join, h.side)) != cudaSuccess) return e;
+    if (h.mixed) k_hvhg<BW, float2><<<blocks, kLanes * kRoles, 0, st>>>(a);
+    else k_hvhg<BW, double2><<<blocks, kLanes * kRoles, 0, st>>>(a);
+    return cudaGetLastError();
+  }
+  if (part == 1) {
+    k_helmholtz<BW><<<blocks, kLanes * kRoles, 0, st>>>(a);
+    return cudaGetLastError();
+  }
   const unsigned ablocks = (unsigned)((h.ns + 255) / 256);
   k_assemble<<<ablocks, 256, 0, st>>>(a);
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
   return cudaStreamWaitEvent(st, h.ev_join, 0);
+}
+
+cudaError_t split_part(Handle &h, int part, int substep, const double *dt_ptr, cudaStream_t st) {
+  switch (h.bw) {
+    case 2: return split_bw<2>(h, part, substep, dt_ptr, st);
+    case 3: return split_bw<3>(h, part, substep, dt_ptr, st);
+    case 4: return split_bw<4>(h, part, substep, dt_ptr, st);
+    case 5: return split_bw<5>(h, part, substep, dt_ptr, st);
+    case 6: return split_bw<6>(h, part, substep, dt_ptr, st);
+    case 7: return split_bw<7>(h, part, substep, dt_ptr, st);
+    default: return cudaErrorInvalidValue;
+  }
 }
 
 }  // namespace
@@ -616,20 +700,23 @@ int64_t split_ub_role(const Handle &h) {
   return (int64_t)h.bw * h.ns + (int64_t)h.bw * h.bw * h.nmodes;
 }
 
+cudaError_t launch_ws_hvhg(Handle &h, int substep, const double *dt_ptr, cudaStream_t st) {
+  return split_part(h, 0, substep, dt_ptr, st);
+}
+
+cudaError_t launch_ws_helmholtz(Handle &h, int substep, const double *dt_ptr, cudaStream_t st) {
+  return split_part(h, 1, substep, dt_ptr, st);
+}
+
+cudaError_t launch_ws_assemble(Handle &h, int substep, const double *dt_ptr, cudaStream_t st) {
+  return split_part(h, 2, substep, dt_ptr, st);
+}
+
 cudaError_t launch_wavespace_split(Handle &h, int substep, const double *dt_ptr, cudaStream_t st) {
-  if (h.cfg.control_amp != 0.0) {
-    cudaError_t e = launch_control_probe(h, st);
-    if (e != cudaSuccess) return e;
-  }
-  switch (h.bw) {
-    case 2: return split_bw<2>(h, substep, dt_ptr, st);
-    case 3: return split_bw<3>(h, substep, dt_ptr, st);
-    case 4: return split_bw<4>(h, substep, dt_ptr, st);
-    case 5: return split_bw<5>(h, substep, dt_ptr, st);
-    case 6: return split_bw<6>(h, substep, dt_ptr, st);
-    case 7: return split_bw<7>(h, substep, dt_ptr, st);
-    default: return cudaErrorInvalidValue;
-  }
+  cudaError_t e = launch_ws_hvhg(h, substep, dt_ptr, st);
+  if (e == cudaSuccess) e = launch_ws_helmholtz(h, substep, dt_ptr, st);
+  if (e == cudaSuccess) e = launch_ws_assemble(h, substep, dt_ptr, st);
+  return e;
 }
 
 }  // namespace kmm

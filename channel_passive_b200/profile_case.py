@@ -1,0 +1,50 @@
+"""A fixed number of RK3 steps of the benchmark workload on one handle, for profiler captures.
+
+    python -m channel_passive_b200.profile_case --steps 2 [--precision mixed|fp64] [--nx 192 ...]
+
+Creates one handle (about 2.5 GB of device memory at 192x129x192 mixed), sets the seeded
+random-phase initial condition, runs --warmup steps through the CUDA graph and then --steps
+steps kernel by kernel (kmm_profile_step), and prints the per-kernel mean device times.  Under a
+profiler the kernels of interest are selected by name (k_hvhg, k_helmholtz, k_assemble,
+k_zinv2, k_xphys2, k_zfwd2, k_mean).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+
+from . import Channel, Config, _lib, ic
+
+RE_TAU = 180.0
+
+
+def main(argv=None) -> int:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--nx", type=int, default=192)
+    ap.add_argument("--ny", type=int, default=129)
+    ap.add_argument("--nz", type=int, default=192)
+    ap.add_argument("--steps", type=int, default=2)
+    ap.add_argument("--warmup", type=int, default=1)
+    ap.add_argument("--precision", choices=("mixed", "fp64"), default="mixed")
+    ap.add_argument("--no-control", action="store_true")
+    args = ap.parse_args(argv)
+    prec = _lib.KMM_PREC_MIXED if args.precision == "mixed" else _lib.KMM_PREC_FP64
+    cfg = Config(nx=args.nx, ny=args.ny, nz=args.nz, lmfx=2.0, lmfz=2.0 / 3.0, stretch=0.9,
+                 nu=1.0 / 2800.0, pr=0.71, fixed_dt=1, precision=prec,
+                 control_amp=0.0 if args.no_control else -1.0, control_yd=-1.0 + 15.0 / RE_TAU)
+    with Channel(cfg) as ch:
+        U0 = ic.seeded_ic(args.nx, args.ny, args.nz, ch.y, 2.0, 2.0 / 3.0, seed=20261203)
+        ch.set_initial_data_uvw(U0, 0.01)
+        if args.warmup:
+            ch.step(args.warmup)
+        prof = ch.profile_step(args.steps)
+        U, _ = ch.download_state()
+    finite = bool(all(math.isfinite(abs(x)) for x in (U[0].sum(), U[1].sum(), U[2].sum(), U[6].sum())))
+    print(json.dumps({"precision": args.precision, "steps": args.steps, "finite": finite,
+                      "kernels_ms": {k: v["ms"] for k, v in prof.items()}}))
+    return 0 if finite else 1
+
+
+if __name__ == "__main__":
+    raise SystemExit(main())

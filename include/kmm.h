@@ -144,13 +144,15 @@ int kmm_step_host(kmm_handle *h, double *U, int nf, double *rk, int nsteps, kmm_
 int kmm_get_stream(const kmm_handle *h, void **stream);
 
 /* Kernel ids reported by kmm_profile_step. */
-#define KMM_NKERNEL 6
+#define KMM_NKERNEL 8
 #define KMM_K_BEGIN 0       /* per-substep scalar reset */
 #define KMM_K_ZINV 1        /* y_to_x: z inverse transform of u, v, w, theta */
 #define KMM_K_XPHYS 2       /* dft_x_realspace: x transforms + products + CFL */
 #define KMM_K_DT 3          /* CFL dt update (substep 1) */
 #define KMM_K_ZFWD 4        /* x_to_y: z forward transform of the 8 products (+ rescale) */
-#define KMM_K_WAVESPACE 5   /* wavespace: per-mode solves and the mean modes */
+#define KMM_K_HVHG 5        /* wavespace part 1: control probe, mean-mode fork, hvhg D0 solves */
+#define KMM_K_HELMHOLTZ 6   /* wavespace part 2: theta, g, phi and v Helmholtz solves */
+#define KMM_K_ASSEMBLE 7    /* wavespace part 3: C1/C2 assembly, u and w, mean-mode join */
 
 /* Runs nsteps RK3 steps launching kernel by kernel with a CUDA event pair around every
  * launch on the handle's stream; ms[k] = mean device time per launch of kernel k,
