@@ -111,11 +111,13 @@ class KmmError(RuntimeError):
 
 
 def load(path: str | os.PathLike | None = None):
-    """Load libkmm.so (once).  Raises if the CUDA library has not been built."""
+    """Load libkmm.so (once).  Raises if the CUDA library has not been built.  The environment
+    variable KMM_LIBRARY selects another build of the same ABI (for example one compiled with
+    different tuning macros)."""
     global _lib
     if _lib is not None:
         return _lib
-    p = Path(path) if path else LIB_PATH
+    p = Path(path) if path else Path(os.environ.get("KMM_LIBRARY") or LIB_PATH)
     if not p.exists():
         raise RuntimeError(f"libkmm.so not found at {p}; build it with "
                            "`python -m channel_passive_b200.build` (nvcc, sm_100a)")

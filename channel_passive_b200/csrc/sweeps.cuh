@@ -16,7 +16,7 @@
 //   backward x_r = z_r - sum_e U(r, r+e) x_{r+e}                     window x_{r..r+2BW}
 // and a band mat-vec (M x)_q = sum_e M(q, q+e) x_{q+e} of the solution is emitted from the
 // backward window as soon as its inputs exist: row q = r+BW at step r (r <= n-2BW), the last
-// BW rows at step n-2BW and the first BW rows at step 1.  All loops over e have compile-time
+// BW rows at step n-2BW and the first BW rows at step 1, in descending order of q.  All loops over e have compile-time
 // trip counts, so the windows stay in registers.
 #pragma once
 
@@ -28,12 +28,25 @@
 
 namespace kmm {
 
-// Rows of look-ahead for the L1 prefetches issued by the sweeps: the per-row loads of a thread
-// are independent of its recurrence, so fetching them a few rows early hides the memory latency
-// that would otherwise stall every row (one warp per scheduler has nothing else to run).
-constexpr int kPrefetchRows = 6;
+// Rows of look-ahead for the prefetches issued by the sweeps: the per-row loads of a thread are
+// independent of its recurrence, so fetching them a few rows early hides the memory latency that
+// would otherwise stall every row (a few warps per scheduler have little else to run).
+// KMM_PREFETCH_ROWS (0 = none) and KMM_PREFETCH_L2 (prefetch into L2 instead of L1) are build
+// tuning macros.
+#ifndef KMM_PREFETCH_ROWS
+#define KMM_PREFETCH_ROWS 3
+#endif
+constexpr int kPrefetchRows = KMM_PREFETCH_ROWS;
 
-__device__ __forceinline__ void pf_l1(const void *p) { asm volatile("prefetch.global.L1 [%0];" ::"l"(p)); }
+__device__ __forceinline__ void pf_l1(const void *p) {
+  if constexpr (kPrefetchRows > 0) {
+#ifdef KMM_PREFETCH_L2
+    asm volatile("prefetch.global.L2 [%0];" ::"l"(p));
+#else
+    asm volatile("prefetch.global.L1 [%0];" ::"l"(p));
+#endif
+  }
+}
 
 struct RLine {
   double *p;
@@ -206,41 +219,49 @@ __device__ __forceinline__ void bwd_emit(int n, UF ufn, Zin zin, Emit emit, Pf p
     };
     if (r > BW) chain.template operator()<BW>();
     else chain.template operator()<2 * BW>();
-    if (r <= n - 2 * BW) emit(r + BW, r, wc, wr);
     if (r == n - 2 * BW)
-      for (int q = n - BW + 1; q <= n; ++q) emit(q, r, wc, wr);
+      for (int q = n; q > n - BW; --q) emit(q, r, wc, wr);
+    if (r <= n - 2 * BW) emit(r + BW, r, wc, wr);
     if (r == 1)
-      for (int q = 1; q <= BW; ++q) emit(q, r, wc, wr);
+      for (int q = BW; q >= 1; --q) emit(q, r, wc, wr);
   }
 }
 
 // Profile Crout LU of a per-mode matrix fused with the forward substitution of NC complex and
-// NR real chains, ascending.  rowA(r, a, centre) fills a[e + 2BW] = A(r, r+e) (for centre rows
-// only |e| <= BW, the entries they use); in(r, bc, br) gives the
-// right-hand sides of row r; out(r, zc, zr) receives the forward results; U goes to ust (for
-// the backward sweep).  Rows 2BW+1..n-BW only touch U(p, p+e) with e <= BW of the last BW rows,
-// which stay in a register window; the first 2BW and last BW rows read U back from ust.
-template <int BW, int NC, int NR, typename RowA, typename In, typename Out, typename Pf = NoPf>
-__device__ __forceinline__ void lu_fwd(int n, RowA rowA, In in, Out out, UBand<BW> ust, Pf pf = Pf()) {
-  constexpr int W = 2 * BW;
-  constexpr int NCc = NC > 0 ? NC : 1, NRr = NR > 0 ? NR : 1;
+// NR real chains, one row per step(), ascending.  rowA(r, a, centre) fills a[e + 2BW] = A(r, r+e)
+// (for centre rows only |e| <= BW, the entries they use); bc / br are the right-hand sides of
+// row r and zc / zr receive the forward results; U goes to ust for the backward sweep.  Rows
+// 2BW+1..n-BW only touch U(p, p+e) with e <= BW of the last BW rows, which stay in a register
+// window; the first 2BW and last BW rows read U back from ust.
+template <int BW, int NC, int NR>
+struct LuSweep {
+  static constexpr int W = 2 * BW;
+  static constexpr int NCc = NC > 0 ? NC : 1, NRr = NR > 0 ? NR : 1;
   double2 wc[NCc][W];
   double wr[NRr][W];
   double Uw[BW][BW];  // Uw[dp-1][e-1] = U(r-dp, r-dp+e)
+  UBand<BW> ust;
+  int n;
+
+  __device__ __forceinline__ void init(int n_, UBand<BW> u) {
+    n = n_;
+    ust = u;
 #pragma unroll
-  for (int k = 0; k < W; ++k) {
+    for (int k = 0; k < W; ++k) {
 #pragma unroll
-    for (int c = 0; c < NCc; ++c) wc[c][k] = z2(0.0, 0.0);
+      for (int c = 0; c < NCc; ++c) wc[c][k] = z2(0.0, 0.0);
 #pragma unroll
-    for (int c = 0; c < NRr; ++c) wr[c][k] = 0.0;
+      for (int c = 0; c < NRr; ++c) wr[c][k] = 0.0;
+    }
+#pragma unroll
+    for (int i = 0; i < BW; ++i)
+#pragma unroll
+      for (int e = 0; e < BW; ++e) Uw[i][e] = 0.0;
   }
-#pragma unroll
-  for (int i = 0; i < BW; ++i)
-#pragma unroll
-    for (int e = 0; e < BW; ++e) Uw[i][e] = 0.0;
-  for (int r = 1; r <= kPrefetchRows && r <= n; ++r) pf(r);
-  for (int r = 1; r <= n; ++r) {
-    if (r + kPrefetchRows <= n) pf(r + kPrefetchRows);
+
+  template <typename RowA>
+  __device__ __forceinline__ void step(int r, RowA rowA, const double2 *bc, const double *br, double2 *zc,
+                                       double *zr) {
     double a[4 * BW + 1];
     double L[W + 1];  // L[d] = L(r, r-d)
     double Ur[W];     // U(r, r+e), e = 1..W
@@ -308,11 +329,6 @@ __device__ __forceinline__ void lu_fwd(int n, RowA rowA, In in, Out out, UBand<B
 #pragma unroll
     for (int e = 0; e < BW; ++e) Uw[0][e] = Ur[e];
     const double rp = L[0];
-    double2 bc[NCc];
-    double br[NRr];
-    in(r, bc, br);
-    double2 zc[NCc];
-    double zr[NRr];
     // L(r, r-d) vanishes for d > BW above the last BW rows
     auto chain = [&]<int D>() {
 #pragma unroll
@@ -347,6 +363,25 @@ __device__ __forceinline__ void lu_fwd(int n, RowA rowA, In in, Out out, UBand<B
       for (int k = 0; k < W - 1; ++k) wr[c][k] = wr[c][k + 1];
       wr[c][W - 1] = zr[c];
     }
+  }
+};
+
+// The LuSweep over rows 1..n: in(r, bc, br) supplies row r's right-hand sides, out(r, zc, zr)
+// receives the forward results.
+template <int BW, int NC, int NR, typename RowA, typename In, typename Out, typename Pf = NoPf>
+__device__ __forceinline__ void lu_fwd(int n, RowA rowA, In in, Out out, UBand<BW> ust, Pf pf = Pf()) {
+  constexpr int NCc = NC > 0 ? NC : 1, NRr = NR > 0 ? NR : 1;
+  LuSweep<BW, NC, NR> lu;
+  lu.init(n, ust);
+  for (int r = 1; r <= kPrefetchRows && r <= n; ++r) pf(r);
+  for (int r = 1; r <= n; ++r) {
+    if (r + kPrefetchRows <= n) pf(r + kPrefetchRows);
+    double2 bc[NCc];
+    double br[NRr];
+    in(r, bc, br);
+    double2 zc[NCc];
+    double zr[NRr];
+    lu.step(r, rowA, bc, br, zc, zr);
     out(r, zc, zr);
   }
 }
