@@ -262,7 +262,7 @@ int download_fields(Handle &h, double *U, int nf, double *rk, cudaStream_t st) {
   const size_t fb = sizeof(double2) * (size_t)h.ns;
   const int slots[4] = {0, 1, 2, 6};
   KMM_CUDA(launch_planes_to_ref(h.S, h.staging, 4, h.nmodes, h.ny, st));
-  KMM_CUDA(launch_planes_to_ref(h.RK, h.staging + 4 * h.ns, 3, h.nmodes, h.ny, st));
+  if (rk) KMM_CUDA(launch_planes_to_ref(h.RK, h.staging + 4 * h.ns, 3, h.nmodes, h.ny, st));
   if (U)
     for (int i = 0; i < 4; ++i)
       KMM_CUDA(cudaMemcpyAsync(U + 2 * (size_t)slots[i] * h.ns, h.staging + i * h.ns, fb, cudaMemcpyDeviceToHost, st));
@@ -635,13 +635,16 @@ int kmm_step(kmm_handle *hh, int nsteps, kmm_scalars *out) {
 }
 
 int kmm_step_host(kmm_handle *hh, double *U, int nf, double *rk, int nsteps, kmm_scalars *out) {
-  if (!hh || !U || !rk || nf < 7) {
+  if (!hh || !U || nf < 7) {
     set_error("kmm_step_host: null pointer or nf < 7");
     return KMM_ERR_ARG;
   }
   Handle &h = *reinterpret_cast<Handle *>(hh);
   int rc = upload_fields(h, U, nf, rk, h.stream);
   if (rc) return rc;
+  // Without rk the stores are rebuilt from U, as the reference's restart option 1 does
+  // (initial_step.f90:31-33).
+  if (!rk) KMM_CUDA(launch_init_stores(h, h.stream));
   if ((rc = kmm_step_async(hh, nsteps))) return rc;
   if ((rc = download_fields(h, U, nf, rk, h.stream))) return rc;
   return kmm_sync(hh, out);

@@ -6,6 +6,7 @@
 
 #include "kmm_internal.h"
 #include "labs.cuh"
+#include "sweeps.cuh"
 
 namespace kmm {
 
@@ -15,7 +16,7 @@ struct InitArgs {
   int ny, nxh, nz;
   int64_t nmodes, ns;
   double2 *S, *RK, *scratch;
-  const double *d2, *d0lu;
+  const double *tabs;  // offset tables T0, T1, T2, L0, U0
   double lmfxr, lmfzr;
 };
 
@@ -23,18 +24,22 @@ __device__ __forceinline__ DLine dline(double2 *base, int64_t off, int64_t m, in
   return DLine{base + off + m, stride};
 }
 
-// set_initial_data_uvw, initial_step.f90:139-179.
+// set_initial_data_uvw, initial_step.f90:139-179: RK_STORE 1 = i kz u - i kx w,
+// RK_STORE 2 = D2 D0^{-1} v - k^2 v, RK_STORE 3 = theta; the mean mode stores U, W, Theta.  One
+// thread per mode: the D0 solve of v runs through the fixed D0 profile LU (sweeps.cuh) and D2 of
+// it is emitted from the backward window.
 template <int BW>
-__global__ void k_init_stores(InitArgs a) {
+__global__ void __launch_bounds__(128) k_init_stores(InitArgs a) {
   const int64_t m = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (m >= a.nmodes) return;
-  const int ny = a.ny;
-  DLine Su = dline(a.S, 0 * a.ns, m, a.nmodes), Sv = dline(a.S, 1 * a.ns, m, a.nmodes);
-  DLine Sw = dline(a.S, 2 * a.ns, m, a.nmodes), St = dline(a.S, 3 * a.ns, m, a.nmodes);
-  DLine R1 = dline(a.RK, 0 * a.ns, m, a.nmodes), R2 = dline(a.RK, 1 * a.ns, m, a.nmodes);
-  DLine R3 = dline(a.RK, 2 * a.ns, m, a.nmodes);
+  const int n = a.ny;
+  const int64_t nm = a.nmodes;
+  const DLine Su = dline(a.S, 0 * a.ns, m, nm), Sv = dline(a.S, 1 * a.ns, m, nm);
+  const DLine Sw = dline(a.S, 2 * a.ns, m, nm), St = dline(a.S, 3 * a.ns, m, nm);
+  const DLine R1 = dline(a.RK, 0 * a.ns, m, nm), R2 = dline(a.RK, 1 * a.ns, m, nm);
+  const DLine R3 = dline(a.RK, 2 * a.ns, m, nm);
   if (m == 0) {
-    for (int i = 1; i <= ny; ++i) {
+    for (int i = 1; i <= n; ++i) {
       R1.st(i, Su.ld(i));
       R2.st(i, Sw.ld(i));
       R3.st(i, St.ld(i));
@@ -44,16 +49,29 @@ __global__ void k_init_stores(InitArgs a) {
   const int kzi = (int)(m / a.nxh), kxi = (int)(m - (int64_t)kzi * a.nxh);
   const int kzint = (kzi <= a.nz / 2) ? kzi : kzi - a.nz;
   const double kx = kxi * a.lmfxr, kz = kzint * a.lmfzr;
-  DLine c = dline(a.scratch, 0, m, a.nmodes);
-  for (int i = 1; i <= ny; ++i) c.st(i, Sv.ld(i));
-  labs_bs<BW>(BandS<BW>{a.d0lu}, c, ny);
-  labs_mat_mul<BW>(BandS<BW>{a.d2}, c, R2, ny);
   const double k2 = kx * kx + kz * kz;
-  for (int i = 1; i <= ny; ++i) {
-    R2.st(i, zsub(R2.ld(i), zscale(k2, Sv.ld(i))));
-    R1.st(i, zsub(zmul(z2(0.0, kz), Su.ld(i)), zmul(z2(0.0, kx), Sw.ld(i))));
-    R3.st(i, St.ld(i));
-  }
+  const Tabs<BW> tb = tabs_at<BW>(a.tabs, n);
+  const DLine Z = dline(a.scratch, 0, m, nm);
+  auto ufix = [&](int r, int e) { return tb.u0[(r - 1) * 2 * BW + e - 1]; };
+  fwd_fixed<BW, 1>(tb, n, [&](int r, double2 *b) { b[0] = Sv.ld(r); },
+                   [&](int r, const double2 *z) { Z.st(r, z[0]); },
+                   [&](int r) { pf_l1(Sv.p + (int64_t)(r - 1) * nm); });
+  bwd_emit<BW, 1, 0>(n, ufix, [&](int r, double2 *zc, double *) { zc[0] = Z.ld(r); },
+      [&](int q, int r, const double2 (&wc)[1][2 * BW + 1], const double (&)[1][2 * BW + 1]) {
+        R2.st(q, zsub(mvc<BW>(tb.t2, q, r, wc[0]), zscale(k2, Sv.ld(q))));
+        R1.st(q, zsub(zmul(z2(0.0, kz), Su.ld(q)), zmul(z2(0.0, kx), Sw.ld(q))));
+        R3.st(q, St.ld(q));
+      },
+      [&](int r) {
+        pf_l1(Z.p + (int64_t)(r - 1) * nm);
+        if (r <= n - 2 * BW) {
+          const int64_t o = (int64_t)(r + BW - 1) * nm;
+          pf_l1(Sv.p + o);
+          pf_l1(Su.p + o);
+          pf_l1(Sw.p + o);
+          pf_l1(St.p + o);
+        }
+      });
 }
 
 // Batched LABS kernels for the unit tests (row 18).
@@ -85,8 +103,7 @@ InitArgs make_init_args(Handle &h) {
   a.S = h.S;
   a.RK = h.RK;
   a.scratch = h.zc;
-  a.d2 = h.dops + off.d2;
-  a.d0lu = h.dops + off.d0lu;
+  a.tabs = h.dops + off.t0;
   a.lmfxr = h.lmfxr;
   a.lmfzr = h.lmfzr;
   return a;

@@ -96,6 +96,19 @@ struct Tabs {
 template <int BW>
 __device__ __forceinline__ const double *trow(const double *t, int r) { return t + (r - 1) * (4 * BW + 1) + 2 * BW; }
 
+// The tables as laid out in the operator buffer: T0, T1, T2 [ny][4BW+1], L0 [ny][2BW+1], U0 [ny][2BW].
+template <int BW>
+__device__ __forceinline__ Tabs<BW> tabs_at(const double *base, int ny) {
+  const int64_t tw = (int64_t)ny * (4 * BW + 1);
+  Tabs<BW> t;
+  t.t0 = base;
+  t.t1 = base + tw;
+  t.t2 = base + 2 * tw;
+  t.l0 = base + 3 * tw;
+  t.u0 = t.l0 + (int64_t)ny * (2 * BW + 1);
+  return t;
+}
+
 // (M x)_q from the backward window w[j] = x_{r+j}: sum_j M(q, r+j-q) w[j].
 template <int BW, typename WT>
 __device__ __forceinline__ double2 mvc(const double *t, int q, int r, const WT &w) {

@@ -69,18 +69,6 @@ struct SplitArgs {
   const double *dt_ptr;
 };
 
-template <int BW>
-__device__ __forceinline__ Tabs<BW> tabs_at(const double *base, int ny) {
-  const int64_t tw = (int64_t)ny * (4 * BW + 1);
-  Tabs<BW> t;
-  t.t0 = base;
-  t.t1 = base + tw;
-  t.t2 = base + 2 * tw;
-  t.l0 = base + 3 * tw;
-  t.u0 = t.l0 + (int64_t)ny * (2 * BW + 1);
-  return t;
-}
-
 template <typename PT> __device__ __forceinline__ double2 ldp(const PT *p);
 template <> __device__ __forceinline__ double2 ldp<double2>(const double2 *p) { return *p; }
 template <> __device__ __forceinline__ double2 ldp<float2>(const float2 *p) {

@@ -215,15 +215,19 @@ class Channel:
         check(self._lib.kmm_sync(self._h, C.byref(s)))
         return s.as_dict()
 
-    def step_host_ptr(self, u_ptr: int, nf: int, rk_ptr: int, nsteps: int = 1) -> dict:
-        """kmm_step_host on raw host pointers (e.g. pinned torch tensors)."""
+    def step_host_ptr(self, u_ptr: int, nf: int, rk_ptr: int | None, nsteps: int = 1) -> dict:
+        """kmm_step_host on raw host pointers (e.g. pinned torch tensors).  rk_ptr None (or 0):
+        RK_STORE is rebuilt from U on the device (restart option 1) and only U is transferred."""
         s = KmmScalars()
-        check(self._lib.kmm_step_host(self._h, C.cast(u_ptr, C.POINTER(C.c_double)), nf,
-                                      C.cast(rk_ptr, C.POINTER(C.c_double)), int(nsteps), C.byref(s)))
+        rk = C.cast(rk_ptr, C.POINTER(C.c_double)) if rk_ptr else None
+        check(self._lib.kmm_step_host(self._h, C.cast(u_ptr, C.POINTER(C.c_double)), nf, rk,
+                                      int(nsteps), C.byref(s)))
         return s.as_dict()
 
-    def step_host(self, U: np.ndarray, RK: np.ndarray, nsteps: int = 1) -> dict:
+    def step_host(self, U: np.ndarray, RK: np.ndarray | None, nsteps: int = 1) -> dict:
         U = _as_state(U, self.config)
+        if RK is None:
+            return self.step_host_ptr(U.ctypes.data, U.shape[0], None, nsteps)
         RK = _as_state(RK, self.config, "RK")
         return self.step_host_ptr(U.ctypes.data, U.shape[0], RK.ctypes.data, nsteps)
 

@@ -137,7 +137,10 @@ int kmm_sync(kmm_handle *h, kmm_scalars *out);
 
 /* End-to-end drop-in with host-resident state: upload U/RK from host memory, run nsteps
  * RK3 steps, download U/RK back.  This is time_march with the reference's ownership of
- * U and RK_STORE (the caller keeps them in host memory). */
+ * U and RK_STORE (the caller keeps them in host memory).  rk may be NULL: between RK3 steps
+ * RK_STORE is a function of u, v, w, theta, so the stores are then rebuilt from U on the
+ * device as the reference's restart option 1 does (initial_step.f90:31-33, set_initial_data_uvw)
+ * and only U (fields 1, 2, 3, 7) crosses the bus, each way. */
 int kmm_step_host(kmm_handle *h, double *U, int nf, double *rk, int nsteps, kmm_scalars *out);
 
 /* The cudaStream_t (as void*) every launch of the handle goes to, for event timing. */

@@ -280,6 +280,23 @@ def test_step_host_matches_resident():
     assert np.array_equal(RKh, RKb)
 
 
+def test_step_host_without_stores_matches_resident():
+    """kmm_step_host with rk = NULL rebuilds RK_STORE from U every call (restart option 1);
+    between RK3 steps the stores are functions of U, so 3 such calls track 3 resident steps."""
+    cfg, p, ops = _setup(nx=16, ny=33, nz=24, control_amp=-1.0)
+    U = seeded_state(cfg, ops.y)
+    with Channel(cfg) as ch:
+        ch.set_initial_data_uvw(U, 0.01)
+        Ua, _ = ch.download_state()
+        ch.step(3)
+        Ub, _ = ch.download_state()
+        Uh = Ua.copy()
+        for _ in range(3):
+            ch.step_host(Uh, None, 1)
+    for s in STATE_SLOTS:
+        assert rel_l2(Uh[s], Ub[s]) < 1e-12, s
+
+
 def test_laminar_fixed_point_gpu():
     cfg, p, ops = _setup(nx=16, ny=33, nz=16)
     U = np.zeros((10, cfg.nz, cfg.nxh, cfg.ny), dtype=np.complex128)
