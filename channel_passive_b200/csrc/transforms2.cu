@@ -23,67 +23,120 @@ template <typename R> __device__ __forceinline__ const typename Cpx<R>::T *tw_of
 template <> __device__ __forceinline__ const double2 *tw_of<double>(const FftPlan &pl) { return pl.tw64; }
 template <> __device__ __forceinline__ const float2 *tw_of<float>(const FftPlan &pl) { return pl.tw32; }
 
-// y_to_x: grid (ceil(nxh/KB), ny, nfield), NT threads
-template <typename R, int N1, int N2, int KB, int NT>
-__global__ void __launch_bounds__(NT) k_zinv2(const double2 *__restrict__ src, typename Cpx<R>::T *__restrict__ dst,
-                                              FftPlan pl, int nz, int nxh, int64_t ns, int64_t nm) {
+// Threads of a z-transform block: one per (line, step-1 or step-2 work item).
+template <int N1, int N2, int KB>
+constexpr int z_threads() {
+  return KB * (N1 > N2 ? N1 : N2);
+}
+
+// The z position of padded index p (3/2 rule of ppdfftw_dft_z_inverse, module_ppdfftw.f90:846-854):
+// kz index for p < nz/2 and p > nz, -1 for the zero band nz/2..nz.
+__device__ __forceinline__ int zpad_src(int p, int nh) { return p < nh ? p : (p > 2 * nh ? p - nh : -1); }
+
+// y_to_x: grid (ceil(nxh/KB), ny, nfield).  Thread (l, n1) of step 1 reads its N2 points
+// x[n1 + N1*n2] of kx line l straight from the Y-pencil (16 consecutive kx per row: one coalesced
+// run), transforms them in registers and leaves them in shared memory; thread (l, k2) of step 2
+// finishes the line and writes X[k2 + N2*k1] straight into the X-pencil slab.
+template <typename R, int N1, int N2, int KB>
+__global__ void __launch_bounds__(z_threads<N1, N2, KB>()) k_zinv2(const double2 *__restrict__ src,
+                                                                  typename Cpx<R>::T *__restrict__ dst,
+                                                                  FftPlan pl, int nz, int nxh, int64_t ns,
+                                                                  int64_t nm) {
   using C = typename Cpx<R>::T;
   constexpr int N = N1 * N2, LD = ip_lda<N1, N2>();
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C *a = reinterpret_cast<C *>(smem_raw);
   const int nh = nz / 2;
   const int kx0 = blockIdx.x * KB, y = blockIdx.y, f = blockIdx.z;
-  const double2 *sp = src + f * ns + (int64_t)y * nz * nxh;
-  for (int w = threadIdx.x; w < N * KB; w += NT) {
-    const int l = w % KB, p = w / KB;
-    int kzi = -1;
-    if (p < nh) kzi = p;
-    else if (p > 2 * nh) kzi = p - nh;
-    C v = cmake<C>(0.0, 0.0);
-    if (kzi >= 0 && kx0 + l < nxh) v = ld_as<C>(sp + (int64_t)kzi * nxh + kx0 + l);
-    a[l * LD + p] = v;
+  const int l = threadIdx.x % KB, item = threadIdx.x / KB;
+  const bool live = kx0 + l < nxh;
+  const C *tw = tw_of<R>(pl);
+  if (item < N1) {
+    const int n1 = item;
+    const double2 *sp = src + f * ns + (int64_t)y * nz * nxh + kx0 + l;
+    C v[N2];
+#pragma unroll
+    for (int n2 = 0; n2 < N2; ++n2) {
+      const int kzi = zpad_src(n1 + N1 * n2, nh);
+      v[n2] = (live && kzi >= 0) ? ld_as<C>(sp + (int64_t)kzi * nxh) : cmake<C>(0.0, 0.0);
+    }
+    reg_dft<C, N2>(v, +1);
+    C *yl = a + l * LD;
+    yl[n1] = v[0];
+#pragma unroll
+    for (int k2 = 1; k2 < N2; ++k2) {
+      C w = tw[n1 * k2];
+      w.y = -w.y;
+      yl[n1 + (N1 + 1) * k2] = n1 > 0 ? cmul(v[k2], w) : v[k2];
+    }
   }
   __syncthreads();
-  fft4_ip<R, N1, N2, KB, NT>(a, LD, tw_of<R>(pl), +1);
-  C *dp = dst + f * nm + (int64_t)y * N * nxh;
-  for (int w = threadIdx.x; w < N * KB; w += NT) {
-    const int l = w % KB, z = w / KB;
-    if (kx0 + l < nxh) dp[(int64_t)z * nxh + kx0 + l] = a[l * LD + z];
+  if (item < N2 && live) {
+    const int k2 = item;
+    const C *yl = a + l * LD;
+    C v[N1];
+#pragma unroll
+    for (int n1 = 0; n1 < N1; ++n1) v[n1] = yl[n1 + (N1 + 1) * k2];
+    reg_dft<C, N1>(v, +1);
+    C *dp = dst + f * nm + (int64_t)y * N * nxh + kx0 + l;
+#pragma unroll
+    for (int k1 = 0; k1 < N1; ++k1) dp[(int64_t)(k2 + N2 * k1) * nxh] = v[k1];
   }
 }
 
-// x_to_y: grid (ceil(nxh/KB), ny, nfield), NT threads
-template <typename R, int N1, int N2, int KB, int NT, typename D>
-__global__ void __launch_bounds__(NT) k_zfwd2(const typename Cpx<R>::T *__restrict__ src, D *__restrict__ dst,
-                                              FftPlan pl, int nz, int nxh, int64_t ns, int64_t nm, double scale) {
+// x_to_y: grid (ceil(nxh/KB), ny, nfield).  The mirror of k_zinv2: step 1 reads the X-pencil
+// slab, step 2 writes the kept frequencies (truncation of ppdfftw_dft_z_forward,
+// module_ppdfftw.f90:811-817) with the kz Nyquist row zeroed and the rescale folded in.
+template <typename R, int N1, int N2, int KB, typename D>
+__global__ void __launch_bounds__(z_threads<N1, N2, KB>()) k_zfwd2(const typename Cpx<R>::T *__restrict__ src,
+                                                                  D *__restrict__ dst, FftPlan pl, int nz, int nxh,
+                                                                  int64_t ns, int64_t nm, double scale) {
   using C = typename Cpx<R>::T;
   constexpr int N = N1 * N2, LD = ip_lda<N1, N2>();
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C *a = reinterpret_cast<C *>(smem_raw);
   const int nh = nz / 2;
   const int kx0 = blockIdx.x * KB, y = blockIdx.y, f = blockIdx.z;
-  const C *sp = src + f * nm + (int64_t)y * N * nxh;
-  for (int w = threadIdx.x; w < N * KB; w += NT) {
-    const int l = w % KB, z = w / KB;
-    a[l * LD + z] = (kx0 + l < nxh) ? sp[(int64_t)z * nxh + kx0 + l] : cmake<C>(0.0, 0.0);
+  const int l = threadIdx.x % KB, item = threadIdx.x / KB;
+  const bool live = kx0 + l < nxh;
+  const C *tw = tw_of<R>(pl);
+  if (item < N1) {
+    const int n1 = item;
+    const C *sp = src + f * nm + (int64_t)y * N * nxh + kx0 + l;
+    C v[N2];
+#pragma unroll
+    for (int n2 = 0; n2 < N2; ++n2) v[n2] = live ? sp[(int64_t)(n1 + N1 * n2) * nxh] : cmake<C>(0.0, 0.0);
+    reg_dft<C, N2>(v, -1);
+    C *yl = a + l * LD;
+    yl[n1] = v[0];
+#pragma unroll
+    for (int k2 = 1; k2 < N2; ++k2) yl[n1 + (N1 + 1) * k2] = n1 > 0 ? cmul(v[k2], tw[n1 * k2]) : v[k2];
   }
   __syncthreads();
-  fft4_ip<R, N1, N2, KB, NT>(a, LD, tw_of<R>(pl), -1);
-  D *dp = dst + f * ns + (int64_t)y * nz * nxh;
-  for (int w = threadIdx.x; w < nz * KB; w += NT) {
-    const int l = w % KB, kzi = w / KB;
-    if (kx0 + l >= nxh) continue;
-    const int k = (kzi < nh) ? kzi : (kzi == nh ? -1 : kzi + nh);
-    D out;
-    if (k < 0) {
-      out.x = 0;
-      out.y = 0;
-    } else {
-      const C v = a[l * LD + k];
-      out.x = (decltype(out.x))(scale * (double)v.x);
-      out.y = (decltype(out.y))(scale * (double)v.y);
+  if (item < N2 && live) {
+    const int k2 = item;
+    const C *yl = a + l * LD;
+    C v[N1];
+#pragma unroll
+    for (int n1 = 0; n1 < N1; ++n1) v[n1] = yl[n1 + (N1 + 1) * k2];
+    reg_dft<C, N1>(v, -1);
+    D *dp = dst + f * ns + (int64_t)y * nz * nxh + kx0 + l;
+#pragma unroll
+    for (int k1 = 0; k1 < N1; ++k1) {
+      const int k = k2 + N2 * k1;
+      int kzi = -1;
+      D out;
+      if (k < nh || k > 2 * nh) {
+        kzi = k < nh ? k : k - nh;
+        out.x = (decltype(out.x))(scale * (double)v[k1].x);
+        out.y = (decltype(out.y))(scale * (double)v[k1].y);
+      } else if (k == nh) {  // the kz Nyquist row is zeroed (module_ppdfftw.f90:811-817)
+        kzi = nh;
+        out.x = 0;
+        out.y = 0;
+      }
+      if (kzi >= 0) dp[(int64_t)kzi * nxh] = out;
     }
-    dp[(int64_t)kzi * nxh + kx0 + l] = out;
   }
 }
 
@@ -211,15 +264,15 @@ template <typename K> void set_smem(K kern, int optin) {
   cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, optin - (int)fa.sharedSizeBytes);
 }
 
-// Lines per block and threads (KB, KT: z transforms; ZB, ZT: x pass), tuned at N = 288 on B200
-// for occupancy: the in-place four-step needs (N1+1)*N2 | 1 complex values of shared memory per
-// line, so these choices keep 39 KB or less per block.
+// Lines per block (KB: z transforms, one thread per line and work item) and rows per block and
+// threads (ZB, ZT: x pass), tuned at N = 288 on B200: a line needs (N1+1)*N2 | 1 complex values
+// of shared memory, so these choices keep 39 KB or less per block.
 template <typename R> struct TCfg;
 template <> struct TCfg<float> {
-  static constexpr int KB = 16, KT = 128, ZB = 2, ZT = 128;
+  static constexpr int KB = 16, ZB = 2, ZT = 128;
 };
 template <> struct TCfg<double> {
-  static constexpr int KB = 4, KT = 128, ZB = 1, ZT = 64;
+  static constexpr int KB = 8, ZB = 1, ZT = 64;
 };
 
 template <typename R, int N1, int N2>
@@ -261,11 +314,11 @@ cudaError_t prepare_transforms2() {
     with_shape(N, [&]<int N1, int N2>() {
       using F = TCfg<float>;
       using D = TCfg<double>;
-      set_smem(k_zinv2<double, N1, N2, D::KB, D::KT>, optin);
-      set_smem(k_zinv2<float, N1, N2, F::KB, F::KT>, optin);
-      set_smem(k_zfwd2<double, N1, N2, D::KB, D::KT, double2>, optin);
-      set_smem(k_zfwd2<float, N1, N2, F::KB, F::KT, float2>, optin);
-      set_smem(k_zfwd2<float, N1, N2, F::KB, F::KT, double2>, optin);
+      set_smem(k_zinv2<double, N1, N2, D::KB>, optin);
+      set_smem(k_zinv2<float, N1, N2, F::KB>, optin);
+      set_smem(k_zfwd2<double, N1, N2, D::KB, double2>, optin);
+      set_smem(k_zfwd2<float, N1, N2, F::KB, float2>, optin);
+      set_smem(k_zfwd2<float, N1, N2, F::KB, double2>, optin);
       set_smem(k_xphys2<double, N1, N2, D::ZB, D::ZT>, optin);
       set_smem(k_xphys2<float, N1, N2, F::ZB, F::ZT>, optin);
     });
@@ -281,7 +334,7 @@ cudaError_t launch_zinv2(Handle &h, const double2 *src, void *mid, int nfield, c
       using C = typename Cpx<R>::T;
       using T = TCfg<R>;
       dim3 grid((unsigned)((h.nxh + T::KB - 1) / T::KB), (unsigned)h.ny, (unsigned)nfield);
-      k_zinv2<R, N1, N2, T::KB, T::KT><<<grid, T::KT, z_smem<R, N1, N2>(), st>>>(
+      k_zinv2<R, N1, N2, T::KB><<<grid, z_threads<N1, N2, T::KB>(), z_smem<R, N1, N2>(), st>>>(
           src, reinterpret_cast<C *>(mid), h.pz, h.nz, h.nxh, h.ns, h.nm);
       err = cudaGetLastError();
     });
@@ -299,7 +352,7 @@ cudaError_t launch_zfwd2(Handle &h, const void *mid, void *dst, int nfield, doub
       using C = typename Cpx<R>::T;
       using T = TCfg<R>;
       dim3 grid((unsigned)((h.nxh + T::KB - 1) / T::KB), (unsigned)h.ny, (unsigned)nfield);
-      k_zfwd2<R, N1, N2, T::KB, T::KT, D><<<grid, T::KT, z_smem<R, N1, N2>(), st>>>(
+      k_zfwd2<R, N1, N2, T::KB, D><<<grid, z_threads<N1, N2, T::KB>(), z_smem<R, N1, N2>(), st>>>(
           reinterpret_cast<const C *>(mid), reinterpret_cast<D *>(dst), h.pz, h.nz, h.nxh, h.ns, h.nm, scale);
       err = cudaGetLastError();
     });
