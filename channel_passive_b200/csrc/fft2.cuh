@@ -29,8 +29,10 @@ constexpr int reg_tw_offset(int M) {
   return -1;
 }
 constexpr int kRegTwTotal = 2 + 3 + 4 + 6 + 8 + 9 + 12 + 16 + 18 + 24 + 32;
-// Defined in the one translation unit that includes this header (transforms2.cu).
+// Defined in the one translation unit that includes this header (transforms2.cu).  The float2
+// copy lets FP32 DFTs take their twiddles as constant operands without conversions.
 __constant__ double2 c_regtw[kRegTwTotal];
+__constant__ float2 c_regtw32[kRegTwTotal];
 
 // First radix of the Stockham factorisation of M (4s first, then 2, then 3).
 constexpr int first_radix(int M) { return (M % 4 == 0 && M != 8 && M != 32) || M == 4 ? 4 : (M % 2 == 0 ? 2 : 3); }
@@ -39,8 +41,13 @@ template <typename C, int M>
 __device__ __forceinline__ C twr(int t, int sign) {
   constexpr int off = reg_tw_offset(M);  // evaluated at compile time: the table offset of size M
   static_assert(off >= 0, "register DFT size without a twiddle table");
-  const double2 w = c_regtw[off + t];
-  return cmake<C>(w.x, sign > 0 ? -w.y : w.y);
+  if constexpr (sizeof(C) == sizeof(float2)) {
+    const float2 w = c_regtw32[off + t];
+    return cmake<C>(w.x, sign > 0 ? -w.y : w.y);
+  } else {
+    const double2 w = c_regtw[off + t];
+    return cmake<C>(w.x, sign > 0 ? -w.y : w.y);
+  }
 }
 
 // One Stockham pass of radix R over M points: Ns = size of the sub-transforms already done.

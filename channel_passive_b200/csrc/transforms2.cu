@@ -297,7 +297,11 @@ cudaError_t fill_regtw() {
     }
     off += M;
   }
-  return cudaMemcpyToSymbol(c_regtw, h, sizeof(h));
+  cudaError_t e = cudaMemcpyToSymbol(c_regtw, h, sizeof(h));
+  if (e != cudaSuccess) return e;
+  float2 h32[kRegTwTotal];
+  for (int i = 0; i < kRegTwTotal; ++i) h32[i] = make_float2((float)h[i].x, (float)h[i].y);
+  return cudaMemcpyToSymbol(c_regtw32, h32, sizeof(h32));
 }
 
 bool fft4_supported(int N) {
