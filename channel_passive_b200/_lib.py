@@ -87,6 +87,7 @@ SIGNATURES = {
     "kmm_sync": (C.c_int, [_P, C.POINTER(KmmScalars)]),
     "kmm_step_host": (C.c_int, [_P, _D, C.c_int, _D, C.c_int, C.POINTER(KmmScalars)]),
     "kmm_get_stream": (C.c_int, [_P, C.POINTER(_P)]),
+    "kmm_get_pressure": (C.c_int, [_P, C.POINTER(C.c_double)]),
     "kmm_profile_step": (C.c_int, [_P, C.c_int, _D, C.POINTER(C.c_int)]),
     "kmm_get_dt": (C.c_int, [_P, _D]),
     "kmm_set_dt": (C.c_int, [_P, C.c_double]),

@@ -650,6 +650,25 @@ int kmm_step_host(kmm_handle *hh, double *U, int nf, double *rk, int nsteps, kmm
   return kmm_sync(hh, out);
 }
 
+int kmm_get_pressure(kmm_handle *hh, double *P) {
+  if (!hh || !P) {
+    set_error("kmm_get_pressure: null pointer");
+    return KMM_ERR_ARG;
+  }
+  Handle &h = *reinterpret_cast<Handle *>(hh);
+  double2 *planes = h.staging, *ref = h.staging + h.ns;
+  const cudaError_t e = launch_pressure(h, planes, h.stream);
+  if (e == cudaErrorNotSupported) {
+    set_error("kmm_get_pressure: nx*3/2 has no four-step FFT shape");
+    return KMM_ERR_CONFIG;
+  }
+  KMM_CUDA(e);
+  KMM_CUDA(launch_planes_to_ref(planes, ref, 1, h.nmodes, h.ny, h.stream));
+  KMM_CUDA(cudaMemcpyAsync(P, ref, sizeof(double2) * (size_t)h.ns, cudaMemcpyDeviceToHost, h.stream));
+  KMM_CUDA(cudaStreamSynchronize(h.stream));
+  return KMM_OK;
+}
+
 int kmm_get_stream(const kmm_handle *hh, void **stream) {
   if (!hh || !stream) return KMM_ERR_ARG;
   *stream = reinterpret_cast<void *>(reinterpret_cast<const Handle *>(hh)->stream);

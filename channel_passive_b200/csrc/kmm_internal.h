@@ -138,7 +138,7 @@ void convert_planes_d2f(const double2 *src, float2 *dst, int64_t n, cudaStream_t
 cudaError_t prepare_transforms2();
 // Four-step transforms (transforms2.cu); return cudaErrorNotSupported for other lengths.
 cudaError_t launch_zinv2(Handle &h, const double2 *src_planes, void *mid, int nfield, cudaStream_t st);
-cudaError_t launch_xphys2(Handle &h, void *mid, int substep, cudaStream_t st);
+cudaError_t launch_xphys2(Handle &h, void *mid, int substep, cudaStream_t st, bool stat = false);
 cudaError_t launch_zfwd2(Handle &h, const void *mid, void *dst_planes, int nfield, double scale,
                          bool dst_fp64, cudaStream_t st);
 // Per-mode solves of one substep (wavespace_split.cu): hvhg, Helmholtz and assembly kernels on
@@ -149,6 +149,10 @@ cudaError_t launch_wavespace_split(Handle &h, int substep, const double *dt_over
 cudaError_t launch_ws_hvhg(Handle &h, int substep, const double *dt_override, cudaStream_t st);
 cudaError_t launch_ws_helmholtz(Handle &h, int substep, const double *dt_override, cudaStream_t st);
 cudaError_t launch_ws_assemble(Handle &h, int substep, const double *dt_override, cudaStream_t st);
+// The pressure of the state (pressure.cu): p planes [y][mode] into out.  Uses MID, P, the
+// solver lines and U region 0 as scratch; cudaErrorNotSupported for x lengths without a
+// four-step shape.
+cudaError_t launch_pressure(Handle &h, double2 *out, cudaStream_t st);
 // Doubles of U factor storage per solver role.
 int64_t split_ub_role(const Handle &h);
 

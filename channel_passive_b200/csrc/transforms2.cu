@@ -151,7 +151,10 @@ struct X2Args {
 
 // dft_x_realspace: grid (ceil(nz32/ZB), ny), NT threads; MID slots 0..3 = u, v, w, theta in,
 // slots 0..7 = f1, f2, f3, f4, f5, f7, f8, f9 out (a block owns its rows).
-template <typename R, int N1, int N2, int ZB, int NT>
+// STAT: the statistics-step products for the pressure instead (f1..f6 with f6 = v v,
+// dft_x_realspace.f90:192-199): packed lines (f1, f2), (f3, f4), (f5, f6); no CFL, and only
+// slots 0..5 are written.
+template <typename R, int N1, int N2, int ZB, int NT, bool STAT = false>
 __global__ void __launch_bounds__(NT) k_xphys2(typename Cpx<R>::T *__restrict__ mid, FftPlan pl, X2Args a_) {
   using C = typename Cpx<R>::T;
   constexpr int N = N1 * N2, LD = ip_lda<N1, N2>();
@@ -196,13 +199,18 @@ __global__ void __launch_bounds__(NT) k_xphys2(typename Cpx<R>::T *__restrict__ 
     C f12, f34, f57, f89;
     f12.x = u * u - bv2; f12.y = u * v;
     f34.x = ww * ww - bv2; f34.y = v * ww;
-    f57.x = u * ww; f57.y = u * t;
-    f89.x = v * t; f89.y = ww * t;
+    if constexpr (STAT) {
+      f57.x = u * ww; f57.y = bv2;
+      f89.x = 0; f89.y = 0;
+    } else {
+      f57.x = u * ww; f57.y = u * t;
+      f89.x = v * t; f89.y = ww * t;
+    }
     a[l * LD + p] = f12;
     a[(ZB + l) * LD + p] = f34;
     a[(2 * ZB + l) * LD + p] = f57;
     a[(3 * ZB + l) * LD + p] = f89;
-    if (a_.substep == 1 && z0 + l < a_.nz32) {
+    if (!STAT && a_.substep == 1 && z0 + l < a_.nz32) {
       const double vel = (fabs((double)u) * a_.dxr) + (fabs((double)v) * dyr) + (fabs((double)ww) * a_.dzr);
       if (!isfinite(vel)) bad = 1;
       else vmax = fmax(vmax, vel);
@@ -210,7 +218,7 @@ __global__ void __launch_bounds__(NT) k_xphys2(typename Cpx<R>::T *__restrict__ 
   }
   __syncthreads();
   fft4_ip<R, N1, N2, 4 * ZB, NT>(a, LD, tw_of<R>(pl), -1);
-  for (int w = threadIdx.x; w < 4 * ZB * nxh; w += NT) {
+  for (int w = threadIdx.x; w < (STAT ? 3 : 4) * ZB * nxh; w += NT) {
     const int k = w % nxh, t = w / nxh, l = t % ZB, bsel = t / ZB;
     if (z0 + l >= a_.nz32) continue;
     const C *line = a + (bsel * ZB + l) * LD;
@@ -222,7 +230,7 @@ __global__ void __launch_bounds__(NT) k_xphys2(typename Cpx<R>::T *__restrict__ 
     mid[(2 * bsel) * a_.nm + off] = A;
     mid[(2 * bsel + 1) * a_.nm + off] = B;
   }
-  if (a_.substep == 1) {
+  if (!STAT && a_.substep == 1) {
     __shared__ double red[NT / 32];
     __shared__ int redbad;
     if (threadIdx.x == 0) redbad = 0;
@@ -325,6 +333,8 @@ cudaError_t prepare_transforms2() {
       set_smem(k_zfwd2<float, N1, N2, F::KB, double2>, optin);
       set_smem(k_xphys2<double, N1, N2, D::ZB, D::ZT>, optin);
       set_smem(k_xphys2<float, N1, N2, F::ZB, F::ZT>, optin);
+      set_smem(k_xphys2<double, N1, N2, D::ZB, D::ZT, true>, optin);
+      set_smem(k_xphys2<float, N1, N2, F::ZB, F::ZT, true>, optin);
     });
   }
   return cudaSuccess;
@@ -370,7 +380,7 @@ cudaError_t launch_zfwd2(Handle &h, const void *mid, void *dst, int nfield, doub
   return err;
 }
 
-cudaError_t launch_xphys2(Handle &h, void *mid, int substep, cudaStream_t st) {
+cudaError_t launch_xphys2(Handle &h, void *mid, int substep, cudaStream_t st, bool stat) {
   cudaError_t err = cudaErrorNotSupported;
   X2Args a;
   a.ny = h.ny;
@@ -387,7 +397,10 @@ cudaError_t launch_xphys2(Handle &h, void *mid, int substep, cudaStream_t st) {
       using C = typename Cpx<R>::T;
       using T = TCfg<R>;
       dim3 grid((unsigned)((h.nz32 + T::ZB - 1) / T::ZB), (unsigned)h.ny);
-      k_xphys2<R, N1, N2, T::ZB, T::ZT><<<grid, T::ZT, x_smem<R, N1, N2>(), st>>>(reinterpret_cast<C *>(mid), h.px, a);
+      if (stat)
+        k_xphys2<R, N1, N2, T::ZB, T::ZT, true><<<grid, T::ZT, x_smem<R, N1, N2>(), st>>>(reinterpret_cast<C *>(mid), h.px, a);
+      else
+        k_xphys2<R, N1, N2, T::ZB, T::ZT><<<grid, T::ZT, x_smem<R, N1, N2>(), st>>>(reinterpret_cast<C *>(mid), h.px, a);
       err = cudaGetLastError();
     });
   };

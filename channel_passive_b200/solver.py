@@ -177,6 +177,14 @@ class Channel:
         check(self._lib.kmm_download_state(self._h, _dptr(U), nf, _dptr(RK)))
         return U, RK
 
+    def get_pressure(self) -> np.ndarray:
+        """get_pressure.f90:1-137 for the current state: the pressure U(:,:,:,6) of the
+        reference, (nz, nxh, ny) complex128 (kmm_get_pressure)."""
+        cfg = self.config
+        P = np.zeros((cfg.nz, cfg.nxh, cfg.ny), dtype=np.complex128)
+        check(self._lib.kmm_get_pressure(self._h, _dptr(P)))
+        return P
+
     @property
     def dt(self) -> float:
         d = C.c_double()

@@ -143,6 +143,14 @@ int kmm_sync(kmm_handle *h, kmm_scalars *out);
  * and only U (fields 1, 2, 3, 7) crosses the bus, each way. */
 int kmm_step_host(kmm_handle *h, double *U, int nf, double *rk, int nsteps, kmm_scalars *out);
 
+/* The pressure of the current state, as a statistics step computes it (get_pressure /
+ * cal_pressure / solve_ppe, get_pressure.f90:1-137, called from get_statistics.f90:458):
+ * the substep-1 products with f6 = v v, the pressure Poisson equation per (kx, kz) with
+ * D1 (Neumann) rows at the walls and zero wall values (the reference never assigns its
+ * stat_PPE_boundary), and -<vv> for the (0,0) mode.  P receives U(:,:,:,6) of the reference,
+ * (nz, nxh, ny) complex128 in host memory.  The state is not changed. */
+int kmm_get_pressure(kmm_handle *h, double *P);
+
 /* The cudaStream_t (as void*) every launch of the handle goes to, for event timing. */
 int kmm_get_stream(const kmm_handle *h, void **stream);
 

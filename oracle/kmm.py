@@ -192,11 +192,13 @@ def x_to_y(Upf: np.ndarray, nz: int) -> np.ndarray:
     return np.ascontiguousarray(np.transpose(small, (2, 0, 1)))  # [kz, kx, y]
 
 
-def dft_x_realspace(Up: np.ndarray, nx: int, substep: int, dxr: float, dzr: float, dyr: np.ndarray):
+def dft_x_realspace(Up: np.ndarray, nx: int, substep: int, dxr: float, dzr: float, dyr: np.ndarray,
+                    stat: bool = False):
     """dft_x_realspace.f90:68-213: per x-line pad, c2r, products, CFL max, r2c, truncate.
 
     Up is [10, y, z32, kx] complex; slots 0,1,2,6 (u,v,w,theta) are read, slots
-    0..4 and 6..9 are written.  Returns velmax (substep 1) or 0.
+    0..4 and 6..9 are written, and slot 5 (f6 = v v, dft_x_realspace.f90:192-199) on a
+    statistics substep (stat).  Returns velmax (substep 1) or 0.
     """
     nxh = nx // 2
     nx32 = nx * 3 // 2
@@ -211,6 +213,8 @@ def dft_x_realspace(Up: np.ndarray, nx: int, substep: int, dxr: float, dzr: floa
     bv2 = v * v
     prods = {8: w * t, 7: v * t, 6: u * t, 4: u * w, 3: v * w, 2: w * w - bv2,
              1: u * v, 0: u * u - bv2, 9: v}
+    if stat:
+        prods[5] = bv2
     velmax = 0.0
     if substep == 1:
         vel = (np.abs(u) * dxr) + (np.abs(v) * dyr[:, None, None]) + (np.abs(w) * dzr)
@@ -629,3 +633,75 @@ def set_initial_data_uvw(U, ops: Operators, p: Params):
                 RK[0, j, k] = (1j * kzr) * U[0, j, k] - (1j * kxr) * U[2, j, k]
                 RK[2, j, k] = U[6, j, k]
     return RK
+
+
+# ----------------------------------------------------------------------------
+# pressure (row 19): get_pressure / cal_pressure / solve_ppe, get_pressure.f90:1-137
+# ----------------------------------------------------------------------------
+def get_uv(a, b):
+    """get_uv, get_statistics.f90:982-1017: <ab>(y) = sum over the stored modes of
+    Re a Re b + Im a Im b, with weight 1 on the kx = 0 plane and 2 elsewhere.
+    a, b are (nz, nxh, ny)."""
+    w = np.full(a.shape[1], 2.0)
+    w[0] = 1.0
+    return np.einsum("zxy,x->y", a.real * b.real + a.imag * b.imag, w)
+
+
+def solve_ppe(u1, u2, u3, u4, u5, u6, ops: Operators, kx, kz, bc1=0.0, bc2=0.0):
+    """solve_ppe, get_pressure.f90:57-137, on lines (ny, M): the pressure Poisson equation
+    (D2 - k^2 D0) c = rhs with Neumann rows (D1) at the walls, p = D0 c.
+
+    u1..u6 are the spectral products u u - v v, u v, w w - v v, v w, u w, v v.  As in the
+    reference, rows 1 and ny of the second D0 solve keep D0^{-1}(v v) (u6 is overwritten only
+    on rows 2..ny-1 before the solve)."""
+    bs, mm = labs.bs, labs.mat_mul
+    k2 = kx * kx + kz * kz
+    kxkz = kx * kz
+    buf1 = np.zeros_like(u1)
+    buf1[1:-1] = kx * kx * u1[1:-1] + kz * kz * u3[1:-1] + k2 * u6[1:-1] + 2.0 * kxkz * u5[1:-1]
+    c6 = bs(ops.D0_lu, u6)
+    buf2 = mm(ops.D2, c6)
+    buf1[1:-1] = buf1[1:-1] - buf2[1:-1]
+    u6b = np.array(c6)
+    u6b[1:-1] = (1j * kx) * u2[1:-1] + (1j * kz) * u4[1:-1]
+    c6b = bs(ops.D0_lu, u6b)
+    buf2 = mm(ops.D1, c6b)
+    buf1[0] = bc1
+    buf1[1:-1] = buf1[1:-1] - 2.0 * buf2[1:-1]
+    buf1[-1] = bc2
+    A = np.array((-k2)[None, None] * ops.D0[..., None] + ops.D2[..., None])
+    A[:, 0] = ops.D1[:, 0][:, None]
+    A[:, -1] = ops.D1[:, -1][:, None]
+    D_buf = labs.lu(A)
+    c = bs(D_buf, buf1)
+    return mm(ops.D0, c)
+
+
+def get_pressure(P, vv, ops: Operators, p: Params):
+    """cal_pressure, get_pressure.f90:17-54: solve_ppe on every mode of the products
+    P (6, nz, nxh, ny) = f1..f6; the (0,0) mode gets -<vv>.  The wall values of the
+    reference (stat_PPE_boundary) are never assigned in its sources, so they are zero.
+    Returns p (nz, nxh, ny)."""
+    kxi, kzi = wavenumbers(p.nx, p.nz)
+    KZ, KX = np.meshgrid(kzi, kxi, indexing="ij")
+    mask = ~((KX == 0) & (KZ == 0))
+    kx = KX[mask] * (1.0 / p.lmfx)
+    kz = KZ[mask] * (1.0 / p.lmfz)
+    lines = [np.ascontiguousarray(P[i][mask].T) for i in range(6)]
+    out = np.zeros((p.nz, p.nxh, p.ny), dtype=np.complex128)
+    out[mask] = solve_ppe(*lines, ops, kx, kz).T
+    out[0, 0] = -vv
+    return out
+
+
+def pressure(U, ops: Operators, p: Params):
+    """The pressure of the state U (10, nz, nxh, ny) as a statistics step computes it
+    (time_march.f90:47-110): <vv> from the state (get_statistics_1), the substep-1 products
+    with f6 = v v through y_to_x, dft_x_realspace and x_to_y, rescale_data, get_pressure."""
+    vv = get_uv(U[1], U[1])
+    Up = np.zeros((10, p.ny, p.nz32, p.nxh), dtype=np.complex128)
+    for f in (0, 1, 2, 6):
+        Up[f] = y_to_x(U[f], p.nz32)
+    dft_x_realspace(Up, p.nx, 2, p.dxr, p.dzr, np.zeros(p.ny), stat=True)
+    P = np.stack([x_to_y(Up[f], p.nz) for f in range(6)]) * p.rescale
+    return get_pressure(P, vv, ops, p)

@@ -336,3 +336,21 @@ def test_nonfinite_state_is_reported():
         with pytest.raises(KmmError) as ei:
             ch.time_march(1)
         assert ei.value.code == _lib.KMM_ERR_NONFINITE
+
+
+@pytest.mark.parametrize("precision,tol", [(0, 1e-11), (1, 1e-5)])
+def test_pressure_matches_oracle(precision, tol):
+    """kmm_get_pressure (get_pressure.f90) against the oracle's statistics-step pressure of the
+    same state, after two steps so that all modes carry energy."""
+    cfg, p, ops = _setup(nx=16, ny=33, nz=24, precision=precision, control_amp=-1.0)
+    U = seeded_state(cfg, ops.y)
+    with Channel(cfg) as ch:
+        ch.set_initial_data_uvw(U, 0.01)
+        ch.step(2)
+        Us, _ = ch.download_state()
+        Pg = ch.get_pressure()
+        Ua, _ = ch.download_state()
+    assert np.array_equal(Us, Ua)  # the state is not changed
+    Po = okmm.pressure(Us, ops, p)
+    assert rel_l2(Pg, Po) < tol
+    assert rel_l2(Pg[0, 0], Po[0, 0]) < 1e-12

@@ -158,3 +158,50 @@ def test_cfl_dt_rule_and_abort():
     q = kmm.Params(nx=8, ny=33, nz=8, fixed_dt=True)
     with pytest.raises(kmm.DtError):
         kmm.time_march(U, RK, ops, q, 1, 2e5, sc)
+
+
+def test_pressure_ppe_banded_matches_dense():
+    """solve_ppe (get_pressure.f90:57-137): the banded LU solve equals a dense solve of the same
+    system -- interior rows (D2 - k^2 D0) c = rhs, Neumann rows D1 c = 0 -- with rhs built as
+    the reference builds it, and p = D0 c."""
+    from channel_passive_b200 import ic
+    p = kmm.Params(nx=16, ny=33, nz=16)
+    ops = kmm.make_operators(p)
+    U = ic.seeded_ic(p.nx, p.ny, p.nz, ops.y, p.lmfx, p.lmfz)
+    rng = np.random.default_rng(7)
+    M = 5
+    lines = [rng.standard_normal((p.ny, M)) + 1j * rng.standard_normal((p.ny, M)) for _ in range(6)]
+    kx = np.array([0.0, 1.0, 2.0, 0.5, 3.0])
+    kz = np.array([1.5, 0.0, -2.0, 4.5, -1.5])
+    P = kmm.solve_ppe(*lines, ops, kx, kz)
+    D0, D1, D2 = (labs.band_to_full(ops.D0), labs.band_to_full(ops.D1), labs.band_to_full(ops.D2))
+    u1, u2, u3, u4, u5, u6 = lines
+    for i in range(M):
+        k2 = kx[i] ** 2 + kz[i] ** 2
+        c6 = np.linalg.solve(D0, u6[:, i])
+        rhs = kx[i] ** 2 * u1[:, i] + kz[i] ** 2 * u3[:, i] + k2 * u6[:, i] + 2 * kx[i] * kz[i] * u5[:, i] - D2 @ c6
+        g = c6.copy()
+        g[1:-1] = 1j * kx[i] * u2[1:-1, i] + 1j * kz[i] * u4[1:-1, i]
+        rhs = rhs - 2 * (D1 @ np.linalg.solve(D0, g))
+        rhs[0] = rhs[-1] = 0.0
+        A = D2 - k2 * D0
+        A[0], A[-1] = D1[0], D1[-1]
+        c = np.linalg.solve(A, rhs)
+        assert np.abs(P[:, i] - D0 @ c).max() <= 1e-10 * max(1.0, np.abs(D0 @ c).max())
+
+
+def test_pressure_mean_mode_and_laminar():
+    """cal_pressure: the (0,0) mode is -<vv> (get_uv weights 1 at kx = 0, 2 elsewhere); a laminar
+    state (v = w = 0) has zero pressure."""
+    from channel_passive_b200 import ic
+    p = kmm.Params(nx=16, ny=33, nz=16)
+    ops = kmm.make_operators(p)
+    U = ic.seeded_ic(p.nx, p.ny, p.nz, ops.y, p.lmfx, p.lmfz)
+    P = kmm.pressure(U, ops, p)
+    v = U[1]
+    vv = (np.abs(v[:, 0]) ** 2).sum(axis=0) + 2 * (np.abs(v[:, 1:]) ** 2).sum(axis=(0, 1))
+    assert np.allclose(P[0, 0].real, -vv, rtol=1e-13, atol=0)
+    assert np.all(P[0, 0].imag == 0)
+    assert np.all(np.isfinite(P))
+    L = _laminar(p, ops)
+    assert np.abs(kmm.pressure(L, ops, p)).max() < 1e-12
