@@ -439,6 +439,12 @@ int kmm_create(const kmm_config *cfg, kmm_handle **out) {
     delete h;
     return KMM_ERR_CONFIG;
   }
+  // The per-mode kernels index within a line, or within a U region of BW lines, in 32 bits.
+  if ((int64_t)(2 * h->bw) * h->ns >= (int64_t)INT32_MAX) {
+    set_error("grid too large: 2*bw*ny*nz*nx/2 must stay below 2^31");
+    delete h;
+    return KMM_ERR_CONFIG;
+  }
   auto fail = [&](int code) {
     kmm_destroy(reinterpret_cast<kmm_handle *>(h));
     return code;

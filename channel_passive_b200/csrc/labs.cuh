@@ -33,18 +33,18 @@ template <typename T> struct Line;
 template <> struct Line<double2> {
   double2 *p;
   int64_t s;
-  __device__ __forceinline__ double2 ld(int i) const { return p[(int64_t)(i - 1) * s]; }
-  __device__ __forceinline__ void st(int i, double2 v) const { p[(int64_t)(i - 1) * s] = v; }
+  __device__ __forceinline__ double2 ld(int i) const { return p[(i - 1) * (int)s]; }
+  __device__ __forceinline__ void st(int i, double2 v) const { p[(i - 1) * (int)s] = v; }
 };
 template <> struct Line<float2> {
   float2 *p;
   int64_t s;
   __device__ __forceinline__ double2 ld(int i) const {
-    float2 v = p[(int64_t)(i - 1) * s];
+    float2 v = p[(i - 1) * (int)s];
     return make_double2((double)v.x, (double)v.y);
   }
   __device__ __forceinline__ void st(int i, double2 v) const {
-    p[(int64_t)(i - 1) * s] = make_float2((float)v.x, (float)v.y);
+    p[(i - 1) * (int)s] = make_float2((float)v.x, (float)v.y);
   }
 };
 using DLine = Line<double2>;

@@ -55,7 +55,7 @@ __global__ void __launch_bounds__(128) k_init_stores(InitArgs a) {
   auto ufix = [&](int r, int e) { return tb.u0[(r - 1) * 2 * BW + e - 1]; };
   fwd_fixed<BW, 1>(tb, n, [&](int r, double2 *b) { b[0] = Sv.ld(r); },
                    [&](int r, const double2 *z) { Z.st(r, z[0]); },
-                   [&](int r) { pf_l1(Sv.p + (int64_t)(r - 1) * nm); });
+                   [&](int r) { pf_l1(Sv.p + (r - 1) * (int)nm); });
   bwd_emit<BW, 1, 0>(n, ufix, [&](int r, double2 *zc, double *) { zc[0] = Z.ld(r); },
       [&](int q, int r, const double2 (&wc)[1][2 * BW + 1], const double (&)[1][2 * BW + 1]) {
         R2.st(q, zsub(mvc<BW>(tb.t2, q, r, wc[0]), zscale(k2, Sv.ld(q))));
@@ -63,9 +63,9 @@ __global__ void __launch_bounds__(128) k_init_stores(InitArgs a) {
         R3.st(q, St.ld(q));
       },
       [&](int r) {
-        pf_l1(Z.p + (int64_t)(r - 1) * nm);
+        pf_l1(Z.p + (r - 1) * (int)nm);
         if (r <= n - 2 * BW) {
-          const int64_t o = (int64_t)(r + BW - 1) * nm;
+          const int64_t o = (r + BW - 1) * (int)nm;
           pf_l1(Sv.p + o);
           pf_l1(Su.p + o);
           pf_l1(Sw.p + o);

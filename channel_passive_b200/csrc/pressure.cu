@@ -48,8 +48,8 @@ __global__ void __launch_bounds__(128) k_ppe(PpeArgs a) {
   const double k2 = kx * kx + kz * kz, kxkz = kx * kz;
   const Tabs<BW> tb = tabs_at<BW>(a.tabs, n);
   const PT *P = reinterpret_cast<const PT *>(a.P) + m;
-  auto prod = [&](int slot, int r) { return ldp<PT>(P + slot * ns + (int64_t)(r - 1) * nm); };
-  auto pfp = [&](int slot, int r) { pf_l1(P + slot * ns + (int64_t)(r - 1) * nm); };
+  auto prod = [&](int slot, int r) { return ldp<PT>(P + slot * ns + (r - 1) * (int)nm); };
+  auto pfp = [&](int slot, int r) { pf_l1(P + slot * ns + (r - 1) * (int)nm); };
   const DLine Z{a.zl + m, nm}, Rh{a.zl + ns + m, nm}, Pout{a.out + m, nm};
   const UBand<BW> ub = make_uband<BW>(a.ub + m, nm, ns);
   auto ufix = [&](int r, int e) { return tb.u0[(r - 1) * 2 * BW + e - 1]; };
@@ -73,7 +73,7 @@ __global__ void __launch_bounds__(128) k_ppe(PpeArgs a) {
         Rh.st(q, rh);
       },
       [&](int r) {
-        pf_l1(Z.p + (int64_t)(r - 1) * nm);
+        pf_l1(Z.p + (r - 1) * (int)nm);
         if (r <= n - 2 * BW) {
           pfp(0, r + BW);
           pfp(2, r + BW);
@@ -107,8 +107,8 @@ __global__ void __launch_bounds__(128) k_ppe(PpeArgs a) {
         }
       },
       [&](int r) {
-        pf_l1(Z.p + (int64_t)(r - 1) * nm);
-        if (r <= n - 2 * BW) pf_l1(Rh.p + (int64_t)(r + BW - 1) * nm);
+        pf_l1(Z.p + (r - 1) * (int)nm);
+        if (r <= n - 2 * BW) pf_l1(Rh.p + (r + BW - 1) * (int)nm);
       });
   // (D2 - k^2 D0, D1 rows at the walls) c = rhs; p = D0 c
   lu_fwd<BW, 1, 0>(n,
@@ -130,16 +130,16 @@ __global__ void __launch_bounds__(128) k_ppe(PpeArgs a) {
       },
       [&](int r, double2 *bc, double *) { bc[0] = Rh.ld(r); },
       [&](int r, const double2 *zc, const double *) { Z.st(r, zc[0]); }, ub,
-      [&](int r) { pf_l1(Rh.p + (int64_t)(r - 1) * nm); });
+      [&](int r) { pf_l1(Rh.p + (r - 1) * (int)nm); });
   bwd_emit<BW, 1, 0>(n, [&](int r, int e) { return ub.get(r, e); },
       [&](int r, double2 *zc, double *) { zc[0] = Z.ld(r); },
       [&](int q, int r, const double2 (&wc)[1][2 * BW + 1], const double (&)[1][2 * BW + 1]) {
         Pout.st(q, mvc<BW>(tb.t0, q, r, wc[0]));
       },
       [&](int r) {
-        pf_l1(Z.p + (int64_t)(r - 1) * nm);
+        pf_l1(Z.p + (r - 1) * (int)nm);
 #pragma unroll
-        for (int e = 1; e <= BW; ++e) pf_l1(ub.p + (int64_t)(e - 1) * ns + (int64_t)(r - 1) * nm);
+        for (int e = 1; e <= BW; ++e) pf_l1(ub.p + (e - 1) * (int)ns + (r - 1) * (int)nm);
       });
 }
 

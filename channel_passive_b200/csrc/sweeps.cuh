@@ -51,8 +51,8 @@ __device__ __forceinline__ void pf_l1(const void *p) {
 struct RLine {
   double *p;
   int64_t s;
-  __device__ __forceinline__ double ld(int i) const { return p[(int64_t)(i - 1) * s]; }
-  __device__ __forceinline__ void st(int i, double v) const { p[(int64_t)(i - 1) * s] = v; }
+  __device__ __forceinline__ double ld(int i) const { return p[(i - 1) * (int)s]; }
+  __device__ __forceinline__ void st(int i, double v) const { p[(i - 1) * (int)s] = v; }
 };
 
 // Per-mode unit-upper factor U(r, r+e), e = 1..2BW.  Inside the profile only the first BW rows
@@ -66,14 +66,14 @@ struct UBand {
   int64_t s;   // stride between rows (number of modes)
   int64_t es;  // stride between offsets (ny * number of modes)
   __device__ __forceinline__ double get(int r, int e) const {
-    if (e <= BW) return p[(int64_t)(e - 1) * es + (int64_t)(r - 1) * s];
-    return r <= BW ? px[(int64_t)((r - 1) * BW + e - BW - 1) * s] : 0.0;
+    if (e <= BW) return p[(e - 1) * (int)es + (r - 1) * (int)s];
+    return r <= BW ? px[((r - 1) * BW + e - BW - 1) * (int)s] : 0.0;
   }
   __device__ __forceinline__ void set(int r, int e, double v) const {
-    if (e <= BW) p[(int64_t)(e - 1) * es + (int64_t)(r - 1) * s] = v;
-    else if (r <= BW) px[(int64_t)((r - 1) * BW + e - BW - 1) * s] = v;
+    if (e <= BW) p[(e - 1) * (int)es + (r - 1) * (int)s] = v;
+    else if (r <= BW) px[((r - 1) * BW + e - BW - 1) * (int)s] = v;
   }
-  __device__ __forceinline__ const double *row_ptr(int r) const { return p + (int64_t)(r - 1) * s; }
+  __device__ __forceinline__ const double *row_ptr(int r) const { return p + (r - 1) * (int)s; }
 };
 template <int BW>
 __device__ __forceinline__ UBand<BW> make_uband(double *base, int64_t s, int64_t es) {

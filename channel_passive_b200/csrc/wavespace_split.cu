@@ -139,8 +139,8 @@ __device__ __forceinline__ void hvhg_role(const SplitArgs &a, const Tabs<BW> &tb
   const double kx = k.kx, kz = k.kz;
   const double kxkz = kx * kz, kx2 = kx * kx, kz2 = kz * kz;
   const PT *P = reinterpret_cast<const PT *>(a.P) + m;
-  auto prod = [&](int slot, int r) { return ldp<PT>(P + slot * ns + (int64_t)(r - 1) * nm); };
-  auto pfp = [&](int slot, int r) { pf_l1(P + slot * ns + (int64_t)(r - 1) * nm); };
+  auto prod = [&](int slot, int r) { return ldp<PT>(P + slot * ns + (r - 1) * (int)nm); };
+  auto pfp = [&](int slot, int r) { pf_l1(P + slot * ns + (r - 1) * (int)nm); };
   const DLine Z0{a.zl + (2 * ROLE) * ns + m, nm}, Z1{a.zl + (2 * ROLE + 1) * ns + m, nm};
   constexpr int store_slot = ROLE == 0 ? 1 : ROLE == 1 ? 2 : 0;  // RK_STORE 2, 3, 1
   constexpr int d2_line = ROLE == 0 ? H_DP : ROLE == 1 ? H_DT : H_DG;
@@ -180,8 +180,8 @@ __device__ __forceinline__ void hvhg_role(const SplitArgs &a, const Tabs<BW> &tb
       [&](int r) {
         if constexpr (ROLE == 0) { pfp(0, r); pfp(2, r); pfp(4, r); }
         else pfp(ROLE == 1 ? 6 : ROLE == 2 ? 1 : 3, r);
-        if constexpr (NC == 2) pf_l1(Rs.p + (int64_t)(r - 1) * nm);
-        if (probe) pf_l1(Sv.p + (int64_t)(r - 1) * nm);
+        if constexpr (NC == 2) pf_l1(Rs.p + (r - 1) * (int)nm);
+        if (probe) pf_l1(Sv.p + (r - 1) * (int)nm);
       });
   if (probe) {
     a.vwall[m] = plo;
@@ -218,8 +218,8 @@ __device__ __forceinline__ void hvhg_role(const SplitArgs &a, const Tabs<BW> &tb
         if constexpr (NC == 2) hl(d2_line).st(q, mvc<BW>(tb.t2, q, r, wc[NC - 1]));
       },
       [&](int r) {
-        pf_l1(Z0.p + (int64_t)(r - 1) * nm);
-        if constexpr (NC == 2) pf_l1(Z1.p + (int64_t)(r - 1) * nm);
+        pf_l1(Z0.p + (r - 1) * (int)nm);
+        if constexpr (NC == 2) pf_l1(Z1.p + (r - 1) * (int)nm);
         if (r <= n - 2 * BW) {
           const int q = r + BW;
           if constexpr (ROLE == 0) { pfp(1, q); pfp(3, q); }
@@ -255,13 +255,13 @@ __device__ __forceinline__ void helmholtz_role(const SplitArgs &a, const Tabs<BW
   const double k2 = mode_k(a, m).k2;
   auto hl = [&](int i) { return DLine{a.hl + i * ns + m, nm}; };
   auto pfl = [&](const void *base, int r) {
-    pf_l1(reinterpret_cast<const char *>(base) + (int64_t)(r - 1) * nm * sizeof(double2));
+    pf_l1(reinterpret_cast<const double2 *>(base) + (r - 1) * (int)nm);
   };
   const UBand<BW> ub = make_uband<BW>(a.ub + ROLE * a.ub_role + m, nm, ns);
   auto uper = [&](int r, int e) { return ub.get(r, e); };
   auto pfu = [&](int r) {  // the U row a backward step reads
 #pragma unroll
-    for (int e = 1; e <= BW; ++e) pf_l1(ub.p + (int64_t)(e - 1) * ns + (int64_t)(r - 1) * nm);
+    for (int e = 1; e <= BW; ++e) pf_l1(ub.p + (e - 1) * (int)ns + (r - 1) * (int)nm);
   };
   const DLine Zr{a.zl + ROLE * ns + m, nm};
 
@@ -372,7 +372,7 @@ __device__ __forceinline__ void helmholtz_role(const SplitArgs &a, const Tabs<BW
     const double p0 = dummy * trow<BW>(tb.t0, 1)[0] - beta * trow<BW>(tb.t2, 1)[0];  // A_g(1,1)
     const RLine Xz{a.xr + m, nm}, X1{a.xr + ns + m, nm}, X2{a.xr + 2 * ns + m, nm};
     const RLine X4{a.xr + 3 * ns + m, nm}, X5{a.xr + 4 * ns + m, nm};
-    auto pfr = [&](const double *base, int r) { pf_l1(base + (int64_t)(r - 1) * nm); };
+    auto pfr = [&](const double *base, int r) { pf_l1(base + (r - 1) * (int)nm); };
     lu_fwd<BW, 0, 1>(n, [&](int r, double *row, bool c) { helm_row<BW>(tb, r, n, dummy, beta, row, c); },
         [&](int r, double2 *, double *br) { br[0] = (r == 1) ? p0 : 0.0; },
         [&](int r, const double2 *, const double *zr) { Xz.st(r, zr[0]); }, ub);
@@ -429,7 +429,7 @@ __global__ void __launch_bounds__(256) k_assemble(SplitArgs a) {
   const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= ns) return;
   const int r = (int)(t / nm) + 1;
-  const int64_t m = t - (int64_t)(r - 1) * nm;
+  const int64_t m = t - (r - 1) * (int)nm;
   if (m == 0) return;
   const int n = a.ny, s = a.substep, rr = n + 1 - r;
   const ModeK k = mode_k(a, m);
@@ -448,8 +448,8 @@ __global__ void __launch_bounds__(256) k_assemble(SplitArgs a) {
     ca = alpha;
   }
   const double *xr = a.xr + m;
-  auto X = [&](int i, int row) { return xr[i * ns + (int64_t)(row - 1) * nm]; };
-  const int64_t o = (int64_t)(r - 1) * nm + m;
+  auto X = [&](int i, int row) { return xr[i * ns + (row - 1) * (int)nm]; };
+  const int64_t o = (r - 1) * (int)nm + m;
   double2 *S = a.S, *Rp = a.RK + ns;
   const double2 v = zadd(zadd(S[ns + o], zscale(X(3, r), C1c)), zscale(X(3, rr), C2c));
   const double2 dv = zsub(zadd(S[2 * ns + o], zscale(X(4, r), C1c)), zscale(X(4, rr), C2c));
@@ -507,13 +507,13 @@ __global__ void k_mean(MeanArgs a) {
   // D0 solves: the flux product (and the store at substep 1)
   fwd_fixed<BW, 2>(tb, n,
       [&](int r, double2 *b) {
-        b[0] = ldp<PT>(P + (int64_t)(r - 1) * a.nmodes);
+        b[0] = ldp<PT>(P + (r - 1) * (int)a.nmodes);
         b[1] = (s == 1) ? store.ld(r) : z2(0.0, 0.0);
       },
       [&](int r, const double2 *z) { Zf.st(r, z[0]); Zs.st(r, z[1]); },
       [&](int r) {
-        pf_l1(P + (int64_t)(r - 1) * a.nmodes);
-        pf_l1(store.p + (int64_t)(r - 1) * a.nmodes);
+        pf_l1(P + (r - 1) * (int)a.nmodes);
+        pf_l1(store.p + (r - 1) * (int)a.nmodes);
       });
   bwd_emit<BW, 2, 0>(n, ufix,
       [&](int r, double2 *zc, double *) { zc[0] = Zf.ld(r); zc[1] = Zs.ld(r); },
@@ -584,7 +584,7 @@ __global__ void k_mean(MeanArgs a) {
           store.st(q, prof);
         }
       },
-      [&](int r) { pf_l1(store.p + (int64_t)(r - 1) * a.nmodes); });
+      [&](int r) { pf_l1(store.p + (r - 1) * (int)a.nmodes); });
   if (line == 1) {  // v mean = 0 (wave00.f90:462)
     const DLine Sv{a.S + ns, a.nmodes};
     for (int r = 1; r <= n; ++r) Sv.st(r, z2(0.0, 0.0));
