@@ -80,7 +80,7 @@ struct ModeK {
   double kx, kz, k2;
 };
 __device__ __forceinline__ ModeK mode_k(const SplitArgs &a, int64_t m) {
-  const int kzi = (int)(m / a.nxh), kxi = (int)(m - (int64_t)kzi * a.nxh);
+  const int mi = (int)m, kzi = mi / a.nxh, kxi = mi - kzi * a.nxh;
   const int kzint = (kzi <= a.nz / 2) ? kzi : kzi - a.nz;  // set_waveno
   ModeK k;
   k.kx = kxi * a.lmfxr;                                   // wavespace.f90:69
@@ -422,15 +422,13 @@ __global__ void __launch_bounds__(kLanes * kRoles, 4) k_helmholtz(SplitArgs a) {
 }
 
 // ------------------------------------------------------------------------------------------
-// k_assemble: one thread per (y, mode), mode fastest.
+// k_assemble: one thread per (y, mode); grid (modes / 256, ny).
 __global__ void __launch_bounds__(256) k_assemble(SplitArgs a) {
   if (a.dsc->err) return;
   const int64_t nm = a.nmodes, ns = a.ns;
-  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= ns) return;
-  const int r = (int)(t / nm) + 1;
-  const int64_t m = t - (r - 1) * (int)nm;
-  if (m == 0) return;
+  const int r = blockIdx.y + 1;
+  const int64_t m = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (m == 0 || m >= nm) return;
   const int n = a.ny, s = a.substep, rr = n + 1 - r;
   const ModeK k = mode_k(a, m);
   // C1, C2 (solve_v_f.f90:293-294); the homogeneous derivative is dvh * (1 + i)
@@ -664,8 +662,8 @@ cudaError_t split_bw(Handle &h, int part, int substep, const double *dt_ptr, cud
     k_helmholtz<BW><<<blocks, kLanes * kRoles, 0, st>>>(a);
     return cudaGetLastError();
   }
-  const unsigned ablocks = (unsigned)((h.ns + 255) / 256);
-  k_assemble<<<ablocks, 256, 0, st>>>(a);
+  const dim3 agrid((unsigned)((h.nmodes + 255) / 256), (unsigned)h.ny);
+  k_assemble<<<agrid, 256, 0, st>>>(a);
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
   return cudaStreamWaitEvent(st, h.ev_join, 0);
 }
