@@ -142,6 +142,7 @@ __global__ void __launch_bounds__(z_threads<N1, N2, KB>()) k_zfwd2(const typenam
 
 struct X2Args {
   int ny, nz32, nxh;
+  float rnxh;  // 1 / nxh: the loops below split w into (w / nxh, w % nxh) without an integer divide
   int64_t nm;
   double dxr, dzr;
   const double *dyr;
@@ -170,7 +171,8 @@ __global__ void __launch_bounds__(NT) k_xphys2(typename Cpx<R>::T *__restrict__ 
   __syncthreads();
   // Z_k = X1_k + i X2_k and its Hermitian mirror at N - k; DC imaginary parts dropped (c2r)
   for (int w = threadIdx.x; w < 2 * ZB * nxh; w += NT) {
-    const int k = w % nxh, t = w / nxh, l = t % ZB, bsel = t / ZB;
+    // exact: (w + 0.5) / nxh stays at least 0.5 / nxh away from an integer, far above float rounding
+    const int t = (int)(((float)w + 0.5f) * a_.rnxh), k = w - t * nxh, l = t % ZB, bsel = t / ZB;
     if (z0 + l >= a_.nz32) continue;
     const int64_t off = row0 + (int64_t)l * nxh + k;
     const int fa = bsel ? 2 : 0, fb = bsel ? 3 : 1;
@@ -219,7 +221,8 @@ __global__ void __launch_bounds__(NT) k_xphys2(typename Cpx<R>::T *__restrict__ 
   __syncthreads();
   fft4_ip<R, N1, N2, 4 * ZB, NT>(a, LD, tw_of<R>(pl), -1);
   for (int w = threadIdx.x; w < (STAT ? 3 : 4) * ZB * nxh; w += NT) {
-    const int k = w % nxh, t = w / nxh, l = t % ZB, bsel = t / ZB;
+    // exact: (w + 0.5) / nxh stays at least 0.5 / nxh away from an integer, far above float rounding
+    const int t = (int)(((float)w + 0.5f) * a_.rnxh), k = w - t * nxh, l = t % ZB, bsel = t / ZB;
     if (z0 + l >= a_.nz32) continue;
     const C *line = a + (bsel * ZB + l) * LD;
     const C zk = line[k], zm = line[k == 0 ? 0 : N - k];
@@ -386,6 +389,7 @@ cudaError_t launch_xphys2(Handle &h, void *mid, int substep, cudaStream_t st, bo
   a.ny = h.ny;
   a.nz32 = h.nz32;
   a.nxh = h.nxh;
+  a.rnxh = 1.0f / (float)h.nxh;
   a.nm = h.nm;
   a.dxr = h.dxr;
   a.dzr = h.dzr;
