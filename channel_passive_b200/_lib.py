@@ -23,6 +23,8 @@ KMM_ERR_TIMEOUT = 6
 KMM_PREC_FP64 = 0
 KMM_PREC_MIXED = 1
 KMM_NOALLOC_MAX_DOUBLES = 2097152
+KMM_STAT_NLINES = 58
+KMM_STAT_NSPEC = 18
 KMM_NKERNEL = 8
 KERNEL_NAMES = ("begin_substep", "zinv", "xphys", "update_dt", "zfwd", "hvhg", "helmholtz", "assemble")
 KMM_GRID_SINE = 0
@@ -88,6 +90,11 @@ SIGNATURES = {
     "kmm_step_host": (C.c_int, [_P, _D, C.c_int, _D, C.c_int, C.POINTER(KmmScalars)]),
     "kmm_get_stream": (C.c_int, [_P, C.POINTER(_P)]),
     "kmm_get_pressure": (C.c_int, [_P, C.POINTER(C.c_double)]),
+    "kmm_get_statistics": (C.c_int, [_P, C.POINTER(C.c_double), C.POINTER(C.c_double),
+                                     C.POINTER(C.c_double), C.POINTER(C.c_double),
+                                     C.POINTER(C.c_double)]),
+    "kmm_stat_line_name": (C.c_char_p, [C.c_int]),
+    "kmm_stat_spec_name": (C.c_char_p, [C.c_int]),
     "kmm_profile_step": (C.c_int, [_P, C.c_int, _D, C.POINTER(C.c_int)]),
     "kmm_get_dt": (C.c_int, [_P, _D]),
     "kmm_set_dt": (C.c_int, [_P, C.c_double]),

@@ -523,7 +523,7 @@ int kmm_destroy(kmm_handle *hh) {
   if (h->stream) cudaStreamSynchronize(h->stream);
   if (h->side) cudaStreamSynchronize(h->side);
   void *ptrs[] = {h->S, h->RK, h->P, h->MID, h->dops, h->gains, h->vwall, h->zc,
-                  h->ec, h->xr, h->ub, h->dvw, h->w00, h->staging,
+                  h->ec, h->xr, h->ub, h->dvw, h->w00, h->staging, h->stat,
                   h->fftpos, h->tw64, h->tw32, h->dsc};
   for (void *p : ptrs)
     if (p) cudaFree(p);
@@ -663,7 +663,9 @@ int kmm_get_pressure(kmm_handle *hh, double *P) {
   }
   Handle &h = *reinterpret_cast<Handle *>(hh);
   double2 *planes = h.staging, *ref = h.staging + h.ns;
-  const cudaError_t e = launch_pressure(h, planes, h.stream);
+  // the wall values nu d2v/dy2 of the state's v into dvw (get_statistics_1's dv/dy call)
+  KMM_CUDA(launch_ydiff(h, 2, h.stream));
+  const cudaError_t e = launch_pressure(h, planes, h.dvw, nullptr, h.stream);
   if (e == cudaErrorNotSupported) {
     set_error("kmm_get_pressure: nx*3/2 has no four-step FFT shape");
     return KMM_ERR_CONFIG;
@@ -674,6 +676,69 @@ int kmm_get_pressure(kmm_handle *hh, double *P) {
   KMM_CUDA(cudaStreamSynchronize(h.stream));
   return KMM_OK;
 }
+
+int kmm_get_statistics(kmm_handle *hh, double *lines, double *spec_kx, double *spec_kz, double *centre,
+                       double *P) {
+  if (!hh) {
+    set_error("kmm_get_statistics: null handle");
+    return KMM_ERR_ARG;
+  }
+  Handle &h = *reinterpret_cast<Handle *>(hh);
+  const StatLayout L = stat_layout(h);
+  if (!h.stat) {
+    int rc;
+    if ((rc = dalloc(h, &h.stat, L.total))) return rc;
+    KMM_CUDA(cudaMemcpy(h.stat + L.center, h.ops.center.data(), sizeof(double) * (size_t)h.ny,
+                        cudaMemcpyHostToDevice));
+  }
+  const cudaError_t e = launch_statistics(h, h.stream);
+  if (e == cudaErrorNotSupported) {
+    set_error("kmm_get_statistics: nx*3/2 has no four-step FFT shape, or nx/2 is too large for the spectra");
+    return KMM_ERR_CONFIG;
+  }
+  KMM_CUDA(e);
+  const size_t ny = (size_t)h.ny;
+  if (lines)
+    KMM_CUDA(cudaMemcpyAsync(lines, h.stat + L.lines, sizeof(double) * KMM_STAT_NLINES * ny,
+                             cudaMemcpyDeviceToHost, h.stream));
+  if (spec_kx)
+    KMM_CUDA(cudaMemcpyAsync(spec_kx, h.stat + L.skx, sizeof(double) * KMM_STAT_NSPEC * (size_t)h.nxh * ny,
+                             cudaMemcpyDeviceToHost, h.stream));
+  if (spec_kz)
+    KMM_CUDA(cudaMemcpyAsync(spec_kz, h.stat + L.skz, sizeof(double) * KMM_STAT_NSPEC * (size_t)h.nz * ny,
+                             cudaMemcpyDeviceToHost, h.stream));
+  if (centre)
+    KMM_CUDA(cudaMemcpyAsync(centre, h.stat + L.scal, 2 * sizeof(double), cudaMemcpyDeviceToHost, h.stream));
+  if (P) {
+    double2 *ref = h.staging + h.ns;
+    KMM_CUDA(launch_planes_to_ref(h.staging, ref, 1, h.nmodes, h.ny, h.stream));
+    KMM_CUDA(cudaMemcpyAsync(P, ref, sizeof(double2) * (size_t)h.ns, cudaMemcpyDeviceToHost, h.stream));
+  }
+  KMM_CUDA(cudaStreamSynchronize(h.stream));
+  return KMM_OK;
+}
+
+namespace {
+// Dataset names of the reference's stat file (get_statistics.f90:60-284, 376-530) and of its
+// spectra file (write_energy_spectra.f90:76-226).
+const char *const kLineNames[KMM_STAT_NLINES] = {
+    "U", "W", "Theta", "dUdy", "dWdy", "dTdy",
+    "uu", "vv", "P", "ww", "tt", "uv", "uw", "vw", "ut", "wt", "vt",
+    "2nududxidudxi", "2nudvdxidvdxi", "2nudwdxidwdxi", "2nududxidvdxi",
+    "omega_x_omega_x", "omega_y_omega_y", "omega_z_omega_z", "omega_x_omega_y",
+    "omega_y_omega_z", "omega_x_omega_z", "v_omega_z", "w_omega_y",
+    "uuu", "vvv", "www", "uuuu", "vvvv", "wwww",
+    "u6", "v6", "w6", "u8", "v8", "w8", "u10", "v10", "w10",
+    "-duuvdy", "-dvvvdy", "-dvwwdy", "-duvvdy",
+    "up", "-dpudy", "vp", "-2dpvdy", "wp", "pp",
+    "2pdudx", "2pdvdy", "2pdwdz", "pdudy+pdvdx"};
+const char *const kSpecNames[KMM_STAT_NSPEC] = {"uu", "vv", "ww", "tt", "uv", "vw", "uw", "ut", "vt",
+                                                "wt", "oxox", "oyoy", "ozoz", "oxoy", "oxoz", "oyoz",
+                                                "voz", "woy"};
+}  // namespace
+
+const char *kmm_stat_line_name(int i) { return (i >= 0 && i < KMM_STAT_NLINES) ? kLineNames[i] : nullptr; }
+const char *kmm_stat_spec_name(int i) { return (i >= 0 && i < KMM_STAT_NSPEC) ? kSpecNames[i] : nullptr; }
 
 int kmm_get_stream(const kmm_handle *hh, void **stream) {
   if (!hh || !stream) return KMM_ERR_ARG;

@@ -21,6 +21,10 @@
 namespace kmm {
 
 constexpr int kMaxPass = 8;
+// Physical-space moment sums of a statistics substep (stats.cuh moment_terms).
+constexpr int kNumMoments = 18;
+// Spectra per direction of a statistics step (stats.cu k_spectra).
+constexpr int kNumSpec = KMM_STAT_NSPEC;
 constexpr int kMinBw = 2;
 constexpr int kMaxBw = 7;
 
@@ -91,6 +95,7 @@ struct Handle {
   double *ub = nullptr;                    //                  U factors, 4 roles (split_ub_role each)
   double2 *dvw = nullptr;                  //                  wall derivatives [3][nmodes]
   double *w00 = nullptr;                   // mean-mode lines (3 threads)
+  double *stat = nullptr;                  // statistics buffers (stat_layout), made on first use
   cudaStream_t side = nullptr;             // mean-mode lines run here, forked from / joined to stream
   cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   double2 *staging = nullptr;              // [7][nz][nxh][ny] reference-layout staging
@@ -138,7 +143,11 @@ void convert_planes_d2f(const double2 *src, float2 *dst, int64_t n, cudaStream_t
 cudaError_t prepare_transforms2();
 // Four-step transforms (transforms2.cu); return cudaErrorNotSupported for other lengths.
 cudaError_t launch_zinv2(Handle &h, const double2 *src_planes, void *mid, int nfield, cudaStream_t st);
-cudaError_t launch_xphys2(Handle &h, void *mid, int substep, cudaStream_t st, bool stat = false);
+// stat: the statistics-step variant (f6 = v v, no CFL); mom (stat only, may be null) receives
+// per-block moment sums [ny][xphys2_row_blocks(h)][kNumMoments].
+cudaError_t launch_xphys2(Handle &h, void *mid, int substep, cudaStream_t st, bool stat = false,
+                          double *mom = nullptr);
+int xphys2_row_blocks(const Handle &h);
 cudaError_t launch_zfwd2(Handle &h, const void *mid, void *dst_planes, int nfield, double scale,
                          bool dst_fp64, cudaStream_t st);
 // Per-mode solves of one substep (wavespace_split.cu): hvhg, Helmholtz and assembly kernels on
@@ -149,10 +158,24 @@ cudaError_t launch_wavespace_split(Handle &h, int substep, const double *dt_over
 cudaError_t launch_ws_hvhg(Handle &h, int substep, const double *dt_override, cudaStream_t st);
 cudaError_t launch_ws_helmholtz(Handle &h, int substep, const double *dt_override, cudaStream_t st);
 cudaError_t launch_ws_assemble(Handle &h, int substep, const double *dt_override, cudaStream_t st);
-// The pressure of the state (pressure.cu): p planes [y][mode] into out.  Uses MID, P, the
-// solver lines and U region 0 as scratch; cudaErrorNotSupported for x lengths without a
-// four-step shape.
-cudaError_t launch_pressure(Handle &h, double2 *out, cudaStream_t st);
+// The pressure of the state (pressure.cu): p planes [y][mode] into out, with the wall values
+// bc [2][nmodes] (launch_ydiff); mom as in launch_xphys2.  Uses MID, P, the solver lines zc
+// and U region 0 as scratch; cudaErrorNotSupported for x lengths without a four-step shape.
+cudaError_t launch_pressure(Handle &h, double2 *out, const double2 *bc, double *mom, cudaStream_t st);
+// y derivatives of the state (stats.cu): for each field f in {u, v, w} with bit f of mask set,
+// ec line f = D1 D0^{-1} f per mode (zc lines 0..2 scratch); with the v bit set, dvw lines 0
+// and 1 = the pressure wall values nu (D2 D0^{-1} v) on rows 1 and ny.
+cudaError_t launch_ydiff(Handle &h, int mask, cudaStream_t st);
+// Offsets (doubles) inside Handle::stat: x-pass moment sums [ny][row blocks][kNumMoments],
+// transport inputs [4][ny], lines [KMM_STAT_NLINES][ny], spectra [kNumSpec][nxh][ny] and
+// [kNumSpec][nz][ny], centre-line values [2], the centre-line vector [ny], line scratch.
+struct StatLayout {
+  int64_t part, tr, lines, skx, skz, scal, center, scr, total;
+};
+StatLayout stat_layout(const Handle &h);
+// The statistics of the state (stats.cu) into Handle::stat; uses the buffers of
+// launch_pressure plus ec and dvw as scratch and leaves the pressure planes in staging[0].
+cudaError_t launch_statistics(Handle &h, cudaStream_t st);
 // Doubles of U factor storage per solver role.
 int64_t split_ub_role(const Handle &h);
 

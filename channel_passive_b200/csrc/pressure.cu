@@ -5,7 +5,9 @@
 // rescale_data), then per (kx, kz)
 //   rhs = kx^2 f1 + kz^2 f3 + k^2 f6 + 2 kx kz f5 - D2 D0^{-1} f6 - 2 D1 D0^{-1} g,
 //   g = i kx f2 + i kz f4 on rows 2..ny-1 and D0^{-1} f6 on rows 1, ny (as the reference
-//   leaves them), rhs = 0 on rows 1, ny (stat_PPE_boundary is never assigned in the reference),
+//   leaves them), rhs on rows 1, ny = the wall values stat_PPE_boundary = nu d2v/dy2 of the
+//   state's v (get_y_dir_deriv_of_field_with_PPE_BC, get_statistics.f90:689-719; stats.cu
+//   k_ydiff computes them),
 //   (D2 - k^2 D0 with D1 rows at the walls) c = rhs,  p = D0 c,
 // and p = -<vv> for the (0,0) mode.  One thread per mode runs the six sweeps (sweeps.cuh): this
 // is a diagnostic of statistics steps, not part of the time step.
@@ -23,6 +25,7 @@ struct PpeArgs {
   int64_t nmodes, ns;
   const void *P;      // products f1..f6 in slots 0..5 (float2 or double2)
   double2 *zl;        // 2 complex scratch lines
+  const double2 *bc;  // [2][nmodes] wall values of rows 1 and ny
   double *ub;         // U factor region
   const double *tabs;
   double lmfxr, lmfzr;
@@ -81,7 +84,8 @@ __global__ void __launch_bounds__(128) k_ppe(PpeArgs a) {
           pfp(5, r + BW);
         }
       });
-  // g = i kx f2 + i kz f4 (rows 2..ny-1), c6 on rows 1, ny; rhs -= 2 D1 D0^{-1} g; walls 0
+  // g = i kx f2 + i kz f4 (rows 2..ny-1), c6 on rows 1, ny; rhs -= 2 D1 D0^{-1} g; the wall
+  // rows take the wall values
   fwd_fixed<BW, 1>(tb, n,
       [&](int r, double2 *b) {
         if (r == 1) b[0] = c6_1;
@@ -99,7 +103,7 @@ __global__ void __launch_bounds__(128) k_ppe(PpeArgs a) {
   bwd_emit<BW, 1, 0>(n, ufix, [&](int r, double2 *zc, double *) { zc[0] = Z.ld(r); },
       [&](int q, int r, const double2 (&wc)[1][2 * BW + 1], const double (&)[1][2 * BW + 1]) {
         if (q == 1 || q == n) {
-          Rh.st(q, z2(0.0, 0.0));
+          Rh.st(q, a.bc[(q == 1 ? 0 : nm) + m]);
         } else {
           const double2 d1 = mvc<BW>(tb.t1, q, r, wc[0]);
           const double2 rh = Rh.ld(q);
@@ -167,7 +171,7 @@ __global__ void __launch_bounds__(256) k_mean_vv(const double2 *__restrict__ v, 
 }
 
 template <int BW>
-cudaError_t ppe_bw(Handle &h, double2 *out, cudaStream_t st) {
+cudaError_t ppe_bw(Handle &h, double2 *out, const double2 *bc, cudaStream_t st) {
   const OpsOffsets off = ops_offsets(h.bw, h.ny);
   PpeArgs a;
   a.ny = h.ny;
@@ -177,6 +181,7 @@ cudaError_t ppe_bw(Handle &h, double2 *out, cudaStream_t st) {
   a.ns = h.ns;
   a.P = h.P;
   a.zl = h.zc;
+  a.bc = bc;
   a.ub = h.ub;
   a.tabs = h.dops + off.t0;
   a.lmfxr = h.lmfxr;
@@ -190,22 +195,22 @@ cudaError_t ppe_bw(Handle &h, double2 *out, cudaStream_t st) {
 
 }  // namespace
 
-cudaError_t launch_pressure(Handle &h, double2 *out, cudaStream_t st) {
+cudaError_t launch_pressure(Handle &h, double2 *out, const double2 *bc, double *mom, cudaStream_t st) {
   // <vv> from the state's v before the transforms overwrite anything (get_statistics_1)
   k_mean_vv<<<h.ny, 256, 0, st>>>(h.S + h.ns, out, h.nmodes, h.nxh);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return e;
   // substep-1 products of a statistics step: f1..f6 in P slots 0..5, rescaled
   if ((e = launch_zinv(h, h.S, h.MID, 4, st)) != cudaSuccess) return e;
-  if ((e = launch_xphys2(h, h.MID, 2, st, true)) != cudaSuccess) return e;
+  if ((e = launch_xphys2(h, h.MID, 2, st, true, mom)) != cudaSuccess) return e;
   if ((e = launch_zfwd(h, h.MID, h.P, 6, h.rescale, !h.mixed, st)) != cudaSuccess) return e;
   switch (h.bw) {
-    case 2: return ppe_bw<2>(h, out, st);
-    case 3: return ppe_bw<3>(h, out, st);
-    case 4: return ppe_bw<4>(h, out, st);
-    case 5: return ppe_bw<5>(h, out, st);
-    case 6: return ppe_bw<6>(h, out, st);
-    case 7: return ppe_bw<7>(h, out, st);
+    case 2: return ppe_bw<2>(h, out, bc, st);
+    case 3: return ppe_bw<3>(h, out, bc, st);
+    case 4: return ppe_bw<4>(h, out, bc, st);
+    case 5: return ppe_bw<5>(h, out, bc, st);
+    case 6: return ppe_bw<6>(h, out, bc, st);
+    case 7: return ppe_bw<7>(h, out, bc, st);
     default: return cudaErrorInvalidValue;
   }
 }

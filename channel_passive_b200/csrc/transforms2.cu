@@ -10,6 +10,7 @@
 
 #include "fft2.cuh"
 #include "kmm_internal.h"
+#include "stats.cuh"
 
 namespace kmm {
 
@@ -148,13 +149,15 @@ struct X2Args {
   const double *dyr;
   int substep;
   DevScalars *dsc;
+  double *mom;  // STAT only, may be null: per-block moment sums [ny][gridDim.x][kNumMoments]
 };
 
 // dft_x_realspace: grid (ceil(nz32/ZB), ny), NT threads; MID slots 0..3 = u, v, w, theta in,
 // slots 0..7 = f1, f2, f3, f4, f5, f7, f8, f9 out (a block owns its rows).
 // STAT: the statistics-step products for the pressure instead (f1..f6 with f6 = v v,
 // dft_x_realspace.f90:192-199): packed lines (f1, f2), (f3, f4), (f5, f6); no CFL, and only
-// slots 0..5 are written.
+// slots 0..5 are written.  With a_.mom set, each block also writes the sums over its physical
+// points of the moments of dft_x_realspace.f90:128-155 (moment_terms), in FP64.
 template <typename R, int N1, int N2, int ZB, int NT, bool STAT = false>
 __global__ void __launch_bounds__(NT) k_xphys2(typename Cpx<R>::T *__restrict__ mid, FftPlan pl, X2Args a_) {
   using C = typename Cpx<R>::T;
@@ -193,10 +196,14 @@ __global__ void __launch_bounds__(NT) k_xphys2(typename Cpx<R>::T *__restrict__ 
   const double dyr = a_.dyr[y];
   double vmax = 0.0;
   int bad = 0;
+  double ms[STAT ? kNumMoments : 1] = {};
   for (int w = threadIdx.x; w < ZB * N; w += NT) {
     const int l = w / N, p = w - l * N;
     const C uv = a[l * LD + p], wt = a[(ZB + l) * LD + p];
     const R u = uv.x, v = uv.y, ww = wt.x, t = wt.y;
+    if constexpr (STAT) {
+      if (a_.mom && z0 + l < a_.nz32) moment_terms(ms, (double)u, (double)v, (double)ww);
+    }
     const R bv2 = v * v;
     C f12, f34, f57, f89;
     f12.x = u * u - bv2; f12.y = u * v;
@@ -232,6 +239,24 @@ __global__ void __launch_bounds__(NT) k_xphys2(typename Cpx<R>::T *__restrict__ 
     const int64_t off = row0 + (int64_t)l * nxh + k;
     mid[(2 * bsel) * a_.nm + off] = A;
     mid[(2 * bsel + 1) * a_.nm + off] = B;
+  }
+  if constexpr (STAT) {
+    if (a_.mom) {
+      // fixed-order block sum: lanes by shuffles, then warps in order
+      __shared__ double mred[NT / 32][kNumMoments];
+#pragma unroll
+      for (int i = 0; i < kNumMoments; ++i) {
+        double x = ms[i];
+        for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+        if ((threadIdx.x & 31) == 0) mred[threadIdx.x >> 5][i] = x;
+      }
+      __syncthreads();
+      if (threadIdx.x < kNumMoments) {
+        double x = 0.0;
+        for (int j = 0; j < NT / 32; ++j) x += mred[j][threadIdx.x];
+        a_.mom[((int64_t)y * gridDim.x + blockIdx.x) * kNumMoments + threadIdx.x] = x;
+      }
+    }
   }
   if (!STAT && a_.substep == 1) {
     __shared__ double red[NT / 32];
@@ -383,7 +408,12 @@ cudaError_t launch_zfwd2(Handle &h, const void *mid, void *dst, int nfield, doub
   return err;
 }
 
-cudaError_t launch_xphys2(Handle &h, void *mid, int substep, cudaStream_t st, bool stat) {
+int xphys2_row_blocks(const Handle &h) {
+  const int zb = h.mixed ? TCfg<float>::ZB : TCfg<double>::ZB;
+  return (h.nz32 + zb - 1) / zb;
+}
+
+cudaError_t launch_xphys2(Handle &h, void *mid, int substep, cudaStream_t st, bool stat, double *mom) {
   cudaError_t err = cudaErrorNotSupported;
   X2Args a;
   a.ny = h.ny;
@@ -396,6 +426,7 @@ cudaError_t launch_xphys2(Handle &h, void *mid, int substep, cudaStream_t st, bo
   a.dyr = h.dops + ops_offsets(h.bw, h.ny).dyr;
   a.substep = substep;
   a.dsc = h.dsc;
+  a.mom = stat ? mom : nullptr;
   auto go = [&]<typename R>() {
     with_shape(h.nx32, [&]<int N1, int N2>() {
       using C = typename Cpx<R>::T;

@@ -185,6 +185,29 @@ class Channel:
         check(self._lib.kmm_get_pressure(self._h, _dptr(P)))
         return P
 
+    def get_statistics(self, pressure: bool = False) -> dict:
+        """The statistics of a statistics step of the current state (kmm_get_statistics:
+        get_statistics_1, write_spectra, the physical moments of dft_x_realspace and
+        get_statistics_2).  Returns {"lines": {name: (ny,)}, "spec_kx": {name: (nxh, ny)},
+        "spec_kz": {name: (nz, ny)}, "U_c", "T_c"} with the reference's dataset names (spectrum
+        "uu" is "Euu_kx" / "Euu_kz" there), plus "P" (nz, nxh, ny) when pressure is set."""
+        cfg = self.config
+        nl, nsp = _lib.KMM_STAT_NLINES, _lib.KMM_STAT_NSPEC
+        lines = np.zeros((nl, cfg.ny))
+        skx = np.zeros((nsp, cfg.nxh, cfg.ny))
+        skz = np.zeros((nsp, cfg.nz, cfg.ny))
+        centre = np.zeros(2)
+        P = np.zeros((cfg.nz, cfg.nxh, cfg.ny), dtype=np.complex128) if pressure else None
+        check(self._lib.kmm_get_statistics(self._h, _dptr(lines), _dptr(skx), _dptr(skz), _dptr(centre),
+                                           _dptr(P) if pressure else None))
+        lnames = [self._lib.kmm_stat_line_name(i).decode() for i in range(nl)]
+        snames = [self._lib.kmm_stat_spec_name(i).decode() for i in range(nsp)]
+        out = {"lines": dict(zip(lnames, lines)), "spec_kx": dict(zip(snames, skx)),
+               "spec_kz": dict(zip(snames, skz)), "U_c": float(centre[0]), "T_c": float(centre[1])}
+        if pressure:
+            out["P"] = P
+        return out
+
     @property
     def dt(self) -> float:
         d = C.c_double()

@@ -146,10 +146,34 @@ int kmm_step_host(kmm_handle *h, double *U, int nf, double *rk, int nsteps, kmm_
 /* The pressure of the current state, as a statistics step computes it (get_pressure /
  * cal_pressure / solve_ppe, get_pressure.f90:1-137, called from get_statistics.f90:458):
  * the substep-1 products with f6 = v v, the pressure Poisson equation per (kx, kz) with
- * D1 (Neumann) rows at the walls and zero wall values (the reference never assigns its
- * stat_PPE_boundary), and -<vv> for the (0,0) mode.  P receives U(:,:,:,6) of the reference,
- * (nz, nxh, ny) complex128 in host memory.  The state is not changed. */
+ * D1 (Neumann) rows at the walls whose values are stat_PPE_boundary = nu d2v/dy2 of the
+ * state's v at the walls (get_y_dir_deriv_of_field_with_PPE_BC, get_statistics.f90:689-719),
+ * and -<vv> for the (0,0) mode.  P receives U(:,:,:,6) of the reference, (ny, nxh, nz)
+ * complex128 in host memory.  The state is not changed. */
 int kmm_get_pressure(kmm_handle *h, double *P);
+
+/* Statistics of the current state, as a statistics step computes them at the start of RK
+ * substep 1 (time_march.f90:47-110): get_statistics_1 (get_statistics.f90:9-368), write_spectra
+ * (write_energy_spectra.f90:9-399), the physical-space moments of dft_x_realspace
+ * (dft_x_realspace.f90:128-155, 238-484) and get_statistics_2 (get_statistics.f90:376-539).
+ * Host outputs, each may be NULL:
+ *   lines    [KMM_STAT_NLINES][ny]           the stat file's lines, in the order of the
+ *                                            KMM_STAT_* indices (kmm_stat_line_name)
+ *   spec_kx  [KMM_STAT_NSPEC][nxh][ny]       Exx_kx datasets, STAT(ny, nxh) each
+ *   spec_kz  [KMM_STAT_NSPEC][nz][ny]        Exx_kz datasets, STAT(ny, nz) each; as in the
+ *                                            reference, "Eozoz_kz" holds the ox-oz cospectrum
+ *                                            (write_energy_spectra.f90:218-219)
+ *   centre   [2]                             U_c and T_c
+ *   P        (ny, nxh, nz) complex128        the pressure (kmm_get_pressure)
+ * The state is not changed.  The first call allocates the statistics buffers on the device. */
+#define KMM_STAT_NLINES 58
+#define KMM_STAT_NSPEC 18
+int kmm_get_statistics(kmm_handle *h, double *lines, double *spec_kx, double *spec_kz,
+                       double *centre, double *P);
+/* Dataset names of line i (without the stat file's path) and of spectrum i (without the
+ * "E" prefix and the "_kx"/"_kz" suffix); NULL out of range. */
+const char *kmm_stat_line_name(int i);
+const char *kmm_stat_spec_name(int i);
 
 /* The cudaStream_t (as void*) every launch of the handle goes to, for event timing. */
 int kmm_get_stream(const kmm_handle *h, void **stream);

@@ -677,31 +677,47 @@ def solve_ppe(u1, u2, u3, u4, u5, u6, ops: Operators, kx, kz, bc1=0.0, bc2=0.0):
     return mm(ops.D0, c)
 
 
-def get_pressure(P, vv, ops: Operators, p: Params):
+def ppe_boundary(v, ops: Operators, p: Params):
+    """get_y_dir_deriv_of_field_with_PPE_BC, get_statistics.f90:689-719 (called from
+    get_statistics_1 before get_pressure): with c = D0^{-1} v per mode,
+    BC1 = nu (D2 c) on row 1 from columns 1..3 and BC2 = nu (D2 c) on row ny from columns
+    ny-2..ny (the band entries LABS_D2_B(bw+1..bw+3, 1) and LABS_D2_B(bw-1..bw+1, ny)).
+    v is (nz, nxh, ny); returns (bc1, bc2), each (nz, nxh) complex."""
+    c = labs.bs(ops.D0_lu, np.ascontiguousarray(v.reshape(-1, v.shape[-1]).T))
+    bw = ops.bw
+    D2 = ops.D2
+    bc1 = p.nu * (D2[bw, 0] * c[0] + D2[bw + 1, 0] * c[1] + D2[bw + 2, 0] * c[2])
+    bc2 = p.nu * (D2[bw - 2, -1] * c[-3] + D2[bw - 1, -1] * c[-2] + D2[bw, -1] * c[-1])
+    return bc1.reshape(v.shape[:2]), bc2.reshape(v.shape[:2])
+
+
+def get_pressure(P, vv, ops: Operators, p: Params, bc=None):
     """cal_pressure, get_pressure.f90:17-54: solve_ppe on every mode of the products
-    P (6, nz, nxh, ny) = f1..f6; the (0,0) mode gets -<vv>.  The wall values of the
-    reference (stat_PPE_boundary) are never assigned in its sources, so they are zero.
-    Returns p (nz, nxh, ny)."""
+    P (6, nz, nxh, ny) = f1..f6 with the wall values bc = (bc1, bc2) (stat_PPE_boundary,
+    (nz, nxh) each; zero when None); the (0,0) mode gets -<vv>.  Returns p (nz, nxh, ny)."""
     kxi, kzi = wavenumbers(p.nx, p.nz)
     KZ, KX = np.meshgrid(kzi, kxi, indexing="ij")
     mask = ~((KX == 0) & (KZ == 0))
     kx = KX[mask] * (1.0 / p.lmfx)
     kz = KZ[mask] * (1.0 / p.lmfz)
     lines = [np.ascontiguousarray(P[i][mask].T) for i in range(6)]
+    bc1, bc2 = (0.0, 0.0) if bc is None else (bc[0][mask], bc[1][mask])
     out = np.zeros((p.nz, p.nxh, p.ny), dtype=np.complex128)
-    out[mask] = solve_ppe(*lines, ops, kx, kz).T
+    out[mask] = solve_ppe(*lines, ops, kx, kz, bc1, bc2).T
     out[0, 0] = -vv
     return out
 
 
 def pressure(U, ops: Operators, p: Params):
     """The pressure of the state U (10, nz, nxh, ny) as a statistics step computes it
-    (time_march.f90:47-110): <vv> from the state (get_statistics_1), the substep-1 products
-    with f6 = v v through y_to_x, dft_x_realspace and x_to_y, rescale_data, get_pressure."""
+    (time_march.f90:47-110): <vv> and the wall values nu d2v/dy2 (ppe_boundary) from the state
+    (get_statistics_1), the substep-1 products with f6 = v v through y_to_x, dft_x_realspace
+    and x_to_y, rescale_data, get_pressure."""
     vv = get_uv(U[1], U[1])
+    bc = ppe_boundary(U[1], ops, p)
     Up = np.zeros((10, p.ny, p.nz32, p.nxh), dtype=np.complex128)
     for f in (0, 1, 2, 6):
         Up[f] = y_to_x(U[f], p.nz32)
     dft_x_realspace(Up, p.nx, 2, p.dxr, p.dzr, np.zeros(p.ny), stat=True)
     P = np.stack([x_to_y(Up[f], p.nz) for f in range(6)]) * p.rescale
-    return get_pressure(P, vv, ops, p)
+    return get_pressure(P, vv, ops, p, bc)

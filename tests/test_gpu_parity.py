@@ -354,3 +354,35 @@ def test_pressure_matches_oracle(precision, tol):
     Po = okmm.pressure(Us, ops, p)
     assert rel_l2(Pg, Po) < tol
     assert rel_l2(Pg[0, 0], Po[0, 0]) < 1e-12
+
+
+@pytest.mark.parametrize("precision,tol", [(0, 1e-11), (1, 1e-5)])
+def test_statistics_match_oracle(precision, tol):
+    """kmm_get_statistics (get_statistics_1, write_spectra, the physical moments of
+    dft_x_realspace, get_statistics_2) against the oracle's statistics of the same state, line by
+    line and spectrum by spectrum; a second call gives identical numbers (fixed-order sums) and the
+    state is unchanged."""
+    from oracle import stats as ostats
+    cfg, p, ops = _setup(nx=16, ny=33, nz=24, precision=precision, control_amp=-1.0)
+    U = seeded_state(cfg, ops.y)
+    with Channel(cfg) as ch:
+        ch.set_initial_data_uvw(U, 0.01)
+        ch.step(2)
+        Us, _ = ch.download_state()
+        g = ch.get_statistics(pressure=True)
+        g2 = ch.get_statistics()
+        Ua, _ = ch.download_state()
+    assert np.array_equal(Us, Ua)
+    for name in ostats.LINE_NAMES:
+        assert np.array_equal(g["lines"][name], g2["lines"][name]), name
+    o = ostats.statistics(Us, ops, p)
+    for i, name in enumerate(ostats.LINE_NAMES):
+        ref = o["lines"][i]
+        err = np.abs(g["lines"][name] - ref).max() / max(np.abs(ref).max(), 1e-30)
+        assert err < tol or np.abs(ref).max() < 1e-14, (name, err)
+    for i, name in enumerate(ostats.SPEC_NAMES):
+        assert rel_l2(g["spec_kx"][name], o["spec_kx"][i]) < tol, ("kx", name)
+        assert rel_l2(g["spec_kz"][name], o["spec_kz"][i]) < tol, ("kz", name)
+    assert abs(g["U_c"] - o["u_center"]) <= 1e-12 * abs(o["u_center"])
+    assert abs(g["T_c"] - o["t_center"]) <= 1e-12 * abs(o["t_center"])
+    assert rel_l2(g["P"], o["P"]) < tol
