@@ -281,23 +281,21 @@ __device__ __forceinline__ void helmholtz_role(const SplitArgs &a, const Tabs<BW
     return zadd(zadd(zscale(zeta, h), zscale(1.0 - alpha * k2, f)), zscale(alpha, d2f));
   };
 
-  if constexpr (ROLE <= 2) {
-    // one complex Helmholtz solve: theta (role 0), g (role 1), phi_p (role 2)
+  {
+    // one complex Helmholtz solve: theta (role 0), g (role 1)
     const double visc = ROLE == 0 ? nu / a.pr : nu;
     const double beta = dt * rkc(2, s) * visc;
     const double dummy = 1.0 + beta * k2;
-    const int sslot = ROLE == 0 ? 2 : ROLE == 1 ? 0 : 1;
+    const int sslot = ROLE == 0 ? 2 : 0;
     const DLine store{a.RK + sslot * ns + m, nm};
-    const DLine d2l = hl(ROLE == 0 ? H_DT : ROLE == 1 ? H_DG : H_DP);
+    const DLine d2l = hl(ROLE == 0 ? H_DT : H_DG);
     auto hsum = [&](int r) {
       if constexpr (ROLE == 0) return hl(H_HT).ld(r);
-      if (ROLE == 1) return zadd(hl(H_G2).ld(r), hl(H_G3).ld(r));
-      return zadd(hl(H_HV0).ld(r), zadd(hl(H_V2).ld(r), hl(H_V3).ld(r)));
+      else return zadd(hl(H_G2).ld(r), hl(H_G3).ld(r));
     };
     auto pfh = [&](int r) {
       if constexpr (ROLE == 0) pfl(hl(H_HT).p, r);
-      else if constexpr (ROLE == 1) { pfl(hl(H_G2).p, r); pfl(hl(H_G3).p, r); }
-      else { pfl(hl(H_HV0).p, r); pfl(hl(H_V2).p, r); pfl(hl(H_V3).p, r); }
+      else { pfl(hl(H_G2).p, r); pfl(hl(H_G3).p, r); }
     };
     lu_fwd<BW, 1, 0>(n, [&](int r, double *row, bool c) { helm_row<BW>(tb, r, n, dummy, beta, row, c); },
         [&](int r, double2 *bc, double *) {
@@ -309,7 +307,7 @@ __device__ __forceinline__ void helmholtz_role(const SplitArgs &a, const Tabs<BW
           pfh(r);
           if (s == 1) pfl(d2l.p, r);
         });
-    const DLine out{ROLE == 0 ? a.S + 3 * ns + m : ROLE == 1 ? a.S + m : a.zl + 4 * ns + m, nm};
+    const DLine out{ROLE == 0 ? a.S + 3 * ns + m : a.S + m, nm};
     bwd_emit<BW, 1, 0>(n, uper, [&](int r, double2 *zc, double *) { zc[0] = Zr.ld(r); },
         [&](int q, int r, const double2 (&wc)[1][2 * BW + 1], const double (&)[1][2 * BW + 1]) {
           const double2 f = mvc<BW>(tb.t0, q, r, wc[0]), d2f = mvc<BW>(tb.t2, q, r, wc[0]);
@@ -325,89 +323,171 @@ __device__ __forceinline__ void helmholtz_role(const SplitArgs &a, const Tabs<BW
             pfl(store.p, q);
           }
         });
-    if constexpr (ROLE != 2) return;
-    // (D2 - k^2 D0) v_p = phi_p with v_p = the wall velocity at rows 1 and n
-    // Opposition control, the extension at the wall rows of the v solve (solve_v_f.f90:251-257,
-    // whose commented lines read vold): v at the walls = A * gain * v(+-y_d).  vold is field 10,
-    // v after the physical round trip (dft_x_realspace.f90:123), which has no kz Nyquist mode
-    // and, at kx = 0, only the Hermitian part (v(kz) + conj v(-kz)) / 2.
-    double2 vlo = z2(0.0, 0.0), vhi = z2(0.0, 0.0);
-    if (a.control_amp != 0.0) {
-      const int kzi = (int)(m / a.nxh), kxi = (int)(m - (int64_t)kzi * a.nxh);
-      if (kzi != a.nz / 2) {
-        vlo = a.vwall[m];
-        vhi = a.vwall[nm + m];
-        if (kxi == 0) {
-          const int64_t mp = (int64_t)((a.nz - kzi) % a.nz) * a.nxh;
-          const double2 pl = a.vwall[mp], ph = a.vwall[nm + mp];
-          vlo = z2(0.5 * (vlo.x + pl.x), 0.5 * (vlo.y - pl.y));
-          vhi = z2(0.5 * (vhi.x + ph.x), 0.5 * (vhi.y - ph.y));
-        }
-        const double gmul = a.control_amp * (double)__ldg(a.gains + m);
-        vlo = zscale(gmul, vlo);
-        vhi = zscale(gmul, vhi);
-      }
-    }
-    lu_fwd<BW, 1, 0>(n, [&](int r, double *row, bool c) { vrow<BW>(tb, r, n, k2, row, c); },
-        [&](int r, double2 *bc, double *) { bc[0] = (r == 1) ? vlo : (r == n) ? vhi : out.ld(r); },
-        [&](int r, const double2 *zc, const double *) { Zr.st(r, zc[0]); }, ub,
-        [&](int r) { pfl(out.p, r); });
-    const DLine Sv{a.S + ns + m, nm}, Sw{a.S + 2 * ns + m, nm};
-    bwd_emit<BW, 1, 0>(n, uper, [&](int r, double2 *zc, double *) { zc[0] = Zr.ld(r); },
-        [&](int q, int r, const double2 (&wc)[1][2 * BW + 1], const double (&)[1][2 * BW + 1]) {
-          const double2 vp = mvc<BW>(tb.t0, q, r, wc[0]), dvp = mvc<BW>(tb.t1, q, r, wc[0]);
-          Sv.st(q, vp);
-          Sw.st(q, dvp);
-          if (q == 1) a.dv[m] = dvp;
-          if (q == n) a.dv[nm + m] = dvp;
-        },
-        [&](int r) {
-          pfl(Zr.p, r);
-          pfu(r);
-        });
-  } else {
-    // phi_h: (alpha D0 - beta D2) phi_h = unit wall vector, then v_h (real chains)
-    const double beta = dt * rkc(2, s) * nu;
-    const double dummy = 1.0 + beta * k2;
-    const double p0 = dummy * trow<BW>(tb.t0, 1)[0] - beta * trow<BW>(tb.t2, 1)[0];  // A_g(1,1)
-    const RLine Xz{a.xr + m, nm}, X1{a.xr + ns + m, nm}, X2{a.xr + 2 * ns + m, nm};
-    const RLine X4{a.xr + 3 * ns + m, nm}, X5{a.xr + 4 * ns + m, nm};
-    auto pfr = [&](const double *base, int r) { pf_l1(base + (r - 1) * (int)nm); };
-    lu_fwd<BW, 0, 1>(n, [&](int r, double *row, bool c) { helm_row<BW>(tb, r, n, dummy, beta, row, c); },
-        [&](int r, double2 *, double *br) { br[0] = (r == 1) ? p0 : 0.0; },
-        [&](int r, const double2 *, const double *zr) { Xz.st(r, zr[0]); }, ub);
-    bwd_emit<BW, 0, 1>(n, uper, [&](int r, double2 *, double *zr) { zr[0] = Xz.ld(r); },
-        [&](int q, int r, const double2 (&)[1][2 * BW + 1], const double (&wr)[1][2 * BW + 1]) {
-          X1.st(q, mvr<BW>(tb.t0, q, r, wr[0]));  // phi_h (real part = imaginary part)
-          X2.st(q, mvr<BW>(tb.t2, q, r, wr[0]));  // D2 phi_h
-        },
-        [&](int r) {
-          pfr(Xz.p, r);
-          pfu(r);
-        });
-    lu_fwd<BW, 0, 1>(n, [&](int r, double *row, bool c) { vrow<BW>(tb, r, n, k2, row, c); },
-        [&](int r, double2 *, double *br) { br[0] = (r == 1 || r == n) ? 0.0 : X1.ld(r); },
-        [&](int r, const double2 *, const double *zr) { Xz.st(r, zr[0]); }, ub,
-        [&](int r) { pfr(X1.p, r); });
-    double dh1 = 0.0, dhn = 0.0;
-    bwd_emit<BW, 0, 1>(n, uper, [&](int r, double2 *, double *zr) { zr[0] = Xz.ld(r); },
-        [&](int q, int r, const double2 (&)[1][2 * BW + 1], const double (&wr)[1][2 * BW + 1]) {
-          const double vh = mvr<BW>(tb.t0, q, r, wr[0]), dvh = mvr<BW>(tb.t1, q, r, wr[0]);
-          X4.st(q, vh);
-          X5.st(q, dvh);
-          if (q == 1) dh1 = dvh;
-          if (q == n) dhn = dvh;
-        },
-        [&](int r) {
-          pfr(Xz.p, r);
-          pfu(r);
-        });
-    a.dv[2 * nm + m] = z2(dh1, dhn);
   }
 }
 
+// Role 2 of k_helmholtz: phi_p together with the unit-wall solution phi_h, then v_p together with
+// v_h.  The two pairs share their operators, so each pair runs as one profile LU (lu_fwd) with a
+// complex chain (the particular solution) and a real chain (the influence solution: phi_h and
+// v_h have equal real and imaginary parts), and one backward sweep.
+//   (alpha D0 - beta D2) phi_p = RK right-hand side,  same operator phi_h = p0 e_1
+//     (solve_v_f.f90:140-153, the LU of solve_g.f90:42-71);
+//   (D2 - k^2 D0) v_p = phi_p with the wall velocities at rows 1 and n, and v_h = phi_h with zero
+//     walls (solve_v_f.f90:202-272).
 template <int BW>
-__global__ void __launch_bounds__(kLanes * kRoles, 4) k_helmholtz(SplitArgs a) {
+__device__ __forceinline__ void helmholtz_phi_v(const SplitArgs &a, const Tabs<BW> &tb, int64_t m) {
+  const int n = a.ny, s = a.substep;
+  const int64_t nm = a.nmodes, ns = a.ns;
+  const double dt = *a.dt_ptr, nu = a.nu;
+  const double k2 = mode_k(a, m).k2;
+  auto hl = [&](int i) { return DLine{a.hl + i * ns + m, nm}; };
+  auto pfl = [&](const void *base, int r) {
+    pf_l1(reinterpret_cast<const double2 *>(base) + (r - 1) * (int)nm);
+  };
+  auto pfr = [&](const double *base, int r) { pf_l1(base + (r - 1) * (int)nm); };
+  const UBand<BW> ub = make_uband<BW>(a.ub + 2 * a.ub_role + m, nm, ns);
+  auto uper = [&](int r, int e) { return ub.get(r, e); };
+  auto pfu = [&](int r) {
+#pragma unroll
+    for (int e = 1; e <= BW; ++e) pf_l1(ub.p + (e - 1) * (int)ns + (r - 1) * (int)nm);
+  };
+  const DLine Zr{a.zl + 2 * ns + m, nm};
+  const RLine Xz{a.xr + m, nm}, X1{a.xr + ns + m, nm}, X2{a.xr + 2 * ns + m, nm};
+  const RLine X4{a.xr + 3 * ns + m, nm}, X5{a.xr + 4 * ns + m, nm};
+
+  const double beta = dt * rkc(2, s) * nu;
+  const double dummy = 1.0 + beta * k2;
+  const double p0 = dummy * trow<BW>(tb.t0, 1)[0] - beta * trow<BW>(tb.t2, 1)[0];  // A_g(1,1)
+  const DLine store{a.RK + ns + m, nm};
+  const DLine d2l = hl(H_DP);
+  auto hsum = [&](int r) { return zadd(hl(H_HV0).ld(r), zadd(hl(H_V2).ld(r), hl(H_V3).ld(r))); };
+  auto pfh = [&](int r) {
+    pfl(hl(H_HV0).p, r);
+    pfl(hl(H_V2).p, r);
+    pfl(hl(H_V3).p, r);
+  };
+  // RK right-hand side of phi (solve_v_f.f90:54-97 with solve_g.f90:84-123's form); walls zero
+  auto rhs = [&](int r) {
+    if (r == 1 || r == n) return z2(0.0, 0.0);
+    const double2 st = store.ld(r), h = hsum(r);
+    if (s == 1) {
+      const double alpha = dt * rkc(1, s) * nu, gamma = dt * rkc(3, s);
+      return zadd(zadd(zscale(1.0 - alpha * k2, st), zscale(gamma, h)), zscale(alpha, d2l.ld(r)));
+    }
+    return zadd(st, zscale(dt * rkc(3, s), h));
+  };
+  auto store_new = [&](double2 h, double2 f, double2 d2f) {
+    if (s == 3) return f;
+    const double alpha = dt * rkc(1, s + 1) * nu, zeta = dt * rkc(4, s + 1);
+    return zadd(zadd(zscale(zeta, h), zscale(1.0 - alpha * k2, f)), zscale(alpha, d2f));
+  };
+  lu_fwd<BW, 1, 1>(n, [&](int r, double *row, bool c) { helm_row<BW>(tb, r, n, dummy, beta, row, c); },
+      [&](int r, double2 *bc, double *br) {
+        bc[0] = rhs(r);
+        br[0] = (r == 1) ? p0 : 0.0;
+      },
+      [&](int r, const double2 *zc, const double *zr) {
+        Zr.st(r, zc[0]);
+        Xz.st(r, zr[0]);
+      },
+      ub,
+      [&](int r) {
+        pfl(store.p, r);
+        pfh(r);
+        if (s == 1) pfl(d2l.p, r);
+      });
+  const DLine out{a.zl + 4 * ns + m, nm};
+  bwd_emit<BW, 1, 1>(n, uper,
+      [&](int r, double2 *zc, double *zr) {
+        zc[0] = Zr.ld(r);
+        zr[0] = Xz.ld(r);
+      },
+      [&](int q, int r, const double2 (&wc)[1][2 * BW + 1], const double (&wr)[1][2 * BW + 1]) {
+        const double2 f = mvc<BW>(tb.t0, q, r, wc[0]), d2f = mvc<BW>(tb.t2, q, r, wc[0]);
+        out.st(q, f);
+        store.st(q, store_new(hsum(q), f, d2f));
+        X1.st(q, mvr<BW>(tb.t0, q, r, wr[0]));  // phi_h (real part = imaginary part)
+        X2.st(q, mvr<BW>(tb.t2, q, r, wr[0]));  // D2 phi_h
+      },
+      [&](int r) {
+        pfl(Zr.p, r);
+        pfr(Xz.p, r);
+        pfu(r);
+        const int q = r + BW;
+        if (r <= n - 2 * BW) {
+          pfh(q);
+          pfl(store.p, q);
+        }
+      });
+  // (D2 - k^2 D0) v = phi with v_p = the wall velocity at rows 1 and n, v_h = 0 there.
+  // Opposition control, the extension at the wall rows of the v solve (solve_v_f.f90:251-257,
+  // whose commented lines read vold): v at the walls = A * gain * v(+-y_d).  vold is field 10,
+  // v after the physical round trip (dft_x_realspace.f90:123), which has no kz Nyquist mode
+  // and, at kx = 0, only the Hermitian part (v(kz) + conj v(-kz)) / 2.
+  double2 vlo = z2(0.0, 0.0), vhi = z2(0.0, 0.0);
+  if (a.control_amp != 0.0) {
+    const int kzi = (int)(m / a.nxh), kxi = (int)(m - (int64_t)kzi * a.nxh);
+    if (kzi != a.nz / 2) {
+      vlo = a.vwall[m];
+      vhi = a.vwall[nm + m];
+      if (kxi == 0) {
+        const int64_t mp = (int64_t)((a.nz - kzi) % a.nz) * a.nxh;
+        const double2 pl = a.vwall[mp], ph = a.vwall[nm + mp];
+        vlo = z2(0.5 * (vlo.x + pl.x), 0.5 * (vlo.y - pl.y));
+        vhi = z2(0.5 * (vhi.x + ph.x), 0.5 * (vhi.y - ph.y));
+      }
+      const double gmul = a.control_amp * (double)__ldg(a.gains + m);
+      vlo = zscale(gmul, vlo);
+      vhi = zscale(gmul, vhi);
+    }
+  }
+  lu_fwd<BW, 1, 1>(n, [&](int r, double *row, bool c) { vrow<BW>(tb, r, n, k2, row, c); },
+      [&](int r, double2 *bc, double *br) {
+        const bool wall = (r == 1 || r == n);
+        bc[0] = (r == 1) ? vlo : (r == n) ? vhi : out.ld(r);
+        br[0] = wall ? 0.0 : X1.ld(r);
+      },
+      [&](int r, const double2 *zc, const double *zr) {
+        Zr.st(r, zc[0]);
+        Xz.st(r, zr[0]);
+      },
+      ub,
+      [&](int r) {
+        pfl(out.p, r);
+        pfr(X1.p, r);
+      });
+  const DLine Sv{a.S + ns + m, nm}, Sw{a.S + 2 * ns + m, nm};
+  double dh1 = 0.0, dhn = 0.0;
+  bwd_emit<BW, 1, 1>(n, uper,
+      [&](int r, double2 *zc, double *zr) {
+        zc[0] = Zr.ld(r);
+        zr[0] = Xz.ld(r);
+      },
+      [&](int q, int r, const double2 (&wc)[1][2 * BW + 1], const double (&wr)[1][2 * BW + 1]) {
+        const double2 vp = mvc<BW>(tb.t0, q, r, wc[0]), dvp = mvc<BW>(tb.t1, q, r, wc[0]);
+        Sv.st(q, vp);
+        Sw.st(q, dvp);
+        if (q == 1) a.dv[m] = dvp;
+        if (q == n) a.dv[nm + m] = dvp;
+        const double vh = mvr<BW>(tb.t0, q, r, wr[0]), dvh = mvr<BW>(tb.t1, q, r, wr[0]);
+        X4.st(q, vh);
+        X5.st(q, dvh);
+        if (q == 1) dh1 = dvh;
+        if (q == n) dhn = dvh;
+      },
+      [&](int r) {
+        pfl(Zr.p, r);
+        pfr(Xz.p, r);
+        pfu(r);
+      });
+  a.dv[2 * nm + m] = z2(dh1, dhn);
+}
+
+// Three roles per mode: theta, g, and phi with v (helmholtz_phi_v).
+constexpr int kHelmRoles = 3;
+
+template <int BW>
+__global__ void __launch_bounds__(kLanes * kHelmRoles, 4) k_helmholtz(SplitArgs a) {
   if (a.dsc->err) return;  // a failed dt update leaves the state untouched
   const int role = threadIdx.x / kLanes;
   const int64_t m = (int64_t)blockIdx.x * kLanes + (threadIdx.x % kLanes);
@@ -416,8 +496,7 @@ __global__ void __launch_bounds__(kLanes * kRoles, 4) k_helmholtz(SplitArgs a) {
   switch (role) {
     case 0: helmholtz_role<BW, 0>(a, tb, m); break;
     case 1: helmholtz_role<BW, 1>(a, tb, m); break;
-    case 2: helmholtz_role<BW, 2>(a, tb, m); break;
-    default: helmholtz_role<BW, 3>(a, tb, m); break;
+    default: helmholtz_phi_v<BW>(a, tb, m); break;
   }
 }
 
@@ -659,7 +738,7 @@ cudaError_t split_bw(Handle &h, int part, int substep, const double *dt_ptr, cud
     return cudaGetLastError();
   }
   if (part == 1) {
-    k_helmholtz<BW><<<blocks, kLanes * kRoles, 0, st>>>(a);
+    k_helmholtz<BW><<<blocks, kLanes * kHelmRoles, 0, st>>>(a);
     return cudaGetLastError();
   }
   const dim3 agrid((unsigned)((h.nmodes + 255) / 256), (unsigned)h.ny);
