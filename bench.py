@@ -468,6 +468,17 @@ def run_kmm(args):
     e2e_value = world * args.e2e_steps / (ms_e2e / 1e3)
     io_bytes = 4 * nspec * 16
 
+    # a statistics step (kmm_get_statistics: statistics, spectra, moments, pressure) of the
+    # current state, outputs left on the device; timed outside the step region
+    mixed.get_statistics(download=False)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(args.stat_calls):
+        mixed.get_statistics(download=False)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms_stat = max_over_ranks(e0.elapsed_time(e1), dist, device) / args.stat_calls
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline_quick(w)
@@ -507,6 +518,9 @@ def run_kmm(args):
         "e2e": {"value": e2e_value, "unit": "steps/s", "h2d_bytes_per_step": io_bytes,
                 "d2h_bytes_per_step": io_bytes,
                 "api": "kmm_step_host(rk = NULL): pinned host U (reference layout; u, v, w, theta) uploaded, RK_STORE rebuilt on the device as restart option 1 does, one RK3 step, U downloaded"},
+        "statistics": {"ms_per_call": ms_stat, "per_step_time": ms_stat / (ms_mixed / args.steps),
+                       "api": "kmm_get_statistics: the 58 stat-file lines, 2 x 18 spectra, U_c, T_c "
+                              "and the pressure of the current state (statistics step), on the device"},
         "gpu_launches": launches_per_step * args.steps,
         "clocks": clocks,
         "last_step": {"dt": out_m["dt"], "dpdx": out_m["phi_dpdx"][3], "tau_w": out_m["wall_shear_stress"],
@@ -533,6 +547,7 @@ def main(argv=None):
     ap.add_argument("--acc-steps", type=int, default=100)
     ap.add_argument("--prof-steps", type=int, default=5)
     ap.add_argument("--e2e-steps", type=int, default=20)
+    ap.add_argument("--stat-calls", type=int, default=5, help="statistics-step calls timed")
     ap.add_argument("--ref-planes", type=int, default=4, help="y-planes per worker in a reference step")
     ap.add_argument("--ref-rows", type=int, default=4, help="kz rows per worker in a reference step")
     ap.add_argument("--no-cpu-baseline", action="store_true")

@@ -1,12 +1,13 @@
 """A fixed number of RK3 steps of the benchmark workload on one handle, for profiler captures.
 
-    python -m channel_passive_b200.profile_case --steps 2 [--precision mixed|fp64] [--nx 192 ...]
+    python -m channel_passive_b200.profile_case --steps 2 [--stats 1] [--precision mixed|fp64] [--nx 192 ...]
 
 Creates one handle (about 2.5 GB of device memory at 192x129x192 mixed), sets the seeded
 random-phase initial condition, runs --warmup steps through the CUDA graph and then --steps
-steps kernel by kernel (kmm_profile_step), and prints the per-kernel mean device times.  Under a
-profiler the kernels of interest are selected by name (k_hvhg, k_helmholtz, k_assemble,
-k_zinv2, k_xphys2, k_zfwd2, k_mean).
+steps kernel by kernel (kmm_profile_step), and prints the per-kernel mean device times; then
+--stats statistics-step calls (kmm_get_statistics).  Under a profiler the kernels of interest
+are selected by name (k_hvhg, k_helmholtz, k_assemble, k_zinv2, k_xphys2, k_zfwd2, k_mean; for
+the statistics k_ydiff, k_mean_vv, k_ppe, k_spectra, k_mom_reduce, k_stat_lines).
 """
 from __future__ import annotations
 
@@ -28,6 +29,7 @@ def main(argv=None) -> int:
     ap.add_argument("--warmup", type=int, default=1)
     ap.add_argument("--precision", choices=("mixed", "fp64"), default="mixed")
     ap.add_argument("--no-control", action="store_true")
+    ap.add_argument("--stats", type=int, default=0)
     args = ap.parse_args(argv)
     prec = _lib.KMM_PREC_MIXED if args.precision == "mixed" else _lib.KMM_PREC_FP64
     cfg = Config(nx=args.nx, ny=args.ny, nz=args.nz, lmfx=2.0, lmfz=2.0 / 3.0, stretch=0.9,
@@ -40,7 +42,12 @@ def main(argv=None) -> int:
             ch.step(args.warmup)
         prof = ch.profile_step(args.steps)
         U, _ = ch.download_state()
+        st = None
+        for _ in range(args.stats):
+            st = ch.get_statistics()
     finite = bool(all(math.isfinite(abs(x)) for x in (U[0].sum(), U[1].sum(), U[2].sum(), U[6].sum())))
+    if st is not None:
+        finite = finite and all(math.isfinite(float(v.sum())) for v in st["lines"].values())
     print(json.dumps({"precision": args.precision, "steps": args.steps, "finite": finite,
                       "kernels_ms": {k: v["ms"] for k, v in prof.items()}}))
     return 0 if finite else 1

@@ -185,12 +185,16 @@ class Channel:
         check(self._lib.kmm_get_pressure(self._h, _dptr(P)))
         return P
 
-    def get_statistics(self, pressure: bool = False) -> dict:
+    def get_statistics(self, pressure: bool = False, download: bool = True) -> dict | None:
         """The statistics of a statistics step of the current state (kmm_get_statistics:
         get_statistics_1, write_spectra, the physical moments of dft_x_realspace and
         get_statistics_2).  Returns {"lines": {name: (ny,)}, "spec_kx": {name: (nxh, ny)},
         "spec_kz": {name: (nz, ny)}, "U_c", "T_c"} with the reference's dataset names (spectrum
-        "uu" is "Euu_kx" / "Euu_kz" there), plus "P" (nz, nxh, ny) when pressure is set."""
+        "uu" is "Euu_kx" / "Euu_kz" there), plus "P" (nz, nxh, ny) when pressure is set.
+        With download=False the numbers are computed and left on the device (None returned)."""
+        if not download:
+            check(self._lib.kmm_get_statistics(self._h, None, None, None, None, None))
+            return None
         cfg = self.config
         nl, nsp = _lib.KMM_STAT_NLINES, _lib.KMM_STAT_NSPEC
         lines = np.zeros((nl, cfg.ny))
