@@ -479,7 +479,8 @@ int kmm_create(const kmm_config *cfg, kmm_handle **out) {
   if ((rc = dalloc(*h, &h->zc, 8 * (size_t)h->ns))) return fail(rc);
   if ((rc = dalloc(*h, &h->ec, 9 * (size_t)h->ns))) return fail(rc);
   if ((rc = dalloc(*h, &h->xr, 6 * (size_t)h->ns))) return fail(rc);
-  if ((rc = dalloc(*h, &h->ub, 4 * (size_t)split_ub_role(*h)))) return fail(rc);
+  if ((rc = dalloc(*h, &h->ub, 3 * (size_t)split_ub_role(*h)))) return fail(rc);
+  if ((rc = dalloc(*h, &h->vf, (size_t)vop_factor_doubles(*h)))) return fail(rc);
   if ((rc = dalloc(*h, &h->dvw, 3 * (size_t)h->nmodes))) return fail(rc);
   if ((rc = dalloc(*h, &h->w00, 3 * (size_t)h->ny * (8 + 2 * h->bw)))) return fail(rc);
   if ((rc = dalloc(*h, &h->staging, 10 * h->ns))) return fail(rc);
@@ -511,6 +512,15 @@ int kmm_create(const kmm_config *cfg, kmm_handle **out) {
     set_error("kernel attribute set-up failed");
     return fail(KMM_ERR_CUDA);
   }
+  {
+    // the v operator depends on k^2 alone: factor it once for the run
+    cudaError_t e = launch_vop_factor(*h, h->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+    if (e != cudaSuccess) {
+      set_error(std::string("v operator factorisation failed: ") + cudaGetErrorString(e));
+      return fail(KMM_ERR_CUDA);
+    }
+  }
   *out = reinterpret_cast<kmm_handle *>(h);
   return KMM_OK;
 }
@@ -523,7 +533,7 @@ int kmm_destroy(kmm_handle *hh) {
   if (h->stream) cudaStreamSynchronize(h->stream);
   if (h->side) cudaStreamSynchronize(h->side);
   void *ptrs[] = {h->S, h->RK, h->P, h->MID, h->dops, h->gains, h->vwall, h->zc,
-                  h->ec, h->xr, h->ub, h->dvw, h->w00, h->staging, h->stat,
+                  h->ec, h->xr, h->ub, h->vf, h->dvw, h->w00, h->staging, h->stat,
                   h->fftpos, h->tw64, h->tw32, h->dsc};
   for (void *p : ptrs)
     if (p) cudaFree(p);

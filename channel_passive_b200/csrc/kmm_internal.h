@@ -92,7 +92,8 @@ struct Handle {
   double2 *zc = nullptr;                   // per-mode solver: forward lines  [8][ny][nmodes]
   double2 *ec = nullptr;                   //                  hvhg outputs   [9][ny][nmodes]
   double *xr = nullptr;                    //                  real lines     [6][ny][nmodes]
-  double *ub = nullptr;                    //                  U factors, 4 roles (split_ub_role each)
+  double *ub = nullptr;                    //                  U factors, 3 roles (split_ub_role each)
+  double *vf = nullptr;                    //                  v operator LU per mode (vop_factor_doubles)
   double2 *dvw = nullptr;                  //                  wall derivatives [3][nmodes]
   double *w00 = nullptr;                   // mean-mode lines (3 threads)
   double *stat = nullptr;                  // statistics buffers (stat_layout), made on first use
@@ -176,6 +177,11 @@ StatLayout stat_layout(const Handle &h);
 // The statistics of the state (stats.cu) into Handle::stat; uses the buffers of
 // launch_pressure plus ec and dvw as scratch and leaves the pressure planes in staging[0].
 cudaError_t launch_statistics(Handle &h, cudaStream_t st);
+// The v operator's profile LU per mode (wavespace_split.cu): doubles of its L part and of the
+// whole (L then U), and the kernel that fills it once per handle.
+int64_t vop_lband_doubles(const Handle &h);
+int64_t vop_factor_doubles(const Handle &h);
+cudaError_t launch_vop_factor(Handle &h, cudaStream_t st);
 // Doubles of U factor storage per solver role.
 int64_t split_ub_role(const Handle &h);
 

@@ -80,6 +80,30 @@ __device__ __forceinline__ UBand<BW> make_uband(double *base, int64_t s, int64_t
   return UBand<BW>{base, base + BW * es, s, es};
 }
 
+// Per-mode L factor of a profile LU kept for later forward sweeps, the UBand idea for L:
+// L(r, r-d) for d = 0..BW (d = 0 holds 1 / L(r, r)) as [BW+1][ny][mode], plus d = BW+1..2BW of
+// the last BW rows (the only rows that reach below r - BW) as [BW][BW][mode].
+// A region for one mode set holds (BW + 1) * es + BW * BW * s doubles.
+template <int BW>
+struct LBand {
+  double *p;   // [BW+1][ny][s]
+  double *px;  // [BW][BW][s], rows n-BW+1..n
+  int64_t s, es;
+  int n;
+  __device__ __forceinline__ double get(int r, int d) const {
+    if (d <= BW) return p[d * (int)es + (r - 1) * (int)s];
+    return r > n - BW ? px[((r - (n - BW) - 1) * BW + d - BW - 1) * (int)s] : 0.0;
+  }
+  __device__ __forceinline__ void set(int r, int d, double v) const {
+    if (d <= BW) p[d * (int)es + (r - 1) * (int)s] = v;
+    else if (r > n - BW) px[((r - (n - BW) - 1) * BW + d - BW - 1) * (int)s] = v;
+  }
+};
+template <int BW>
+__device__ __forceinline__ LBand<BW> make_lband(double *base, int64_t s, int64_t es, int n) {
+  return LBand<BW>{base, base + (BW + 1) * es, s, es, n};
+}
+
 template <int BW>
 __device__ __forceinline__ int row_lo(int r, int n) { return (r <= n - BW) ? (r - BW > 1 ? r - BW : 1) : n - 2 * BW; }
 template <int BW>
@@ -246,13 +270,15 @@ __device__ __forceinline__ void bwd_emit(int n, UF ufn, Zin zin, Emit emit, Pf p
 // row r and zc / zr receive the forward results; U goes to ust for the backward sweep.  Rows
 // 2BW+1..n-BW only touch U(p, p+e) with e <= BW of the last BW rows, which stay in a register
 // window; the first 2BW and last BW rows read U back from ust.
-template <int BW, int NC, int NR>
+// With KEEP_L, step() leaves row r's L (Lk[d] = L(r, r-d), Lk[0] = 1 / L(r, r)) in Lk.
+template <int BW, int NC, int NR, bool KEEP_L = false>
 struct LuSweep {
   static constexpr int W = 2 * BW;
   static constexpr int NCc = NC > 0 ? NC : 1, NRr = NR > 0 ? NR : 1;
   double2 wc[NCc][W];
   double wr[NRr][W];
   double Uw[BW][BW];  // Uw[dp-1][e-1] = U(r-dp, r-dp+e)
+  double Lk[KEEP_L ? W + 1 : 1];
   UBand<BW> ust;
   int n;
 
@@ -342,6 +368,10 @@ struct LuSweep {
 #pragma unroll
     for (int e = 0; e < BW; ++e) Uw[0][e] = Ur[e];
     const double rp = L[0];
+    if constexpr (KEEP_L) {
+#pragma unroll
+      for (int d = 0; d <= W; ++d) Lk[d] = L[d];
+    }
     // L(r, r-d) vanishes for d > BW above the last BW rows
     auto chain = [&]<int D>() {
 #pragma unroll
@@ -395,6 +425,70 @@ __device__ __forceinline__ void lu_fwd(int n, RowA rowA, In in, Out out, UBand<B
     double2 zc[NCc];
     double zr[NRr];
     lu.step(r, rowA, bc, br, zc, zr);
+    out(r, zc, zr);
+  }
+}
+
+// Forward substitution with a per-mode L kept by a KEEP_L LuSweep, for NC complex and NR real
+// chains, ascending (the arithmetic of LuSweep::step's chains).
+template <int BW, int NC, int NR, typename In, typename Out, typename Pf = NoPf>
+__device__ __forceinline__ void fwd_lband(const LBand<BW> &lb, int n, In in, Out out, Pf pf = Pf()) {
+  constexpr int W = 2 * BW;
+  constexpr int NCc = NC > 0 ? NC : 1, NRr = NR > 0 ? NR : 1;
+  double2 wc[NCc][W];
+  double wr[NRr][W];
+#pragma unroll
+  for (int k = 0; k < W; ++k) {
+#pragma unroll
+    for (int c = 0; c < NCc; ++c) wc[c][k] = z2(0.0, 0.0);
+#pragma unroll
+    for (int c = 0; c < NRr; ++c) wr[c][k] = 0.0;
+  }
+  for (int r = 1; r <= kPrefetchRows && r <= n; ++r) pf(r);
+  for (int r = 1; r <= n; ++r) {
+    if (r + kPrefetchRows <= n) pf(r + kPrefetchRows);
+    double2 bc[NCc];
+    double br[NRr];
+    in(r, bc, br);
+    double2 zc[NCc];
+    double zr[NRr];
+    const double rp = lb.get(r, 0);
+    auto chain = [&]<int D>() {
+      double L[D + 1];
+#pragma unroll
+      for (int d = 1; d <= D; ++d) L[d] = lb.get(r, d);
+#pragma unroll
+      for (int c = 0; c < NC; ++c) {
+        double2 acc = bc[c];
+#pragma unroll
+        for (int d = 1; d <= D; ++d) {
+          acc.x -= L[d] * wc[c][W - d].x;
+          acc.y -= L[d] * wc[c][W - d].y;
+        }
+        zc[c] = z2(acc.x * rp, acc.y * rp);
+      }
+#pragma unroll
+      for (int c = 0; c < NR; ++c) {
+        double acc = br[c];
+#pragma unroll
+        for (int d = 1; d <= D; ++d) acc -= L[d] * wr[c][W - d];
+        zr[c] = acc * rp;
+      }
+    };
+    if (r <= n - BW) chain.template operator()<BW>();
+    else chain.template operator()<W>();
+#pragma unroll
+    for (int c = 0; c < NC; ++c) {
+#pragma unroll
+      for (int k = 0; k < W - 1; ++k) wc[c][k] = wc[c][k + 1];
+      wc[c][W - 1] = zc[c];
+    }
+#pragma unroll
+    for (int c = 0; c < NR; ++c) {
+#pragma unroll
+      for (int k = 0; k < W - 1; ++k) wr[c][k] = wr[c][k + 1];
+      wr[c][W - 1] = zr[c];
+    }
     out(r, zc, zr);
   }
 }

@@ -56,7 +56,7 @@ struct SplitArgs {
   double2 *zl;       // [8][ny][nm] role-private forward lines
   double2 *hl;       // [H_COUNT][ny][nm] hvhg outputs
   double *xr;        // [6][ny][nm] real lines of role 3
-  double *ub;        // [4][ub_role] per-role U factors
+  double *ub;        // [3][ub_role] per-role U factors
   int64_t ub_role;   // doubles per role
   double2 *dv;       // [3][nm] dv_p(1), dv_p(n), (dv_h(1), dv_h(n))
   const double *tabs;   // t0, t1, t2, l0, u0
@@ -67,6 +67,8 @@ struct SplitArgs {
   double nu, pr, lmfxr, lmfzr;
   DevScalars *dsc;
   const double *dt_ptr;
+  double *vf;        // the v operator's profile LU per mode: LBand, then UBand at vf + vf_l
+  int64_t vf_l;
 };
 
 template <typename PT> __device__ __forceinline__ double2 ldp(const PT *p);
@@ -441,7 +443,10 @@ __device__ __forceinline__ void helmholtz_phi_v(const SplitArgs &a, const Tabs<B
       vhi = zscale(gmul, vhi);
     }
   }
-  lu_fwd<BW, 1, 1>(n, [&](int r, double *row, bool c) { vrow<BW>(tb, r, n, k2, row, c); },
+  // the v operator does not change during a run: its factors come from k_vop_factor
+  const LBand<BW> vl = make_lband<BW>(a.vf + m, nm, ns, n);
+  const UBand<BW> vu = make_uband<BW>(a.vf + a.vf_l + m, nm, ns);
+  fwd_lband<BW, 1, 1>(vl, n,
       [&](int r, double2 *bc, double *br) {
         const bool wall = (r == 1 || r == n);
         bc[0] = (r == 1) ? vlo : (r == n) ? vhi : out.ld(r);
@@ -451,14 +456,15 @@ __device__ __forceinline__ void helmholtz_phi_v(const SplitArgs &a, const Tabs<B
         Zr.st(r, zc[0]);
         Xz.st(r, zr[0]);
       },
-      ub,
       [&](int r) {
         pfl(out.p, r);
         pfr(X1.p, r);
+#pragma unroll
+        for (int d = 0; d <= BW; ++d) pf_l1(vl.p + d * (int)ns + (r - 1) * (int)nm);
       });
   const DLine Sv{a.S + ns + m, nm}, Sw{a.S + 2 * ns + m, nm};
   double dh1 = 0.0, dhn = 0.0;
-  bwd_emit<BW, 1, 1>(n, uper,
+  bwd_emit<BW, 1, 1>(n, [&](int r, int e) { return vu.get(r, e); },
       [&](int r, double2 *zc, double *zr) {
         zc[0] = Zr.ld(r);
         zr[0] = Xz.ld(r);
@@ -478,9 +484,32 @@ __device__ __forceinline__ void helmholtz_phi_v(const SplitArgs &a, const Tabs<B
       [&](int r) {
         pfl(Zr.p, r);
         pfr(Xz.p, r);
-        pfu(r);
+#pragma unroll
+        for (int e = 1; e <= BW; ++e) pf_l1(vu.p + (e - 1) * (int)ns + (r - 1) * (int)nm);
       });
   a.dv[2 * nm + m] = z2(dh1, dhn);
+}
+
+// The profile LU of the v operator (D2 - k^2 D0 with Dirichlet first and last rows, the matrix
+// of solve_v_f.f90:202-231) of every mode, once per handle: it depends on k^2 alone.  Same
+// LuSweep arithmetic as a per-substep factorisation, so the factors are the same numbers.
+template <int BW>
+__global__ void __launch_bounds__(128) k_vop_factor(SplitArgs a) {
+  const int64_t m = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (m >= a.nmodes) return;
+  const int n = a.ny;
+  const Tabs<BW> tb = tabs_at<BW>(a.tabs, n);
+  const double k2 = mode_k(a, m).k2;
+  const LBand<BW> lb = make_lband<BW>(a.vf + m, a.nmodes, a.ns, n);
+  LuSweep<BW, 0, 0, true> lu;
+  lu.init(n, make_uband<BW>(a.vf + a.vf_l + m, a.nmodes, a.ns));
+  for (int r = 1; r <= n; ++r) {
+    double2 bc[1] = {z2(0.0, 0.0)}, zc[1];
+    double br[1] = {0.0}, zr[1];
+    lu.step(r, [&](int rr, double *row, bool c) { vrow<BW>(tb, rr, n, k2, row, c); }, bc, br, zc, zr);
+#pragma unroll
+    for (int d = 0; d <= 2 * BW; ++d) lb.set(r, d, lu.Lk[d]);
+  }
 }
 
 // Three roles per mode: theta, g, and phi with v (helmholtz_phi_v).
@@ -702,6 +731,8 @@ cudaError_t split_bw(Handle &h, int part, int substep, const double *dt_ptr, cud
   a.lmfzr = h.lmfzr;
   a.dsc = h.dsc;
   a.dt_ptr = dtp;
+  a.vf = h.vf;
+  a.vf_l = vop_lband_doubles(h);
 
   MeanArgs ma;
   ma.ny = h.ny;
@@ -763,6 +794,37 @@ cudaError_t split_part(Handle &h, int part, int substep, const double *dt_ptr, c
 
 int64_t split_ub_role(const Handle &h) {
   return (int64_t)h.bw * h.ns + (int64_t)h.bw * h.bw * h.nmodes;
+}
+
+int64_t vop_lband_doubles(const Handle &h) {
+  return (int64_t)(h.bw + 1) * h.ns + (int64_t)h.bw * h.bw * h.nmodes;
+}
+
+int64_t vop_factor_doubles(const Handle &h) { return vop_lband_doubles(h) + split_ub_role(h); }
+
+cudaError_t launch_vop_factor(Handle &h, cudaStream_t st) {
+  SplitArgs a{};
+  a.ny = h.ny;
+  a.nxh = h.nxh;
+  a.nz = h.nz;
+  a.nmodes = h.nmodes;
+  a.ns = h.ns;
+  a.tabs = h.dops + ops_offsets(h.bw, h.ny).t0;
+  a.lmfxr = h.lmfxr;
+  a.lmfzr = h.lmfzr;
+  a.vf = h.vf;
+  a.vf_l = vop_lband_doubles(h);
+  const unsigned blocks = (unsigned)((h.nmodes + 127) / 128);
+  switch (h.bw) {
+    case 2: k_vop_factor<2><<<blocks, 128, 0, st>>>(a); break;
+    case 3: k_vop_factor<3><<<blocks, 128, 0, st>>>(a); break;
+    case 4: k_vop_factor<4><<<blocks, 128, 0, st>>>(a); break;
+    case 5: k_vop_factor<5><<<blocks, 128, 0, st>>>(a); break;
+    case 6: k_vop_factor<6><<<blocks, 128, 0, st>>>(a); break;
+    case 7: k_vop_factor<7><<<blocks, 128, 0, st>>>(a); break;
+    default: return cudaErrorInvalidValue;
+  }
+  return cudaGetLastError();
 }
 
 cudaError_t launch_ws_hvhg(Handle &h, int substep, const double *dt_ptr, cudaStream_t st) {
