@@ -38,6 +38,42 @@ namespace kmm {
 #endif
 constexpr int kPrefetchRows = KMM_PREFETCH_ROWS;
 
+// cp.async copies global -> shared that bypass registers, tracked in per-thread commit groups.
+__device__ __forceinline__ void cp_async16(void *sdst, const void *gsrc) {
+  const unsigned sa = (unsigned)__cvta_generic_to_shared(sdst);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(sa), "l"(gsrc) : "memory");
+}
+__device__ __forceinline__ void cp_async8(void *sdst, const void *gsrc) {
+  const unsigned sa = (unsigned)__cvta_generic_to_shared(sdst);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(sa), "l"(gsrc) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
+// Steps of look-ahead of an asynchronously staged sweep, and its ring slots.
+constexpr int kStageAhead = 2;
+constexpr int kStageSlots = kStageAhead + 1;
+
+// A thread-private ring in shared memory of kStageSlots slots x K 16-byte units, interleaved
+// across the block's nt threads (unit (slot, k) of thread t at smem[(slot * K + k) * nt + t]):
+// the rows one sweep step reads, copied in by cp.async kStageAhead steps before that step.
+// Slots are indexed by the sweep step (the row being eliminated), so a step's inputs may come
+// from other rows (the emission rows q = r + BW of a backward sweep).
+template <int K>
+struct Ring {
+  double2 *base;  // this thread's column: smem + threadIdx.x
+  int nt;
+  __device__ __forceinline__ double2 *at(int step, int k) const { return base + ((step % kStageSlots) * K + k) * nt; }
+  __device__ __forceinline__ void get(int step, int k, const double2 *g) const { cp_async16(at(step, k), g); }
+  __device__ __forceinline__ void get(int step, int k, const float2 *g) const { cp_async8(at(step, k), g); }
+  __device__ __forceinline__ void get(int step, int k, const double *g) const { cp_async8(at(step, k), g); }
+  __device__ __forceinline__ double2 c(int step, int k) const { return *at(step, k); }
+  __device__ __forceinline__ double d(int step, int k) const { return *reinterpret_cast<const double *>(at(step, k)); }
+};
+
 __device__ __forceinline__ void pf_l1(const void *p) {
   if constexpr (kPrefetchRows > 0) {
 #ifdef KMM_PREFETCH_L2
@@ -161,7 +197,10 @@ struct NoPf {
   __device__ __forceinline__ void operator()(int) const {}
 };
 
-template <int BW, int NC, typename In, typename Out, typename Pf = NoPf>
+// Every sweep runs pf(r) PF steps before step r reads row r's inputs.  With ASYNC, pf issues
+// cp.async copies: each step commits one group (possibly empty) and waits for the group of the
+// current step, so PF groups stay in flight.
+template <int BW, int NC, int PF = kPrefetchRows, bool ASYNC = false, typename In, typename Out, typename Pf = NoPf>
 __device__ __forceinline__ void fwd_fixed(const Tabs<BW> &tb, int n, In in, Out out, Pf pf = Pf()) {
   constexpr int W = 2 * BW;
   double2 w[NC][W];
@@ -169,9 +208,16 @@ __device__ __forceinline__ void fwd_fixed(const Tabs<BW> &tb, int n, In in, Out 
   for (int c = 0; c < NC; ++c)
 #pragma unroll
     for (int k = 0; k < W; ++k) w[c][k] = z2(0.0, 0.0);
-  for (int r = 1; r <= kPrefetchRows && r <= n; ++r) pf(r);
+  for (int r = 1; r <= PF; ++r) {
+    if (r <= n) pf(r);
+    if constexpr (ASYNC) cp_async_commit();
+  }
   for (int r = 1; r <= n; ++r) {
-    if (r + kPrefetchRows <= n) pf(r + kPrefetchRows);
+    if (r + PF <= n) pf(r + PF);
+    if constexpr (ASYNC) {
+      cp_async_commit();
+      cp_async_wait<PF>();
+    }
     double2 b[NC];
     in(r, b);
     const double *L = tb.l0 + (r - 1) * (W + 1);
@@ -205,7 +251,8 @@ __device__ __forceinline__ void fwd_fixed(const Tabs<BW> &tb, int n, In in, Out 
 
 // Backward substitution (unit U given by ufn(r, e)) for NC complex and NR real chains,
 // descending, with mat-vec emission: emit(q, r, wc, wr) where wc[c][j] = x_{r+j}.
-template <int BW, int NC, int NR, typename UF, typename Zin, typename Emit, typename Pf = NoPf>
+template <int BW, int NC, int NR, int PF = kPrefetchRows, bool ASYNC = false, typename UF, typename Zin,
+          typename Emit, typename Pf = NoPf>
 __device__ __forceinline__ void bwd_emit(int n, UF ufn, Zin zin, Emit emit, Pf pf = Pf()) {
   constexpr int W = 2 * BW + 1;
   constexpr int NCc = NC > 0 ? NC : 1, NRr = NR > 0 ? NR : 1;
@@ -218,9 +265,16 @@ __device__ __forceinline__ void bwd_emit(int n, UF ufn, Zin zin, Emit emit, Pf p
 #pragma unroll
     for (int c = 0; c < NRr; ++c) wr[c][j] = 0.0;
   }
-  for (int r = n; r > n - kPrefetchRows && r >= 1; --r) pf(r);
+  for (int r = n; r > n - PF; --r) {
+    if (r >= 1) pf(r);
+    if constexpr (ASYNC) cp_async_commit();
+  }
   for (int r = n; r >= 1; --r) {
-    if (r - kPrefetchRows >= 1) pf(r - kPrefetchRows);
+    if (r - PF >= 1) pf(r - PF);
+    if constexpr (ASYNC) {
+      cp_async_commit();
+      cp_async_wait<PF>();
+    }
 #pragma unroll
     for (int j = W - 1; j >= 1; --j) {
 #pragma unroll
@@ -411,14 +465,22 @@ struct LuSweep {
 
 // The LuSweep over rows 1..n: in(r, bc, br) supplies row r's right-hand sides, out(r, zc, zr)
 // receives the forward results.
-template <int BW, int NC, int NR, typename RowA, typename In, typename Out, typename Pf = NoPf>
+template <int BW, int NC, int NR, int PF = kPrefetchRows, bool ASYNC = false, typename RowA, typename In,
+          typename Out, typename Pf = NoPf>
 __device__ __forceinline__ void lu_fwd(int n, RowA rowA, In in, Out out, UBand<BW> ust, Pf pf = Pf()) {
   constexpr int NCc = NC > 0 ? NC : 1, NRr = NR > 0 ? NR : 1;
   LuSweep<BW, NC, NR> lu;
   lu.init(n, ust);
-  for (int r = 1; r <= kPrefetchRows && r <= n; ++r) pf(r);
+  for (int r = 1; r <= PF; ++r) {
+    if (r <= n) pf(r);
+    if constexpr (ASYNC) cp_async_commit();
+  }
   for (int r = 1; r <= n; ++r) {
-    if (r + kPrefetchRows <= n) pf(r + kPrefetchRows);
+    if (r + PF <= n) pf(r + PF);
+    if constexpr (ASYNC) {
+      cp_async_commit();
+      cp_async_wait<PF>();
+    }
     double2 bc[NCc];
     double br[NRr];
     in(r, bc, br);
@@ -430,9 +492,11 @@ __device__ __forceinline__ void lu_fwd(int n, RowA rowA, In in, Out out, UBand<B
 }
 
 // Forward substitution with a per-mode L kept by a KEEP_L LuSweep, for NC complex and NR real
-// chains, ascending (the arithmetic of LuSweep::step's chains).
-template <int BW, int NC, int NR, typename In, typename Out, typename Pf = NoPf>
-__device__ __forceinline__ void fwd_lband(const LBand<BW> &lb, int n, In in, Out out, Pf pf = Pf()) {
+// chains, ascending (the arithmetic of LuSweep::step's chains); lget(r, d) = L(r, r-d), d = 0
+// giving 1 / L(r, r).
+template <int BW, int NC, int NR, int PF = kPrefetchRows, bool ASYNC = false, typename LGet, typename In,
+          typename Out, typename Pf = NoPf>
+__device__ __forceinline__ void fwd_lband(LGet lget, int n, In in, Out out, Pf pf = Pf()) {
   constexpr int W = 2 * BW;
   constexpr int NCc = NC > 0 ? NC : 1, NRr = NR > 0 ? NR : 1;
   double2 wc[NCc][W];
@@ -444,19 +508,26 @@ __device__ __forceinline__ void fwd_lband(const LBand<BW> &lb, int n, In in, Out
 #pragma unroll
     for (int c = 0; c < NRr; ++c) wr[c][k] = 0.0;
   }
-  for (int r = 1; r <= kPrefetchRows && r <= n; ++r) pf(r);
+  for (int r = 1; r <= PF; ++r) {
+    if (r <= n) pf(r);
+    if constexpr (ASYNC) cp_async_commit();
+  }
   for (int r = 1; r <= n; ++r) {
-    if (r + kPrefetchRows <= n) pf(r + kPrefetchRows);
+    if (r + PF <= n) pf(r + PF);
+    if constexpr (ASYNC) {
+      cp_async_commit();
+      cp_async_wait<PF>();
+    }
     double2 bc[NCc];
     double br[NRr];
     in(r, bc, br);
     double2 zc[NCc];
     double zr[NRr];
-    const double rp = lb.get(r, 0);
+    const double rp = lget(r, 0);
     auto chain = [&]<int D>() {
       double L[D + 1];
 #pragma unroll
-      for (int d = 1; d <= D; ++d) L[d] = lb.get(r, d);
+      for (int d = 1; d <= D; ++d) L[d] = lget(r, d);
 #pragma unroll
       for (int c = 0; c < NC; ++c) {
         double2 acc = bc[c];

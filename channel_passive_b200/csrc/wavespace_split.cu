@@ -248,23 +248,22 @@ __global__ void __launch_bounds__(kLanes * kRoles, 4) k_hvhg(SplitArgs a) {
 }
 
 // ------------------------------------------------------------------------------------------
-// k_helmholtz
+// k_helmholtz.  Every sweep stages the rows it reads through a thread-private shared-memory ring
+// (Ring, cp.async kStageAhead steps ahead): the kernel's 12 warps per SM would need more L1 than
+// there is to keep prefetched lines until use.  Units per step: kHelmUnits<BW>.
+template <int BW>
+constexpr int kHelmUnits = 5 + BW;
+
 template <int BW, int ROLE>
-__device__ __forceinline__ void helmholtz_role(const SplitArgs &a, const Tabs<BW> &tb, int64_t m) {
+__device__ __forceinline__ void helmholtz_role(const SplitArgs &a, const Tabs<BW> &tb, int64_t m,
+                                               const Ring<kHelmUnits<BW>> &ring) {
   const int n = a.ny, s = a.substep;
   const int64_t nm = a.nmodes, ns = a.ns;
   const double dt = *a.dt_ptr, nu = a.nu;
   const double k2 = mode_k(a, m).k2;
   auto hl = [&](int i) { return DLine{a.hl + i * ns + m, nm}; };
-  auto pfl = [&](const void *base, int r) {
-    pf_l1(reinterpret_cast<const double2 *>(base) + (r - 1) * (int)nm);
-  };
+  auto row = [&](const auto *base, int r) { return base + (r - 1) * (int)nm; };
   const UBand<BW> ub = make_uband<BW>(a.ub + ROLE * a.ub_role + m, nm, ns);
-  auto uper = [&](int r, int e) { return ub.get(r, e); };
-  auto pfu = [&](int r) {  // the U row a backward step reads
-#pragma unroll
-    for (int e = 1; e <= BW; ++e) pf_l1(ub.p + (e - 1) * (int)ns + (r - 1) * (int)nm);
-  };
   const DLine Zr{a.zl + ROLE * ns + m, nm};
 
   // RK right-hand side (solve_g.f90:84-123): rows 1 and n are the Dirichlet rows (zero)
@@ -283,49 +282,52 @@ __device__ __forceinline__ void helmholtz_role(const SplitArgs &a, const Tabs<BW
     return zadd(zadd(zscale(zeta, h), zscale(1.0 - alpha * k2, f)), zscale(alpha, d2f));
   };
 
-  {
-    // one complex Helmholtz solve: theta (role 0), g (role 1)
-    const double visc = ROLE == 0 ? nu / a.pr : nu;
-    const double beta = dt * rkc(2, s) * visc;
-    const double dummy = 1.0 + beta * k2;
-    const int sslot = ROLE == 0 ? 2 : 0;
-    const DLine store{a.RK + sslot * ns + m, nm};
-    const DLine d2l = hl(ROLE == 0 ? H_DT : H_DG);
-    auto hsum = [&](int r) {
-      if constexpr (ROLE == 0) return hl(H_HT).ld(r);
-      else return zadd(hl(H_G2).ld(r), hl(H_G3).ld(r));
-    };
-    auto pfh = [&](int r) {
-      if constexpr (ROLE == 0) pfl(hl(H_HT).p, r);
-      else { pfl(hl(H_G2).p, r); pfl(hl(H_G3).p, r); }
-    };
-    lu_fwd<BW, 1, 0>(n, [&](int r, double *row, bool c) { helm_row<BW>(tb, r, n, dummy, beta, row, c); },
-        [&](int r, double2 *bc, double *) {
-          bc[0] = rhs(store.ld(r), hsum(r), s == 1 ? d2l.ld(r) : z2(0.0, 0.0), visc, r);
-        },
-        [&](int r, const double2 *zc, const double *) { Zr.st(r, zc[0]); }, ub,
-        [&](int r) {
-          pfl(store.p, r);
-          pfh(r);
-          if (s == 1) pfl(d2l.p, r);
-        });
-    const DLine out{ROLE == 0 ? a.S + 3 * ns + m : a.S + m, nm};
-    bwd_emit<BW, 1, 0>(n, uper, [&](int r, double2 *zc, double *) { zc[0] = Zr.ld(r); },
-        [&](int q, int r, const double2 (&wc)[1][2 * BW + 1], const double (&)[1][2 * BW + 1]) {
-          const double2 f = mvc<BW>(tb.t0, q, r, wc[0]), d2f = mvc<BW>(tb.t2, q, r, wc[0]);
-          out.st(q, f);
-          store.st(q, store_new(hsum(q), f, d2f, visc));
-        },
-        [&](int r) {
-          pfl(Zr.p, r);
-          pfu(r);
-          const int q = r + BW;
-          if (r <= n - 2 * BW) {
-            pfh(q);
-            pfl(store.p, q);
-          }
-        });
-  }
+  // one complex Helmholtz solve: theta (role 0, h = HT), g (role 1, h = G2 + G3)
+  const double visc = ROLE == 0 ? nu / a.pr : nu;
+  const double beta = dt * rkc(2, s) * visc;
+  const double dummy = 1.0 + beta * k2;
+  const int sslot = ROLE == 0 ? 2 : 0;
+  const DLine store{a.RK + sslot * ns + m, nm};
+  const DLine d2l = hl(ROLE == 0 ? H_DT : H_DG);
+  const double2 *hA = hl(ROLE == 0 ? H_HT : H_G2).p, *hB = hl(H_G3).p;
+  auto hsum = [&](int r) {
+    if constexpr (ROLE == 0) return hl(H_HT).ld(r);
+    else return zadd(hl(H_G2).ld(r), hl(H_G3).ld(r));
+  };
+  // forward units: 0 store, 1 hA, 2 hB, 3 D2 store (substep 1)
+  lu_fwd<BW, 1, 0, kStageAhead, true>(n, [&](int r, double *rw, bool c) { helm_row<BW>(tb, r, n, dummy, beta, rw, c); },
+      [&](int r, double2 *bc, double *) {
+        const double2 h = ROLE == 0 ? ring.c(r, 1) : zadd(ring.c(r, 1), ring.c(r, 2));
+        bc[0] = rhs(ring.c(r, 0), h, s == 1 ? ring.c(r, 3) : z2(0.0, 0.0), visc, r);
+      },
+      [&](int r, const double2 *zc, const double *) { Zr.st(r, zc[0]); }, ub,
+      [&](int r) {
+        ring.get(r, 0, row(store.p, r));
+        ring.get(r, 1, row(hA, r));
+        if (ROLE == 1) ring.get(r, 2, row(hB, r));
+        if (s == 1) ring.get(r, 3, row(d2l.p, r));
+      });
+  // backward units: 0 Z(r), 1..BW U(r, e), BW+1 hA(q), BW+2 hB(q) with q = r + BW
+  const DLine out{ROLE == 0 ? a.S + 3 * ns + m : a.S + m, nm};
+  bwd_emit<BW, 1, 0, kStageAhead, true>(n, [&](int r, int e) { return e <= BW ? ring.d(r, e) : ub.get(r, e); },
+      [&](int r, double2 *zc, double *) { zc[0] = ring.c(r, 0); },
+      [&](int q, int r, const double2 (&wc)[1][2 * BW + 1], const double (&)[1][2 * BW + 1]) {
+        const double2 f = mvc<BW>(tb.t0, q, r, wc[0]), d2f = mvc<BW>(tb.t2, q, r, wc[0]);
+        out.st(q, f);
+        double2 h;
+        if (q == r + BW) h = ROLE == 0 ? ring.c(r, BW + 1) : zadd(ring.c(r, BW + 1), ring.c(r, BW + 2));
+        else h = hsum(q);
+        store.st(q, store_new(h, f, d2f, visc));
+      },
+      [&](int r) {
+        ring.get(r, 0, row(Zr.p, r));
+#pragma unroll
+        for (int e = 1; e <= BW; ++e) ring.get(r, e, ub.p + (e - 1) * (int)ns + (r - 1) * (int)nm);
+        if (r <= n - 2 * BW) {
+          ring.get(r, BW + 1, row(hA, r + BW));
+          if (ROLE == 1) ring.get(r, BW + 2, row(hB, r + BW));
+        }
+      });
 }
 
 // Role 2 of k_helmholtz: phi_p together with the unit-wall solution phi_h, then v_p together with
@@ -337,22 +339,15 @@ __device__ __forceinline__ void helmholtz_role(const SplitArgs &a, const Tabs<BW
 //   (D2 - k^2 D0) v_p = phi_p with the wall velocities at rows 1 and n, and v_h = phi_h with zero
 //     walls (solve_v_f.f90:202-272).
 template <int BW>
-__device__ __forceinline__ void helmholtz_phi_v(const SplitArgs &a, const Tabs<BW> &tb, int64_t m) {
+__device__ __forceinline__ void helmholtz_phi_v(const SplitArgs &a, const Tabs<BW> &tb, int64_t m,
+                                                const Ring<kHelmUnits<BW>> &ring) {
   const int n = a.ny, s = a.substep;
   const int64_t nm = a.nmodes, ns = a.ns;
   const double dt = *a.dt_ptr, nu = a.nu;
   const double k2 = mode_k(a, m).k2;
   auto hl = [&](int i) { return DLine{a.hl + i * ns + m, nm}; };
-  auto pfl = [&](const void *base, int r) {
-    pf_l1(reinterpret_cast<const double2 *>(base) + (r - 1) * (int)nm);
-  };
-  auto pfr = [&](const double *base, int r) { pf_l1(base + (r - 1) * (int)nm); };
+  auto row = [&](const auto *base, int r) { return base + (r - 1) * (int)nm; };
   const UBand<BW> ub = make_uband<BW>(a.ub + 2 * a.ub_role + m, nm, ns);
-  auto uper = [&](int r, int e) { return ub.get(r, e); };
-  auto pfu = [&](int r) {
-#pragma unroll
-    for (int e = 1; e <= BW; ++e) pf_l1(ub.p + (e - 1) * (int)ns + (r - 1) * (int)nm);
-  };
   const DLine Zr{a.zl + 2 * ns + m, nm};
   const RLine Xz{a.xr + m, nm}, X1{a.xr + ns + m, nm}, X2{a.xr + 2 * ns + m, nm};
   const RLine X4{a.xr + 3 * ns + m, nm}, X5{a.xr + 4 * ns + m, nm};
@@ -362,19 +357,14 @@ __device__ __forceinline__ void helmholtz_phi_v(const SplitArgs &a, const Tabs<B
   const double p0 = dummy * trow<BW>(tb.t0, 1)[0] - beta * trow<BW>(tb.t2, 1)[0];  // A_g(1,1)
   const DLine store{a.RK + ns + m, nm};
   const DLine d2l = hl(H_DP);
+  const double2 *h0 = hl(H_HV0).p, *h1 = hl(H_V2).p, *h2 = hl(H_V3).p;
   auto hsum = [&](int r) { return zadd(hl(H_HV0).ld(r), zadd(hl(H_V2).ld(r), hl(H_V3).ld(r))); };
-  auto pfh = [&](int r) {
-    pfl(hl(H_HV0).p, r);
-    pfl(hl(H_V2).p, r);
-    pfl(hl(H_V3).p, r);
-  };
   // RK right-hand side of phi (solve_v_f.f90:54-97 with solve_g.f90:84-123's form); walls zero
-  auto rhs = [&](int r) {
+  auto rhs = [&](double2 st, double2 h, double2 d2, int r) {
     if (r == 1 || r == n) return z2(0.0, 0.0);
-    const double2 st = store.ld(r), h = hsum(r);
     if (s == 1) {
       const double alpha = dt * rkc(1, s) * nu, gamma = dt * rkc(3, s);
-      return zadd(zadd(zscale(1.0 - alpha * k2, st), zscale(gamma, h)), zscale(alpha, d2l.ld(r)));
+      return zadd(zadd(zscale(1.0 - alpha * k2, st), zscale(gamma, h)), zscale(alpha, d2));
     }
     return zadd(st, zscale(dt * rkc(3, s), h));
   };
@@ -383,9 +373,11 @@ __device__ __forceinline__ void helmholtz_phi_v(const SplitArgs &a, const Tabs<B
     const double alpha = dt * rkc(1, s + 1) * nu, zeta = dt * rkc(4, s + 1);
     return zadd(zadd(zscale(zeta, h), zscale(1.0 - alpha * k2, f)), zscale(alpha, d2f));
   };
-  lu_fwd<BW, 1, 1>(n, [&](int r, double *row, bool c) { helm_row<BW>(tb, r, n, dummy, beta, row, c); },
+  // phi forward units: 0 store, 1..3 HV0, V2, V3, 4 D2 store (substep 1)
+  lu_fwd<BW, 1, 1, kStageAhead, true>(n, [&](int r, double *rw, bool c) { helm_row<BW>(tb, r, n, dummy, beta, rw, c); },
       [&](int r, double2 *bc, double *br) {
-        bc[0] = rhs(r);
+        const double2 h = zadd(ring.c(r, 1), zadd(ring.c(r, 2), ring.c(r, 3)));
+        bc[0] = rhs(ring.c(r, 0), h, s == 1 ? ring.c(r, 4) : z2(0.0, 0.0), r);
         br[0] = (r == 1) ? p0 : 0.0;
       },
       [&](int r, const double2 *zc, const double *zr) {
@@ -394,31 +386,37 @@ __device__ __forceinline__ void helmholtz_phi_v(const SplitArgs &a, const Tabs<B
       },
       ub,
       [&](int r) {
-        pfl(store.p, r);
-        pfh(r);
-        if (s == 1) pfl(d2l.p, r);
+        ring.get(r, 0, row(store.p, r));
+        ring.get(r, 1, row(h0, r));
+        ring.get(r, 2, row(h1, r));
+        ring.get(r, 3, row(h2, r));
+        if (s == 1) ring.get(r, 4, row(d2l.p, r));
       });
+  // phi backward units: 0 Z(r), 1 Xz(r), 2..BW+1 U(r, e), BW+2..BW+4 HV0, V2, V3 at q = r + BW
   const DLine out{a.zl + 4 * ns + m, nm};
-  bwd_emit<BW, 1, 1>(n, uper,
+  bwd_emit<BW, 1, 1, kStageAhead, true>(n, [&](int r, int e) { return e <= BW ? ring.d(r, 1 + e) : ub.get(r, e); },
       [&](int r, double2 *zc, double *zr) {
-        zc[0] = Zr.ld(r);
-        zr[0] = Xz.ld(r);
+        zc[0] = ring.c(r, 0);
+        zr[0] = ring.d(r, 1);
       },
       [&](int q, int r, const double2 (&wc)[1][2 * BW + 1], const double (&wr)[1][2 * BW + 1]) {
         const double2 f = mvc<BW>(tb.t0, q, r, wc[0]), d2f = mvc<BW>(tb.t2, q, r, wc[0]);
         out.st(q, f);
-        store.st(q, store_new(hsum(q), f, d2f));
+        const double2 h = (q == r + BW) ? zadd(ring.c(r, BW + 2), zadd(ring.c(r, BW + 3), ring.c(r, BW + 4)))
+                                        : hsum(q);
+        store.st(q, store_new(h, f, d2f));
         X1.st(q, mvr<BW>(tb.t0, q, r, wr[0]));  // phi_h (real part = imaginary part)
         X2.st(q, mvr<BW>(tb.t2, q, r, wr[0]));  // D2 phi_h
       },
       [&](int r) {
-        pfl(Zr.p, r);
-        pfr(Xz.p, r);
-        pfu(r);
-        const int q = r + BW;
+        ring.get(r, 0, row(Zr.p, r));
+        ring.get(r, 1, row(Xz.p, r));
+#pragma unroll
+        for (int e = 1; e <= BW; ++e) ring.get(r, 1 + e, ub.p + (e - 1) * (int)ns + (r - 1) * (int)nm);
         if (r <= n - 2 * BW) {
-          pfh(q);
-          pfl(store.p, q);
+          ring.get(r, BW + 2, row(h0, r + BW));
+          ring.get(r, BW + 3, row(h1, r + BW));
+          ring.get(r, BW + 4, row(h2, r + BW));
         }
       });
   // (D2 - k^2 D0) v = phi with v_p = the wall velocity at rows 1 and n, v_h = 0 there.
@@ -446,28 +444,30 @@ __device__ __forceinline__ void helmholtz_phi_v(const SplitArgs &a, const Tabs<B
   // the v operator does not change during a run: its factors come from k_vop_factor
   const LBand<BW> vl = make_lband<BW>(a.vf + m, nm, ns, n);
   const UBand<BW> vu = make_uband<BW>(a.vf + a.vf_l + m, nm, ns);
-  fwd_lband<BW, 1, 1>(vl, n,
+  // v forward units: 0 phi_p(r), 1 phi_h(r), 2..BW+2 L(r, r-d) for d = 0..BW
+  fwd_lband<BW, 1, 1, kStageAhead, true>([&](int r, int d) { return d <= BW ? ring.d(r, 2 + d) : vl.get(r, d); }, n,
       [&](int r, double2 *bc, double *br) {
         const bool wall = (r == 1 || r == n);
-        bc[0] = (r == 1) ? vlo : (r == n) ? vhi : out.ld(r);
-        br[0] = wall ? 0.0 : X1.ld(r);
+        bc[0] = (r == 1) ? vlo : (r == n) ? vhi : ring.c(r, 0);
+        br[0] = wall ? 0.0 : ring.d(r, 1);
       },
       [&](int r, const double2 *zc, const double *zr) {
         Zr.st(r, zc[0]);
         Xz.st(r, zr[0]);
       },
       [&](int r) {
-        pfl(out.p, r);
-        pfr(X1.p, r);
+        ring.get(r, 0, row(out.p, r));
+        ring.get(r, 1, row(X1.p, r));
 #pragma unroll
-        for (int d = 0; d <= BW; ++d) pf_l1(vl.p + d * (int)ns + (r - 1) * (int)nm);
+        for (int d = 0; d <= BW; ++d) ring.get(r, 2 + d, vl.p + d * (int)ns + (r - 1) * (int)nm);
       });
+  // v backward units: 0 Z(r), 1 Xz(r), 2..BW+1 U(r, e)
   const DLine Sv{a.S + ns + m, nm}, Sw{a.S + 2 * ns + m, nm};
   double dh1 = 0.0, dhn = 0.0;
-  bwd_emit<BW, 1, 1>(n, [&](int r, int e) { return vu.get(r, e); },
+  bwd_emit<BW, 1, 1, kStageAhead, true>(n, [&](int r, int e) { return e <= BW ? ring.d(r, 1 + e) : vu.get(r, e); },
       [&](int r, double2 *zc, double *zr) {
-        zc[0] = Zr.ld(r);
-        zr[0] = Xz.ld(r);
+        zc[0] = ring.c(r, 0);
+        zr[0] = ring.d(r, 1);
       },
       [&](int q, int r, const double2 (&wc)[1][2 * BW + 1], const double (&wr)[1][2 * BW + 1]) {
         const double2 vp = mvc<BW>(tb.t0, q, r, wc[0]), dvp = mvc<BW>(tb.t1, q, r, wc[0]);
@@ -482,10 +482,10 @@ __device__ __forceinline__ void helmholtz_phi_v(const SplitArgs &a, const Tabs<B
         if (q == n) dhn = dvh;
       },
       [&](int r) {
-        pfl(Zr.p, r);
-        pfr(Xz.p, r);
+        ring.get(r, 0, row(Zr.p, r));
+        ring.get(r, 1, row(Xz.p, r));
 #pragma unroll
-        for (int e = 1; e <= BW; ++e) pf_l1(vu.p + (e - 1) * (int)ns + (r - 1) * (int)nm);
+        for (int e = 1; e <= BW; ++e) ring.get(r, 1 + e, vu.p + (e - 1) * (int)ns + (r - 1) * (int)nm);
       });
   a.dv[2 * nm + m] = z2(dh1, dhn);
 }
@@ -516,16 +516,23 @@ __global__ void __launch_bounds__(128) k_vop_factor(SplitArgs a) {
 constexpr int kHelmRoles = 3;
 
 template <int BW>
+constexpr size_t helm_smem() {
+  return sizeof(double2) * (size_t)kStageSlots * kHelmUnits<BW> * kLanes * kHelmRoles;
+}
+
+template <int BW>
 __global__ void __launch_bounds__(kLanes * kHelmRoles, 4) k_helmholtz(SplitArgs a) {
+  extern __shared__ double2 helm_ring[];
   if (a.dsc->err) return;  // a failed dt update leaves the state untouched
   const int role = threadIdx.x / kLanes;
   const int64_t m = (int64_t)blockIdx.x * kLanes + (threadIdx.x % kLanes);
   if (m == 0 || m >= a.nmodes) return;
   const Tabs<BW> tb = tabs_at<BW>(a.tabs, a.ny);
+  const Ring<kHelmUnits<BW>> ring{helm_ring + threadIdx.x, (int)blockDim.x};
   switch (role) {
-    case 0: helmholtz_role<BW, 0>(a, tb, m); break;
-    case 1: helmholtz_role<BW, 1>(a, tb, m); break;
-    default: helmholtz_phi_v<BW>(a, tb, m); break;
+    case 0: helmholtz_role<BW, 0>(a, tb, m, ring); break;
+    case 1: helmholtz_role<BW, 1>(a, tb, m, ring); break;
+    default: helmholtz_phi_v<BW>(a, tb, m, ring); break;
   }
 }
 
@@ -769,7 +776,7 @@ cudaError_t split_bw(Handle &h, int part, int substep, const double *dt_ptr, cud
     return cudaGetLastError();
   }
   if (part == 1) {
-    k_helmholtz<BW><<<blocks, kLanes * kHelmRoles, 0, st>>>(a);
+    k_helmholtz<BW><<<blocks, kLanes * kHelmRoles, helm_smem<BW>(), st>>>(a);
     return cudaGetLastError();
   }
   const dim3 agrid((unsigned)((h.nmodes + 255) / 256), (unsigned)h.ny);
@@ -815,6 +822,21 @@ cudaError_t launch_vop_factor(Handle &h, cudaStream_t st) {
   a.vf = h.vf;
   a.vf_l = vop_lband_doubles(h);
   const unsigned blocks = (unsigned)((h.nmodes + 127) / 128);
+  // the Helmholtz kernel's staging ring may exceed the default 48 KB of dynamic shared memory
+  auto ring_smem = [](auto kern, size_t bytes) {
+    return cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+  };
+  cudaError_t e = cudaSuccess;
+  switch (h.bw) {
+    case 2: e = ring_smem(k_helmholtz<2>, helm_smem<2>()); break;
+    case 3: e = ring_smem(k_helmholtz<3>, helm_smem<3>()); break;
+    case 4: e = ring_smem(k_helmholtz<4>, helm_smem<4>()); break;
+    case 5: e = ring_smem(k_helmholtz<5>, helm_smem<5>()); break;
+    case 6: e = ring_smem(k_helmholtz<6>, helm_smem<6>()); break;
+    case 7: e = ring_smem(k_helmholtz<7>, helm_smem<7>()); break;
+    default: break;
+  }
+  if (e != cudaSuccess) return e;
   switch (h.bw) {
     case 2: k_vop_factor<2><<<blocks, 128, 0, st>>>(a); break;
     case 3: k_vop_factor<3><<<blocks, 128, 0, st>>>(a); break;
