@@ -54,7 +54,7 @@ __device__ __forceinline__ void cp_async_wait() {
 }
 
 // Steps of look-ahead of an asynchronously staged sweep, and its ring slots.
-constexpr int kStageAhead = 2;
+constexpr int kStageAhead = 1;
 constexpr int kStageSlots = kStageAhead + 1;
 
 // A thread-private ring in shared memory of kStageSlots slots x K 16-byte units, interleaved
@@ -72,6 +72,10 @@ struct Ring {
   __device__ __forceinline__ void get(int step, int k, const double *g) const { cp_async8(at(step, k), g); }
   __device__ __forceinline__ double2 c(int step, int k) const { return *at(step, k); }
   __device__ __forceinline__ double d(int step, int k) const { return *reinterpret_cast<const double *>(at(step, k)); }
+  __device__ __forceinline__ double2 f(int step, int k) const {  // a float2 unit, widened
+    const float2 v = *reinterpret_cast<const float2 *>(at(step, k));
+    return make_double2((double)v.x, (double)v.y);
+  }
 };
 
 __device__ __forceinline__ void pf_l1(const void *p) {

@@ -132,9 +132,20 @@ __device__ __forceinline__ void vrow(const Tabs<BW> &tb, int r, int n, double k2
 }
 
 // ------------------------------------------------------------------------------------------
-// k_hvhg: role ROLE of mode m; NC = 2 adds the store's D0 solve at substep 1.
+// k_hvhg: role ROLE of mode m; NC = 2 adds the store's D0 solve at substep 1.  The sweeps stage
+// their rows through a shared-memory ring (Ring, cp.async kStageAhead steps ahead) of
+// kHvhgUnits units per step.
+constexpr int kHvhgUnits = 5;
+
+template <typename PT>
+__device__ __forceinline__ double2 ring_prod(const Ring<kHvhgUnits> &ring, int step, int k) {
+  if constexpr (sizeof(PT) == sizeof(float2)) return ring.f(step, k);
+  else return ring.c(step, k);
+}
+
 template <int BW, typename PT, int ROLE, int NC>
-__device__ __forceinline__ void hvhg_role(const SplitArgs &a, const Tabs<BW> &tb, int64_t m) {
+__device__ __forceinline__ void hvhg_role(const SplitArgs &a, const Tabs<BW> &tb, int64_t m,
+                                          const Ring<kHvhgUnits> &ring) {
   const int n = a.ny;
   const int64_t nm = a.nmodes, ns = a.ns;
   const ModeK k = mode_k(a, m);
@@ -142,7 +153,8 @@ __device__ __forceinline__ void hvhg_role(const SplitArgs &a, const Tabs<BW> &tb
   const double kxkz = kx * kz, kx2 = kx * kx, kz2 = kz * kz;
   const PT *P = reinterpret_cast<const PT *>(a.P) + m;
   auto prod = [&](int slot, int r) { return ldp<PT>(P + slot * ns + (r - 1) * (int)nm); };
-  auto pfp = [&](int slot, int r) { pf_l1(P + slot * ns + (r - 1) * (int)nm); };
+  auto prow = [&](int slot, int r) { return P + slot * ns + (r - 1) * (int)nm; };
+  auto rp = [&](int step, int u) { return ring_prod<PT>(ring, step, u); };
   const DLine Z0{a.zl + (2 * ROLE) * ns + m, nm}, Z1{a.zl + (2 * ROLE + 1) * ns + m, nm};
   constexpr int store_slot = ROLE == 0 ? 1 : ROLE == 1 ? 2 : 0;  // RK_STORE 2, 3, 1
   constexpr int d2_line = ROLE == 0 ? H_DP : ROLE == 1 ? H_DT : H_DG;
@@ -156,58 +168,66 @@ __device__ __forceinline__ void hvhg_role(const SplitArgs &a, const Tabs<BW> &tb
   const DLine Sv{a.S + ns + m, nm};
   double2 plo = z2(0.0, 0.0), phi = z2(0.0, 0.0);
 
-  fwd_fixed<BW, NC>(tb, n,
+  // forward units: role 0 f1, f3, f5 at 0..2; roles 1-3 their product at 0 (role 3's v at 1);
+  // the store (NC = 2) at 3
+  fwd_fixed<BW, NC, kStageAhead, true>(tb, n,
       [&](int r, double2 *b) {
         if constexpr (ROLE == 0) {
-          const double2 f1 = prod(0, r), f3 = prod(2, r), f5 = prod(4, r);
+          const double2 f1 = rp(r, 0), f3 = rp(r, 1), f5 = rp(r, 2);
           b[0] = zsub(zsub(zscale(-kx2, f1), zscale(2.0 * kxkz, f5)), zscale(kz2, f3));
-        } else if constexpr (ROLE == 1) {
-          b[0] = prod(6, r);
-        } else if constexpr (ROLE == 2) {
-          b[0] = prod(1, r);
-        } else {
-          b[0] = prod(3, r);
+        } else if constexpr (ROLE == 3) {
+          b[0] = rp(r, 0);
           if (probe) {
-            const double2 v = Sv.ld(r);
+            const double2 v = ring.c(r, 1);
             plo = zadd(plo, zscale(__ldg(a.wlo + r - 1), v));
             phi = zadd(phi, zscale(__ldg(a.whi + r - 1), v));
           }
+        } else {
+          b[0] = rp(r, 0);
         }
-        if constexpr (NC == 2) b[1] = Rs.ld(r);
+        if constexpr (NC == 2) b[1] = ring.c(r, 3);
       },
       [&](int r, const double2 *z) {
         Z0.st(r, z[0]);
         if constexpr (NC == 2) Z1.st(r, z[1]);
       },
       [&](int r) {
-        if constexpr (ROLE == 0) { pfp(0, r); pfp(2, r); pfp(4, r); }
-        else pfp(ROLE == 1 ? 6 : ROLE == 2 ? 1 : 3, r);
-        if constexpr (NC == 2) pf_l1(Rs.p + (r - 1) * (int)nm);
-        if (probe) pf_l1(Sv.p + (r - 1) * (int)nm);
+        if constexpr (ROLE == 0) {
+          ring.get(r, 0, prow(0, r));
+          ring.get(r, 1, prow(2, r));
+          ring.get(r, 2, prow(4, r));
+        } else {
+          ring.get(r, 0, prow(ROLE == 1 ? 6 : ROLE == 2 ? 1 : 3, r));
+        }
+        if constexpr (NC == 2) ring.get(r, 3, Rs.p + (r - 1) * (int)nm);
+        if (probe) ring.get(r, 1, Sv.p + (r - 1) * (int)nm);
       });
   if (probe) {
     a.vwall[m] = plo;
     a.vwall[nm + m] = phi;
   }
 
-  bwd_emit<BW, NC, 0>(n, ufix,
+  // backward units: Z0 at 0, Z1 (NC = 2) at 1, the emission's products at q = r + BW from 2
+  bwd_emit<BW, NC, 0, kStageAhead, true>(n, ufix,
       [&](int r, double2 *zc, double *) {
-        zc[0] = Z0.ld(r);
-        if constexpr (NC == 2) zc[1] = Z1.ld(r);
+        zc[0] = ring.c(r, 0);
+        if constexpr (NC == 2) zc[1] = ring.c(r, 1);
       },
       [&](int q, int r, const double2 (&wc)[NC][2 * BW + 1], const double (&)[1][2 * BW + 1]) {
+        const bool st = (q == r + BW);
         if constexpr (ROLE == 0) {
           const double c2i = kx * kx * kx + kx * (kz * kz), c4i = (kx * kx) * kz + kz * kz * kz;
-          const double2 f2 = prod(1, q), f4 = prod(3, q);
+          const double2 f2 = st ? rp(r, 2) : prod(1, q), f4 = st ? rp(r, 3) : prod(3, q);
           const double2 ehv = z2(-c2i * f2.y - c4i * f4.y, c2i * f2.x + c4i * f4.x);
           hl(H_HV0).st(q, zadd(ehv, mvc<BW>(tb.t1, q, r, wc[0])));
         } else if constexpr (ROLE == 1) {
-          const double2 f7 = prod(5, q), f9 = prod(7, q);
+          const double2 f7 = st ? rp(r, 2) : prod(5, q), f9 = st ? rp(r, 3) : prod(7, q);
           const double2 t7 = z2(-kx * f7.y - kz * f9.y, kx * f7.x + kz * f9.x);
           const double2 t = zadd(t7, mvc<BW>(tb.t1, q, r, wc[0]));
           hl(H_HT).st(q, z2(-t.x, -t.y));
         } else if constexpr (ROLE == 2) {
-          const double2 f1 = prod(0, q), f3 = prod(2, q), f5 = prod(4, q);
+          const double2 f1 = st ? rp(r, 2) : prod(0, q), f3 = st ? rp(r, 3) : prod(2, q);
+          const double2 f5 = st ? rp(r, 4) : prod(4, q);
           const double2 a1 = zadd(zscale(kxkz, zsub(f1, f3)), zscale(kz2 - kx2, f5));
           const double2 d1 = mvc<BW>(tb.t1, q, r, wc[0]), d2 = mvc<BW>(tb.t2, q, r, wc[0]);
           hl(H_G2).st(q, zadd(a1, z2(kz * d1.y, -kz * d1.x)));
@@ -220,30 +240,42 @@ __device__ __forceinline__ void hvhg_role(const SplitArgs &a, const Tabs<BW> &tb
         if constexpr (NC == 2) hl(d2_line).st(q, mvc<BW>(tb.t2, q, r, wc[NC - 1]));
       },
       [&](int r) {
-        pf_l1(Z0.p + (r - 1) * (int)nm);
-        if constexpr (NC == 2) pf_l1(Z1.p + (r - 1) * (int)nm);
+        ring.get(r, 0, Z0.p + (r - 1) * (int)nm);
+        if constexpr (NC == 2) ring.get(r, 1, Z1.p + (r - 1) * (int)nm);
         if (r <= n - 2 * BW) {
           const int q = r + BW;
-          if constexpr (ROLE == 0) { pfp(1, q); pfp(3, q); }
-          else if constexpr (ROLE == 1) { pfp(5, q); pfp(7, q); }
-          else if constexpr (ROLE == 2) { pfp(0, q); pfp(2, q); pfp(4, q); }
+          if constexpr (ROLE == 0) {
+            ring.get(r, 2, prow(1, q));
+            ring.get(r, 3, prow(3, q));
+          } else if constexpr (ROLE == 1) {
+            ring.get(r, 2, prow(5, q));
+            ring.get(r, 3, prow(7, q));
+          } else if constexpr (ROLE == 2) {
+            ring.get(r, 2, prow(0, q));
+            ring.get(r, 3, prow(2, q));
+            ring.get(r, 4, prow(4, q));
+          }
         }
       });
 }
 
+constexpr size_t hvhg_smem() { return sizeof(double2) * (size_t)kStageSlots * kHvhgUnits * kLanes * kRoles; }
+
 template <int BW, typename PT>
 __global__ void __launch_bounds__(kLanes * kRoles, 4) k_hvhg(SplitArgs a) {
+  extern __shared__ double2 hvhg_ring[];
   if (a.dsc->err) return;
   const int role = threadIdx.x / kLanes;
   const int64_t m = (int64_t)blockIdx.x * kLanes + (threadIdx.x % kLanes);
   if (m == 0 || m >= a.nmodes) return;
   const Tabs<BW> tb = tabs_at<BW>(a.tabs, a.ny);
+  const Ring<kHvhgUnits> ring{hvhg_ring + threadIdx.x, (int)blockDim.x};
   const bool s1 = a.substep == 1;
   switch (role) {
-    case 0: s1 ? hvhg_role<BW, PT, 0, 2>(a, tb, m) : hvhg_role<BW, PT, 0, 1>(a, tb, m); break;
-    case 1: s1 ? hvhg_role<BW, PT, 1, 2>(a, tb, m) : hvhg_role<BW, PT, 1, 1>(a, tb, m); break;
-    case 2: s1 ? hvhg_role<BW, PT, 2, 2>(a, tb, m) : hvhg_role<BW, PT, 2, 1>(a, tb, m); break;
-    default: hvhg_role<BW, PT, 3, 1>(a, tb, m); break;
+    case 0: s1 ? hvhg_role<BW, PT, 0, 2>(a, tb, m, ring) : hvhg_role<BW, PT, 0, 1>(a, tb, m, ring); break;
+    case 1: s1 ? hvhg_role<BW, PT, 1, 2>(a, tb, m, ring) : hvhg_role<BW, PT, 1, 1>(a, tb, m, ring); break;
+    case 2: s1 ? hvhg_role<BW, PT, 2, 2>(a, tb, m, ring) : hvhg_role<BW, PT, 2, 1>(a, tb, m, ring); break;
+    default: hvhg_role<BW, PT, 3, 1>(a, tb, m, ring); break;
   }
 }
 
@@ -771,8 +803,8 @@ cudaError_t split_bw(Handle &h, int part, int substep, const double *dt_ptr, cud
     else k_mean<BW, double2><<<1, 32, 0, h.side>>>(ma);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
     if ((e = cudaEventRecord(h.ev_join, h.side)) != cudaSuccess) return e;
-    if (h.mixed) k_hvhg<BW, float2><<<blocks, kLanes * kRoles, 0, st>>>(a);
-    else k_hvhg<BW, double2><<<blocks, kLanes * kRoles, 0, st>>>(a);
+    if (h.mixed) k_hvhg<BW, float2><<<blocks, kLanes * kRoles, hvhg_smem(), st>>>(a);
+    else k_hvhg<BW, double2><<<blocks, kLanes * kRoles, hvhg_smem(), st>>>(a);
     return cudaGetLastError();
   }
   if (part == 1) {
