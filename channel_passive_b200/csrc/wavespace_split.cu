@@ -660,6 +660,7 @@ __global__ void k_mean(MeanArgs a) {
         pf_l1(P + (r - 1) * (int)a.nmodes);
         pf_l1(store.p + (r - 1) * (int)a.nmodes);
       });
+  auto pfw = [&](const DLine &l, int r) { pf_l1(l.p + (r - 1)); };
   bwd_emit<BW, 2, 0>(n, ufix,
       [&](int r, double2 *zc, double *) { zc[0] = Zf.ld(r); zc[1] = Zs.ld(r); },
       [&](int q, int r, const double2 (&wc)[2][2 * BW + 1], const double (&)[1][2 * BW + 1]) {
@@ -675,17 +676,30 @@ __global__ void k_mean(MeanArgs a) {
         }
         // wave00.f90:169-173: zero wall rows, interior real part + u_gal, imaginary part 1
         R.st(q, (q == 1 || q == n) ? z2(0.0, 0.0) : z2(b.x + gal, 1.0));
+      },
+      [&](int r) {
+        pfw(Zf, r);
+        pfw(Zs, r);
+        if (r <= n - 2 * BW) pf_l1(store.p + (r + BW - 1) * (int)a.nmodes);
       });
   // (D0 - beta D2) c = rhs, Dirichlet rows
   const double beta = dt * rkc(2, s) * visc;
   lu_fwd<BW, 1, 0>(n, [&](int r, double *row, bool c) { helm_row<BW>(tb, r, n, 1.0, beta, row, c); },
       [&](int r, double2 *bc, double *) { bc[0] = R.ld(r); },
-      [&](int r, const double2 *zc, const double *) { R.st(r, zc[0]); }, ub);
-  {  // backward substitution storing the coefficients (the integral needs all of them)
+      [&](int r, const double2 *zc, const double *) { R.st(r, zc[0]); }, ub, [&](int r) { pfw(R, r); });
+  // backward substitution storing the coefficients; the integral (LABS_integration) runs along,
+  // summed from row n down
+  double2 integral = z2(0.0, 0.0);
+  {
     double2 w[2 * BW + 1];
 #pragma unroll
     for (int j = 0; j <= 2 * BW; ++j) w[j] = z2(0.0, 0.0);
     for (int r = n; r >= 1; --r) {
+      if (r > kPrefetchRows) {
+        pfw(R, r - kPrefetchRows);
+#pragma unroll
+        for (int e = 1; e <= BW; ++e) pf_l1(ub.p + (e - 1) * (int)n + (r - kPrefetchRows - 1));
+      }
 #pragma unroll
       for (int j = 2 * BW; j >= 1; --j) w[j] = w[j - 1];
       double2 acc = R.ld(r);
@@ -697,27 +711,26 @@ __global__ void k_mean(MeanArgs a) {
       }
       w[0] = acc;
       R.st(r, acc);
+      integral = zadd(integral, zscale(__ldg(a.integ + r - 1), acc));
     }
   }
-  double2 integral = z2(0.0, 0.0);
-  for (int i = 1; i <= n; ++i) integral = zadd(integral, zscale(__ldg(a.integ + i - 1), R.ld(i)));  // LABS_integration
   double phi = (bulk - 0.5 * integral.x) / (0.5 * integral.y);  // calculate_phi
   if (line == 1) phi = 0.0;                                       // wave00.f90:396
-  // c = Re c + phi Im c (real); mean profile D0 c, store alpha' D2 c + profile - zeta' d
-  for (int r = 1; r <= n; ++r) {
+  // c = Re c + phi Im c (real), formed where it is read: the wall stresses and the last sweep
+  auto creal = [&](int r) {
     const double2 c = R.ld(r);
-    Zf.st(r, z2(c.x + phi * c.y, 0.0));
-  }
+    return c.x + phi * c.y;
+  };
   if (s == 3) {
     const double *r1 = trow<BW>(tb.t1, 1), *rn = trow<BW>(tb.t1, n);
-    const double wall = r1[0] * Zf.ld(1).x + r1[1] * Zf.ld(2).x - rn[-1] * Zf.ld(n - 1).x - rn[0] * Zf.ld(n).x;
+    const double wall = r1[0] * creal(1) + r1[1] * creal(2) - rn[-1] * creal(n - 1) - rn[0] * creal(n);
     if (line == 0) a.dsc->wall_shear_stress = 0.5 * a.nu * wall;
     if (line == 2) a.dsc->wall_theta_stress = 0.5 * a.nu / a.pr * wall;
   }
   if (line == 0) a.dsc->phi_dpdx[s - 1] = phi;
   if (line == 2) a.dsc->phi_dtdx[s - 1] = phi;
   bwd_emit<BW, 1, 0>(n, [&](int, int) { return 0.0; },
-      [&](int r, double2 *zc, double *) { zc[0] = Zf.ld(r); },
+      [&](int r, double2 *zc, double *) { zc[0] = z2(creal(r), 0.0); },
       [&](int q, int r, const double2 (&wc)[1][2 * BW + 1], const double (&)[1][2 * BW + 1]) {
         double2 prof = mvc<BW>(tb.t0, q, r, wc[0]);
         prof.x -= gal;
@@ -729,7 +742,10 @@ __global__ void k_mean(MeanArgs a) {
           store.st(q, prof);
         }
       },
-      [&](int r) { pf_l1(store.p + (r - 1) * (int)a.nmodes); });
+      [&](int r) {
+        pfw(R, r);
+        if (r <= n - 2 * BW) pfw(DF, r + BW);
+      });
   if (line == 1) {  // v mean = 0 (wave00.f90:462)
     const DLine Sv{a.S + ns, a.nmodes};
     for (int r = 1; r <= n; ++r) Sv.st(r, z2(0.0, 0.0));
