@@ -38,6 +38,10 @@ namespace {
 constexpr int kLanes = 32;  // modes per block; one warp per role
 constexpr int kRoles = 4;
 
+// Lines k_hvhg hands to k_helmholtz.  The six nonlinear-term lines H_HV0..H_V3 are combinations
+// of the products and are stored at the products' precision PT (float2 in the mixed path, packed
+// at (PT *)hl + i * ns); the substep-1 lines H_DP, H_DT, H_DG (D2 D0^{-1} of the FP64 RK stores)
+// stay double2 at hl + i * ns.
 enum HLine { H_HV0 = 0, H_HT, H_G2, H_V2, H_G3, H_V3, H_DP, H_DT, H_DG, H_COUNT };
 
 // Low-storage RK3 coefficients alpha, beta, gamma, zeta of substeps 1-3
@@ -132,20 +136,9 @@ __device__ __forceinline__ void vrow(const Tabs<BW> &tb, int r, int n, double k2
 }
 
 // ------------------------------------------------------------------------------------------
-// k_hvhg: role ROLE of mode m; NC = 2 adds the store's D0 solve at substep 1.  The sweeps stage
-// their rows through a shared-memory ring (Ring, cp.async kStageAhead steps ahead) of
-// kHvhgUnits units per step.
-constexpr int kHvhgUnits = 5;
-
-template <typename PT>
-__device__ __forceinline__ double2 ring_prod(const Ring<kHvhgUnits> &ring, int step, int k) {
-  if constexpr (sizeof(PT) == sizeof(float2)) return ring.f(step, k);
-  else return ring.c(step, k);
-}
-
+// k_hvhg: role ROLE of mode m; NC = 2 adds the store's D0 solve at substep 1.
 template <int BW, typename PT, int ROLE, int NC>
-__device__ __forceinline__ void hvhg_role(const SplitArgs &a, const Tabs<BW> &tb, int64_t m,
-                                          const Ring<kHvhgUnits> &ring) {
+__device__ __forceinline__ void hvhg_role(const SplitArgs &a, const Tabs<BW> &tb, int64_t m) {
   const int n = a.ny;
   const int64_t nm = a.nmodes, ns = a.ns;
   const ModeK k = mode_k(a, m);
@@ -153,13 +146,13 @@ __device__ __forceinline__ void hvhg_role(const SplitArgs &a, const Tabs<BW> &tb
   const double kxkz = kx * kz, kx2 = kx * kx, kz2 = kz * kz;
   const PT *P = reinterpret_cast<const PT *>(a.P) + m;
   auto prod = [&](int slot, int r) { return ldp<PT>(P + slot * ns + (r - 1) * (int)nm); };
-  auto prow = [&](int slot, int r) { return P + slot * ns + (r - 1) * (int)nm; };
-  auto rp = [&](int step, int u) { return ring_prod<PT>(ring, step, u); };
+  auto pfp = [&](int slot, int r) { pf_l1(P + slot * ns + (r - 1) * (int)nm); };
   const DLine Z0{a.zl + (2 * ROLE) * ns + m, nm}, Z1{a.zl + (2 * ROLE + 1) * ns + m, nm};
   constexpr int store_slot = ROLE == 0 ? 1 : ROLE == 1 ? 2 : 0;  // RK_STORE 2, 3, 1
   constexpr int d2_line = ROLE == 0 ? H_DP : ROLE == 1 ? H_DT : H_DG;
   const DLine Rs{a.RK + store_slot * ns + m, nm};
   auto hl = [&](int i) { return DLine{a.hl + i * ns + m, nm}; };
+  auto hv = [&](int i) { return Line<PT>{reinterpret_cast<PT *>(a.hl) + i * ns + m, nm}; };
   auto ufix = [&](int r, int e) { return tb.u0[(r - 1) * 2 * BW + e - 1]; };
   // Role 3 also probes the wall-normal velocity at the detection planes for opposition
   // control: v(+-y_d) = w . v over the substep's starting v, with the precomputed weights
@@ -168,114 +161,94 @@ __device__ __forceinline__ void hvhg_role(const SplitArgs &a, const Tabs<BW> &tb
   const DLine Sv{a.S + ns + m, nm};
   double2 plo = z2(0.0, 0.0), phi = z2(0.0, 0.0);
 
-  // forward units: role 0 f1, f3, f5 at 0..2; roles 1-3 their product at 0 (role 3's v at 1);
-  // the store (NC = 2) at 3
-  fwd_fixed<BW, NC, kStageAhead, true>(tb, n,
+  fwd_fixed<BW, NC>(tb, n,
       [&](int r, double2 *b) {
         if constexpr (ROLE == 0) {
-          const double2 f1 = rp(r, 0), f3 = rp(r, 1), f5 = rp(r, 2);
+          const double2 f1 = prod(0, r), f3 = prod(2, r), f5 = prod(4, r);
           b[0] = zsub(zsub(zscale(-kx2, f1), zscale(2.0 * kxkz, f5)), zscale(kz2, f3));
-        } else if constexpr (ROLE == 3) {
-          b[0] = rp(r, 0);
+        } else if constexpr (ROLE == 1) {
+          b[0] = prod(6, r);
+        } else if constexpr (ROLE == 2) {
+          b[0] = prod(1, r);
+        } else {
+          b[0] = prod(3, r);
           if (probe) {
-            const double2 v = ring.c(r, 1);
+            const double2 v = Sv.ld(r);
             plo = zadd(plo, zscale(__ldg(a.wlo + r - 1), v));
             phi = zadd(phi, zscale(__ldg(a.whi + r - 1), v));
           }
-        } else {
-          b[0] = rp(r, 0);
         }
-        if constexpr (NC == 2) b[1] = ring.c(r, 3);
+        if constexpr (NC == 2) b[1] = Rs.ld(r);
       },
       [&](int r, const double2 *z) {
         Z0.st(r, z[0]);
         if constexpr (NC == 2) Z1.st(r, z[1]);
       },
       [&](int r) {
-        if constexpr (ROLE == 0) {
-          ring.get(r, 0, prow(0, r));
-          ring.get(r, 1, prow(2, r));
-          ring.get(r, 2, prow(4, r));
-        } else {
-          ring.get(r, 0, prow(ROLE == 1 ? 6 : ROLE == 2 ? 1 : 3, r));
-        }
-        if constexpr (NC == 2) ring.get(r, 3, Rs.p + (r - 1) * (int)nm);
-        if (probe) ring.get(r, 1, Sv.p + (r - 1) * (int)nm);
+        if constexpr (ROLE == 0) { pfp(0, r); pfp(2, r); pfp(4, r); }
+        else pfp(ROLE == 1 ? 6 : ROLE == 2 ? 1 : 3, r);
+        if constexpr (NC == 2) pf_l1(Rs.p + (r - 1) * (int)nm);
+        if (probe) pf_l1(Sv.p + (r - 1) * (int)nm);
       });
   if (probe) {
     a.vwall[m] = plo;
     a.vwall[nm + m] = phi;
   }
 
-  // backward units: Z0 at 0, Z1 (NC = 2) at 1, the emission's products at q = r + BW from 2
-  bwd_emit<BW, NC, 0, kStageAhead, true>(n, ufix,
+  bwd_emit<BW, NC, 0>(n, ufix,
       [&](int r, double2 *zc, double *) {
-        zc[0] = ring.c(r, 0);
-        if constexpr (NC == 2) zc[1] = ring.c(r, 1);
+        zc[0] = Z0.ld(r);
+        if constexpr (NC == 2) zc[1] = Z1.ld(r);
       },
       [&](int q, int r, const double2 (&wc)[NC][2 * BW + 1], const double (&)[1][2 * BW + 1]) {
-        const bool st = (q == r + BW);
         if constexpr (ROLE == 0) {
           const double c2i = kx * kx * kx + kx * (kz * kz), c4i = (kx * kx) * kz + kz * kz * kz;
-          const double2 f2 = st ? rp(r, 2) : prod(1, q), f4 = st ? rp(r, 3) : prod(3, q);
+          const double2 f2 = prod(1, q), f4 = prod(3, q);
           const double2 ehv = z2(-c2i * f2.y - c4i * f4.y, c2i * f2.x + c4i * f4.x);
-          hl(H_HV0).st(q, zadd(ehv, mvc<BW>(tb.t1, q, r, wc[0])));
+          hv(H_HV0).st(q, zadd(ehv, mvc<BW>(tb.t1, q, r, wc[0])));
         } else if constexpr (ROLE == 1) {
-          const double2 f7 = st ? rp(r, 2) : prod(5, q), f9 = st ? rp(r, 3) : prod(7, q);
+          const double2 f7 = prod(5, q), f9 = prod(7, q);
           const double2 t7 = z2(-kx * f7.y - kz * f9.y, kx * f7.x + kz * f9.x);
           const double2 t = zadd(t7, mvc<BW>(tb.t1, q, r, wc[0]));
-          hl(H_HT).st(q, z2(-t.x, -t.y));
+          hv(H_HT).st(q, z2(-t.x, -t.y));
         } else if constexpr (ROLE == 2) {
-          const double2 f1 = st ? rp(r, 2) : prod(0, q), f3 = st ? rp(r, 3) : prod(2, q);
-          const double2 f5 = st ? rp(r, 4) : prod(4, q);
+          const double2 f1 = prod(0, q), f3 = prod(2, q), f5 = prod(4, q);
           const double2 a1 = zadd(zscale(kxkz, zsub(f1, f3)), zscale(kz2 - kx2, f5));
           const double2 d1 = mvc<BW>(tb.t1, q, r, wc[0]), d2 = mvc<BW>(tb.t2, q, r, wc[0]);
-          hl(H_G2).st(q, zadd(a1, z2(kz * d1.y, -kz * d1.x)));
-          hl(H_V2).st(q, z2(-kx * d2.y, kx * d2.x));
+          hv(H_G2).st(q, zadd(a1, z2(kz * d1.y, -kz * d1.x)));
+          hv(H_V2).st(q, z2(-kx * d2.y, kx * d2.x));
         } else {
           const double2 d1 = mvc<BW>(tb.t1, q, r, wc[0]), d2 = mvc<BW>(tb.t2, q, r, wc[0]);
-          hl(H_G3).st(q, z2(-kx * d1.y, kx * d1.x));
-          hl(H_V3).st(q, z2(-kz * d2.y, kz * d2.x));
+          hv(H_G3).st(q, z2(-kx * d1.y, kx * d1.x));
+          hv(H_V3).st(q, z2(-kz * d2.y, kz * d2.x));
         }
         if constexpr (NC == 2) hl(d2_line).st(q, mvc<BW>(tb.t2, q, r, wc[NC - 1]));
       },
       [&](int r) {
-        ring.get(r, 0, Z0.p + (r - 1) * (int)nm);
-        if constexpr (NC == 2) ring.get(r, 1, Z1.p + (r - 1) * (int)nm);
+        pf_l1(Z0.p + (r - 1) * (int)nm);
+        if constexpr (NC == 2) pf_l1(Z1.p + (r - 1) * (int)nm);
         if (r <= n - 2 * BW) {
           const int q = r + BW;
-          if constexpr (ROLE == 0) {
-            ring.get(r, 2, prow(1, q));
-            ring.get(r, 3, prow(3, q));
-          } else if constexpr (ROLE == 1) {
-            ring.get(r, 2, prow(5, q));
-            ring.get(r, 3, prow(7, q));
-          } else if constexpr (ROLE == 2) {
-            ring.get(r, 2, prow(0, q));
-            ring.get(r, 3, prow(2, q));
-            ring.get(r, 4, prow(4, q));
-          }
+          if constexpr (ROLE == 0) { pfp(1, q); pfp(3, q); }
+          else if constexpr (ROLE == 1) { pfp(5, q); pfp(7, q); }
+          else if constexpr (ROLE == 2) { pfp(0, q); pfp(2, q); pfp(4, q); }
         }
       });
 }
 
-constexpr size_t hvhg_smem() { return sizeof(double2) * (size_t)kStageSlots * kHvhgUnits * kLanes * kRoles; }
-
 template <int BW, typename PT>
 __global__ void __launch_bounds__(kLanes * kRoles, 4) k_hvhg(SplitArgs a) {
-  extern __shared__ double2 hvhg_ring[];
   if (a.dsc->err) return;
   const int role = threadIdx.x / kLanes;
   const int64_t m = (int64_t)blockIdx.x * kLanes + (threadIdx.x % kLanes);
   if (m == 0 || m >= a.nmodes) return;
   const Tabs<BW> tb = tabs_at<BW>(a.tabs, a.ny);
-  const Ring<kHvhgUnits> ring{hvhg_ring + threadIdx.x, (int)blockDim.x};
   const bool s1 = a.substep == 1;
   switch (role) {
-    case 0: s1 ? hvhg_role<BW, PT, 0, 2>(a, tb, m, ring) : hvhg_role<BW, PT, 0, 1>(a, tb, m, ring); break;
-    case 1: s1 ? hvhg_role<BW, PT, 1, 2>(a, tb, m, ring) : hvhg_role<BW, PT, 1, 1>(a, tb, m, ring); break;
-    case 2: s1 ? hvhg_role<BW, PT, 2, 2>(a, tb, m, ring) : hvhg_role<BW, PT, 2, 1>(a, tb, m, ring); break;
-    default: hvhg_role<BW, PT, 3, 1>(a, tb, m, ring); break;
+    case 0: s1 ? hvhg_role<BW, PT, 0, 2>(a, tb, m) : hvhg_role<BW, PT, 0, 1>(a, tb, m); break;
+    case 1: s1 ? hvhg_role<BW, PT, 1, 2>(a, tb, m) : hvhg_role<BW, PT, 1, 1>(a, tb, m); break;
+    case 2: s1 ? hvhg_role<BW, PT, 2, 2>(a, tb, m) : hvhg_role<BW, PT, 2, 1>(a, tb, m); break;
+    default: hvhg_role<BW, PT, 3, 1>(a, tb, m); break;
   }
 }
 
@@ -286,7 +259,14 @@ __global__ void __launch_bounds__(kLanes * kRoles, 4) k_hvhg(SplitArgs a) {
 template <int BW>
 constexpr int kHelmUnits = 5 + BW;
 
-template <int BW, int ROLE>
+// A staged nonlinear-term unit, widened to double2.
+template <typename PT, int K>
+__device__ __forceinline__ double2 ring_hv(const Ring<K> &ring, int step, int k) {
+  if constexpr (sizeof(PT) == sizeof(float2)) return ring.f(step, k);
+  else return ring.c(step, k);
+}
+
+template <int BW, int ROLE, typename PT>
 __device__ __forceinline__ void helmholtz_role(const SplitArgs &a, const Tabs<BW> &tb, int64_t m,
                                                const Ring<kHelmUnits<BW>> &ring) {
   const int n = a.ny, s = a.substep;
@@ -321,15 +301,17 @@ __device__ __forceinline__ void helmholtz_role(const SplitArgs &a, const Tabs<BW
   const int sslot = ROLE == 0 ? 2 : 0;
   const DLine store{a.RK + sslot * ns + m, nm};
   const DLine d2l = hl(ROLE == 0 ? H_DT : H_DG);
-  const double2 *hA = hl(ROLE == 0 ? H_HT : H_G2).p, *hB = hl(H_G3).p;
+  auto hv = [&](int i) { return Line<PT>{reinterpret_cast<PT *>(a.hl) + i * ns + m, nm}; };
+  const PT *hA = hv(ROLE == 0 ? H_HT : H_G2).p, *hB = hv(H_G3).p;
   auto hsum = [&](int r) {
-    if constexpr (ROLE == 0) return hl(H_HT).ld(r);
-    else return zadd(hl(H_G2).ld(r), hl(H_G3).ld(r));
+    if constexpr (ROLE == 0) return hv(H_HT).ld(r);
+    else return zadd(hv(H_G2).ld(r), hv(H_G3).ld(r));
   };
+  auto rh = [&](int step, int k) { return ring_hv<PT>(ring, step, k); };
   // forward units: 0 store, 1 hA, 2 hB, 3 D2 store (substep 1)
   lu_fwd<BW, 1, 0, kStageAhead, true>(n, [&](int r, double *rw, bool c) { helm_row<BW>(tb, r, n, dummy, beta, rw, c); },
       [&](int r, double2 *bc, double *) {
-        const double2 h = ROLE == 0 ? ring.c(r, 1) : zadd(ring.c(r, 1), ring.c(r, 2));
+        const double2 h = ROLE == 0 ? rh(r, 1) : zadd(rh(r, 1), rh(r, 2));
         bc[0] = rhs(ring.c(r, 0), h, s == 1 ? ring.c(r, 3) : z2(0.0, 0.0), visc, r);
       },
       [&](int r, const double2 *zc, const double *) { Zr.st(r, zc[0]); }, ub,
@@ -347,7 +329,7 @@ __device__ __forceinline__ void helmholtz_role(const SplitArgs &a, const Tabs<BW
         const double2 f = mvc<BW>(tb.t0, q, r, wc[0]), d2f = mvc<BW>(tb.t2, q, r, wc[0]);
         out.st(q, f);
         double2 h;
-        if (q == r + BW) h = ROLE == 0 ? ring.c(r, BW + 1) : zadd(ring.c(r, BW + 1), ring.c(r, BW + 2));
+        if (q == r + BW) h = ROLE == 0 ? rh(r, BW + 1) : zadd(rh(r, BW + 1), rh(r, BW + 2));
         else h = hsum(q);
         store.st(q, store_new(h, f, d2f, visc));
       },
@@ -370,7 +352,7 @@ __device__ __forceinline__ void helmholtz_role(const SplitArgs &a, const Tabs<BW
 //     (solve_v_f.f90:140-153, the LU of solve_g.f90:42-71);
 //   (D2 - k^2 D0) v_p = phi_p with the wall velocities at rows 1 and n, and v_h = phi_h with zero
 //     walls (solve_v_f.f90:202-272).
-template <int BW>
+template <int BW, typename PT>
 __device__ __forceinline__ void helmholtz_phi_v(const SplitArgs &a, const Tabs<BW> &tb, int64_t m,
                                                 const Ring<kHelmUnits<BW>> &ring) {
   const int n = a.ny, s = a.substep;
@@ -389,8 +371,10 @@ __device__ __forceinline__ void helmholtz_phi_v(const SplitArgs &a, const Tabs<B
   const double p0 = dummy * trow<BW>(tb.t0, 1)[0] - beta * trow<BW>(tb.t2, 1)[0];  // A_g(1,1)
   const DLine store{a.RK + ns + m, nm};
   const DLine d2l = hl(H_DP);
-  const double2 *h0 = hl(H_HV0).p, *h1 = hl(H_V2).p, *h2 = hl(H_V3).p;
-  auto hsum = [&](int r) { return zadd(hl(H_HV0).ld(r), zadd(hl(H_V2).ld(r), hl(H_V3).ld(r))); };
+  auto hv = [&](int i) { return Line<PT>{reinterpret_cast<PT *>(a.hl) + i * ns + m, nm}; };
+  const PT *h0 = hv(H_HV0).p, *h1 = hv(H_V2).p, *h2 = hv(H_V3).p;
+  auto hsum = [&](int r) { return zadd(hv(H_HV0).ld(r), zadd(hv(H_V2).ld(r), hv(H_V3).ld(r))); };
+  auto rh = [&](int step, int k) { return ring_hv<PT>(ring, step, k); };
   // RK right-hand side of phi (solve_v_f.f90:54-97 with solve_g.f90:84-123's form); walls zero
   auto rhs = [&](double2 st, double2 h, double2 d2, int r) {
     if (r == 1 || r == n) return z2(0.0, 0.0);
@@ -408,7 +392,7 @@ __device__ __forceinline__ void helmholtz_phi_v(const SplitArgs &a, const Tabs<B
   // phi forward units: 0 store, 1..3 HV0, V2, V3, 4 D2 store (substep 1)
   lu_fwd<BW, 1, 1, kStageAhead, true>(n, [&](int r, double *rw, bool c) { helm_row<BW>(tb, r, n, dummy, beta, rw, c); },
       [&](int r, double2 *bc, double *br) {
-        const double2 h = zadd(ring.c(r, 1), zadd(ring.c(r, 2), ring.c(r, 3)));
+        const double2 h = zadd(rh(r, 1), zadd(rh(r, 2), rh(r, 3)));
         bc[0] = rhs(ring.c(r, 0), h, s == 1 ? ring.c(r, 4) : z2(0.0, 0.0), r);
         br[0] = (r == 1) ? p0 : 0.0;
       },
@@ -434,8 +418,7 @@ __device__ __forceinline__ void helmholtz_phi_v(const SplitArgs &a, const Tabs<B
       [&](int q, int r, const double2 (&wc)[1][2 * BW + 1], const double (&wr)[1][2 * BW + 1]) {
         const double2 f = mvc<BW>(tb.t0, q, r, wc[0]), d2f = mvc<BW>(tb.t2, q, r, wc[0]);
         out.st(q, f);
-        const double2 h = (q == r + BW) ? zadd(ring.c(r, BW + 2), zadd(ring.c(r, BW + 3), ring.c(r, BW + 4)))
-                                        : hsum(q);
+        const double2 h = (q == r + BW) ? zadd(rh(r, BW + 2), zadd(rh(r, BW + 3), rh(r, BW + 4))) : hsum(q);
         store.st(q, store_new(h, f, d2f));
         X1.st(q, mvr<BW>(tb.t0, q, r, wr[0]));  // phi_h (real part = imaginary part)
         X2.st(q, mvr<BW>(tb.t2, q, r, wr[0]));  // D2 phi_h
@@ -552,7 +535,7 @@ constexpr size_t helm_smem() {
   return sizeof(double2) * (size_t)kStageSlots * kHelmUnits<BW> * kLanes * kHelmRoles;
 }
 
-template <int BW>
+template <int BW, typename PT>
 __global__ void __launch_bounds__(kLanes * kHelmRoles, 4) k_helmholtz(SplitArgs a) {
   extern __shared__ double2 helm_ring[];
   if (a.dsc->err) return;  // a failed dt update leaves the state untouched
@@ -562,9 +545,9 @@ __global__ void __launch_bounds__(kLanes * kHelmRoles, 4) k_helmholtz(SplitArgs 
   const Tabs<BW> tb = tabs_at<BW>(a.tabs, a.ny);
   const Ring<kHelmUnits<BW>> ring{helm_ring + threadIdx.x, (int)blockDim.x};
   switch (role) {
-    case 0: helmholtz_role<BW, 0>(a, tb, m, ring); break;
-    case 1: helmholtz_role<BW, 1>(a, tb, m, ring); break;
-    default: helmholtz_phi_v<BW>(a, tb, m, ring); break;
+    case 0: helmholtz_role<BW, 0, PT>(a, tb, m, ring); break;
+    case 1: helmholtz_role<BW, 1, PT>(a, tb, m, ring); break;
+    default: helmholtz_phi_v<BW, PT>(a, tb, m, ring); break;
   }
 }
 
@@ -819,12 +802,13 @@ cudaError_t split_bw(Handle &h, int part, int substep, const double *dt_ptr, cud
     else k_mean<BW, double2><<<1, 32, 0, h.side>>>(ma);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
     if ((e = cudaEventRecord(h.ev_join, h.side)) != cudaSuccess) return e;
-    if (h.mixed) k_hvhg<BW, float2><<<blocks, kLanes * kRoles, hvhg_smem(), st>>>(a);
-    else k_hvhg<BW, double2><<<blocks, kLanes * kRoles, hvhg_smem(), st>>>(a);
+    if (h.mixed) k_hvhg<BW, float2><<<blocks, kLanes * kRoles, 0, st>>>(a);
+    else k_hvhg<BW, double2><<<blocks, kLanes * kRoles, 0, st>>>(a);
     return cudaGetLastError();
   }
   if (part == 1) {
-    k_helmholtz<BW><<<blocks, kLanes * kHelmRoles, helm_smem<BW>(), st>>>(a);
+    if (h.mixed) k_helmholtz<BW, float2><<<blocks, kLanes * kHelmRoles, helm_smem<BW>(), st>>>(a);
+    else k_helmholtz<BW, double2><<<blocks, kLanes * kHelmRoles, helm_smem<BW>(), st>>>(a);
     return cudaGetLastError();
   }
   const dim3 agrid((unsigned)((h.nmodes + 255) / 256), (unsigned)h.ny);
@@ -876,12 +860,30 @@ cudaError_t launch_vop_factor(Handle &h, cudaStream_t st) {
   };
   cudaError_t e = cudaSuccess;
   switch (h.bw) {
-    case 2: e = ring_smem(k_helmholtz<2>, helm_smem<2>()); break;
-    case 3: e = ring_smem(k_helmholtz<3>, helm_smem<3>()); break;
-    case 4: e = ring_smem(k_helmholtz<4>, helm_smem<4>()); break;
-    case 5: e = ring_smem(k_helmholtz<5>, helm_smem<5>()); break;
-    case 6: e = ring_smem(k_helmholtz<6>, helm_smem<6>()); break;
-    case 7: e = ring_smem(k_helmholtz<7>, helm_smem<7>()); break;
+    case 2:
+      e = ring_smem(k_helmholtz<2, float2>, helm_smem<2>());
+      if (e == cudaSuccess) e = ring_smem(k_helmholtz<2, double2>, helm_smem<2>());
+      break;
+    case 3:
+      e = ring_smem(k_helmholtz<3, float2>, helm_smem<3>());
+      if (e == cudaSuccess) e = ring_smem(k_helmholtz<3, double2>, helm_smem<3>());
+      break;
+    case 4:
+      e = ring_smem(k_helmholtz<4, float2>, helm_smem<4>());
+      if (e == cudaSuccess) e = ring_smem(k_helmholtz<4, double2>, helm_smem<4>());
+      break;
+    case 5:
+      e = ring_smem(k_helmholtz<5, float2>, helm_smem<5>());
+      if (e == cudaSuccess) e = ring_smem(k_helmholtz<5, double2>, helm_smem<5>());
+      break;
+    case 6:
+      e = ring_smem(k_helmholtz<6, float2>, helm_smem<6>());
+      if (e == cudaSuccess) e = ring_smem(k_helmholtz<6, double2>, helm_smem<6>());
+      break;
+    case 7:
+      e = ring_smem(k_helmholtz<7, float2>, helm_smem<7>());
+      if (e == cudaSuccess) e = ring_smem(k_helmholtz<7, double2>, helm_smem<7>());
+      break;
     default: break;
   }
   if (e != cudaSuccess) return e;
