@@ -147,7 +147,10 @@ __device__ __forceinline__ void hvhg_role(const SplitArgs &a, const Tabs<BW> &tb
   const PT *P = reinterpret_cast<const PT *>(a.P) + m;
   auto prod = [&](int slot, int r) { return ldp<PT>(P + slot * ns + (r - 1) * (int)nm); };
   auto pfp = [&](int slot, int r) { pf_l1(P + slot * ns + (r - 1) * (int)nm); };
-  const DLine Z0{a.zl + (2 * ROLE) * ns + m, nm}, Z1{a.zl + (2 * ROLE + 1) * ns + m, nm};
+  // the product chain's forward results at the products' precision (PT), the store chain's
+  // (substep 1, FP64 state) in double2
+  const Line<PT> Z0{reinterpret_cast<PT *>(a.zl + (2 * ROLE) * ns) + m, nm};
+  const DLine Z1{a.zl + (2 * ROLE + 1) * ns + m, nm};
   constexpr int store_slot = ROLE == 0 ? 1 : ROLE == 1 ? 2 : 0;  // RK_STORE 2, 3, 1
   constexpr int d2_line = ROLE == 0 ? H_DP : ROLE == 1 ? H_DT : H_DG;
   const DLine Rs{a.RK + store_slot * ns + m, nm};
