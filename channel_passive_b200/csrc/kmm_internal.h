@@ -169,9 +169,9 @@ cudaError_t launch_pressure(Handle &h, double2 *out, const double2 *bc, double *
 cudaError_t launch_ydiff(Handle &h, int mask, cudaStream_t st);
 // Offsets (doubles) inside Handle::stat: x-pass moment sums [ny][row blocks][kNumMoments],
 // transport inputs [4][ny], lines [KMM_STAT_NLINES][ny], spectra [kNumSpec][nxh][ny] and
-// [kNumSpec][nz][ny], centre-line values [2], the centre-line vector [ny].
+// [kNumSpec][nz][ny], centre-line values [2], the centre-line vector [ny], line scratch.
 struct StatLayout {
-  int64_t part, tr, lines, skx, skz, scal, center, total;
+  int64_t part, tr, lines, skx, skz, scal, center, scr, total;
 };
 StatLayout stat_layout(const Handle &h);
 // The statistics of the state (stats.cu) into Handle::stat; uses the buffers of

@@ -251,6 +251,7 @@ struct LinesArgs {
   const double *tr;   // [4][ny] transport inputs
   double *lines;      // [58][ny]
   double *scal;       // u_center, t_center
+  double2 *scr;       // [9][2][ny] scratch
   double u_gal;
 };
 
@@ -263,10 +264,9 @@ struct LinesArgs {
 // and the mean lines U = Re U00 + u_gal, W, Theta (get_u, get_statistics.f90:1024-1048).
 template <int BW>
 __global__ void k_stat_lines(LinesArgs a) {
-  extern __shared__ double2 lsm[];  // [9][2][ny]: the lines live in shared memory
   const int job = threadIdx.x, n = a.ny;
   if (job >= 9) return;
-  const DLine c{lsm + job * 2 * n, 1}, out{lsm + job * 2 * n + n, 1};
+  const DLine c{a.scr + (int64_t)job * 2 * n, 1}, out{a.scr + (int64_t)job * 2 * n + n, 1};
   const int field = job == 0 ? 0 : (job == 1 ? 2 : 3);
   for (int r = 1; r <= n; ++r) {
     double2 x;
@@ -304,11 +304,9 @@ cudaError_t stat_lines_bw(Handle &h, const StatLayout &L, cudaStream_t st) {
   a.tr = h.stat + L.tr;
   a.lines = h.stat + L.lines;
   a.scal = h.stat + L.scal;
+  a.scr = reinterpret_cast<double2 *>(h.stat + L.scr);
   a.u_gal = h.cfg.u_gal;
-  const size_t smem = sizeof(double2) * 9 * 2 * (size_t)h.ny;
-  cudaError_t e = cudaFuncSetAttribute(k_stat_lines<BW>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  if (e != cudaSuccess) return e;
-  k_stat_lines<BW><<<1, 32, smem, st>>>(a);
+  k_stat_lines<BW><<<1, 32, 0, st>>>(a);
   return cudaGetLastError();
 }
 
@@ -357,6 +355,9 @@ StatLayout stat_layout(const Handle &h) {
   o += 2;
   L.center = o;
   o += h.ny;
+  o = (o + 1) & ~(int64_t)1;  // double2 alignment of the scratch lines
+  L.scr = o;
+  o += 9 * 2 * 2 * (int64_t)h.ny;
   L.total = o;
   return L;
 }
