@@ -483,9 +483,10 @@ def run_kmm(args):
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline_quick(w)
 
-    # per substep: begin, zinv, xphys, zfwd, control probe, mean lines, hvhg, helmholtz,
-    # assemble; plus the dt update of substep 1
-    launches_per_step = 3 * (8 + (1 if w["control_amp"] != 0.0 else 0)) + 1
+    # per substep: begin, zinv, xphys, zfwd, mean lines, hvhg (which also takes the control
+    # probes), helmholtz, assemble; plus the dt update of substep 1 (the ncu launch list of
+    # profiles/step_launches_192x129x192_mixed.md counts the same)
+    launches_per_step = 3 * 8 + 1
     line = {
         "metric": METRIC,
         "value": value,
