@@ -484,8 +484,7 @@ def run_kmm(args):
         cpu = cpu_baseline_quick(w)
 
     # per substep: begin, zinv, xphys, zfwd, mean lines, hvhg (which also takes the control
-    # probes), helmholtz, assemble; plus the dt update of substep 1 (the ncu launch list of
-    # profiles/step_launches_192x129x192_mixed.md counts the same)
+    # probes), helmholtz, assemble; plus the dt update of substep 1
     launches_per_step = 3 * 8 + 1
     line = {
         "metric": METRIC,
