@@ -34,7 +34,7 @@ namespace kmm {
 // KMM_PREFETCH_ROWS (0 = none) and KMM_PREFETCH_L2 (prefetch into L2 instead of L1) are build
 // tuning macros.
 #ifndef KMM_PREFETCH_ROWS
-#define KMM_PREFETCH_ROWS 3
+#define KMM_PREFETCH_ROWS 4
 #endif
 constexpr int kPrefetchRows = KMM_PREFETCH_ROWS;
 
