@@ -463,10 +463,16 @@ int kmm_create(const kmm_config *cfg, kmm_handle **out) {
   if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess ||
       cudaStreamCreateWithFlags(&h->side, cudaStreamNonBlocking) != cudaSuccess ||
       cudaEventCreateWithFlags(&h->ev_fork, cudaEventDisableTiming) != cudaSuccess ||
-      cudaEventCreateWithFlags(&h->ev_join, cudaEventDisableTiming) != cudaSuccess) {
+      cudaEventCreateWithFlags(&h->ev_join, cudaEventDisableTiming) != cudaSuccess ||
+      cudaStreamCreateWithFlags(&h->copy, cudaStreamNonBlocking) != cudaSuccess) {
     set_error("cudaStreamCreate failed");
     return fail(KMM_ERR_CUDA);
   }
+  for (auto &ev : h->ev_io)
+    if (cudaEventCreateWithFlags(&ev, cudaEventDisableTiming) != cudaSuccess) {
+      set_error("cudaEventCreate failed");
+      return fail(KMM_ERR_CUDA);
+    }
   const size_t r2 = h->mixed ? sizeof(float2) : sizeof(double2);
   OpsOffsets off = ops_offsets(h->bw, h->ny);
   if ((rc = dalloc(*h, &h->S, 4 * h->ns))) return fail(rc);
@@ -537,8 +543,12 @@ int kmm_destroy(kmm_handle *hh) {
                   h->fftpos, h->tw64, h->tw32, h->dsc};
   for (void *p : ptrs)
     if (p) cudaFree(p);
+  if (h->copy) cudaStreamSynchronize(h->copy);
   if (h->ev_fork) cudaEventDestroy(h->ev_fork);
   if (h->ev_join) cudaEventDestroy(h->ev_join);
+  for (auto ev : h->ev_io)
+    if (ev) cudaEventDestroy(ev);
+  if (h->copy) cudaStreamDestroy(h->copy);
   if (h->side) cudaStreamDestroy(h->side);
   if (h->stream) cudaStreamDestroy(h->stream);
   delete h;
@@ -650,12 +660,53 @@ int kmm_step(kmm_handle *hh, int nsteps, kmm_scalars *out) {
   return kmm_sync(hh, out);
 }
 
+// kmm_step_host without RK_STORE: the four fields cross the bus one at a time on h.copy while
+// h.stream lays out the ones already there, and the D0 solve that rebuilds RK_STORE 2 from v
+// (v goes first) runs under the copies of u, w, theta; on the way back each field's layout
+// permutation overlaps the previous field's copy.  Same kernels and arithmetic as the serial
+// path, in another order.
+static int step_host_pipelined(Handle &h, double *U, int nsteps, kmm_scalars *out) {
+  const size_t fb = sizeof(double2) * (size_t)h.ns;
+  const int slots[4] = {0, 1, 2, 6};  // U slots of u, v, w, theta = S fields 0..3
+  const int order[4] = {1, 0, 2, 3};
+  cudaEvent_t *ev = h.ev_io;
+  // the copies may overwrite staging only after earlier work on stream is done with it
+  KMM_CUDA(cudaEventRecord(ev[8], h.stream));
+  KMM_CUDA(cudaStreamWaitEvent(h.copy, ev[8], 0));
+  for (int i = 0; i < 4; ++i) {
+    const int f = order[i];
+    KMM_CUDA(cudaMemcpyAsync(h.staging + f * h.ns, U + 2 * (size_t)slots[f] * h.ns, fb, cudaMemcpyHostToDevice,
+                             h.copy));
+    KMM_CUDA(cudaEventRecord(ev[f], h.copy));
+  }
+  for (int i = 0; i < 4; ++i) {
+    const int f = order[i];
+    KMM_CUDA(cudaStreamWaitEvent(h.stream, ev[f], 0));
+    KMM_CUDA(launch_ref_to_planes(h.staging + f * h.ns, h.S + f * h.ns, 1, h.nmodes, h.ny, h.stream));
+    if (f == 1) KMM_CUDA(launch_init_phi(h, h.stream));
+  }
+  KMM_CUDA(launch_init_elem(h, h.stream));
+  int rc;
+  if ((rc = kmm_step_async(reinterpret_cast<kmm_handle *>(&h), nsteps))) return rc;
+  for (int f = 0; f < 4; ++f) {
+    KMM_CUDA(launch_planes_to_ref(h.S + f * h.ns, h.staging + f * h.ns, 1, h.nmodes, h.ny, h.stream));
+    KMM_CUDA(cudaEventRecord(ev[4 + f], h.stream));
+    KMM_CUDA(cudaStreamWaitEvent(h.copy, ev[4 + f], 0));
+    KMM_CUDA(cudaMemcpyAsync(U + 2 * (size_t)slots[f] * h.ns, h.staging + f * h.ns, fb, cudaMemcpyDeviceToHost,
+                             h.copy));
+  }
+  KMM_CUDA(cudaEventRecord(ev[8], h.copy));
+  KMM_CUDA(cudaStreamWaitEvent(h.stream, ev[8], 0));
+  return kmm_sync(reinterpret_cast<kmm_handle *>(&h), out);
+}
+
 int kmm_step_host(kmm_handle *hh, double *U, int nf, double *rk, int nsteps, kmm_scalars *out) {
   if (!hh || !U || nf < 7) {
     set_error("kmm_step_host: null pointer or nf < 7");
     return KMM_ERR_ARG;
   }
   Handle &h = *reinterpret_cast<Handle *>(hh);
+  if (!rk) return step_host_pipelined(h, U, nsteps, out);
   int rc = upload_fields(h, U, nf, rk, h.stream);
   if (rc) return rc;
   // Without rk the stores are rebuilt from U, as the reference's restart option 1 does

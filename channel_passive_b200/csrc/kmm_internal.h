@@ -99,6 +99,8 @@ struct Handle {
   double *stat = nullptr;                  // statistics buffers (stat_layout), made on first use
   cudaStream_t side = nullptr;             // mean-mode lines run here, forked from / joined to stream
   cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+  cudaStream_t copy = nullptr;             // host <-> device copies of kmm_step_host, beside stream
+  cudaEvent_t ev_io[9] = {};               // its per-field hand-offs between copy and stream
   double2 *staging = nullptr;              // [7][nz][nxh][ny] reference-layout staging
   int *fftpos = nullptr;
   double2 *tw64 = nullptr;
@@ -128,6 +130,10 @@ cudaError_t launch_zfwd(Handle &h, const void *mid, void *dst_planes, int nfield
 cudaError_t launch_update_dt(Handle &h, int substep, cudaStream_t st);
 cudaError_t launch_begin_substep(Handle &h, int substep, cudaStream_t st);
 cudaError_t launch_init_stores(Handle &h, cudaStream_t st);
+// set_initial_data_uvw in two parts: RK_STORE 2 of the modes other than (0,0), which needs only
+// v (launch_init_phi), and the element-wise rest (launch_init_elem, needs u, w, theta).
+cudaError_t launch_init_phi(Handle &h, cudaStream_t st);
+cudaError_t launch_init_elem(Handle &h, cudaStream_t st);
 cudaError_t launch_ref_to_planes(const double2 *src, double2 *dst, int nfield, int64_t nmodes,
                                  int ny, cudaStream_t st);
 cudaError_t launch_planes_to_ref(const double2 *src, double2 *dst, int nfield, int64_t nmodes,

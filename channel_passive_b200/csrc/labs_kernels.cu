@@ -27,11 +27,12 @@ __device__ __forceinline__ DLine dline(double2 *base, int64_t off, int64_t m, in
 // set_initial_data_uvw, initial_step.f90:139-179: RK_STORE 1 = i kz u - i kx w,
 // RK_STORE 2 = D2 D0^{-1} v - k^2 v, RK_STORE 3 = theta; the mean mode stores U, W, Theta.  One
 // thread per mode: the D0 solve of v runs through the fixed D0 profile LU (sweeps.cuh) and D2 of
-// it is emitted from the backward window.
-template <int BW>
+// it is emitted from the backward window.  PHI_ONLY: RK_STORE 2 of the modes other than (0,0),
+// which needs v alone (k_init_elem does the rest), so it can start before u, w, theta arrive.
+template <int BW, bool PHI_ONLY = false>
 __global__ void __launch_bounds__(128) k_init_stores(InitArgs a) {
   const int64_t m = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (m >= a.nmodes) return;
+  if (m >= a.nmodes || (PHI_ONLY && m == 0)) return;
   const int n = a.ny;
   const int64_t nm = a.nmodes;
   const DLine Su = dline(a.S, 0 * a.ns, m, nm), Sv = dline(a.S, 1 * a.ns, m, nm);
@@ -59,19 +60,43 @@ __global__ void __launch_bounds__(128) k_init_stores(InitArgs a) {
   bwd_emit<BW, 1, 0>(n, ufix, [&](int r, double2 *zc, double *) { zc[0] = Z.ld(r); },
       [&](int q, int r, const double2 (&wc)[1][2 * BW + 1], const double (&)[1][2 * BW + 1]) {
         R2.st(q, zsub(mvc<BW>(tb.t2, q, r, wc[0]), zscale(k2, Sv.ld(q))));
-        R1.st(q, zsub(zmul(z2(0.0, kz), Su.ld(q)), zmul(z2(0.0, kx), Sw.ld(q))));
-        R3.st(q, St.ld(q));
+        if constexpr (!PHI_ONLY) {
+          R1.st(q, zsub(zmul(z2(0.0, kz), Su.ld(q)), zmul(z2(0.0, kx), Sw.ld(q))));
+          R3.st(q, St.ld(q));
+        }
       },
       [&](int r) {
         pf_l1(Z.p + (r - 1) * (int)nm);
         if (r <= n - 2 * BW) {
           const int64_t o = (r + BW - 1) * (int)nm;
           pf_l1(Sv.p + o);
+          if constexpr (PHI_ONLY) return;
           pf_l1(Su.p + o);
           pf_l1(Sw.p + o);
           pf_l1(St.p + o);
         }
       });
+}
+
+// The element-wise rest of set_initial_data_uvw beside k_init_stores<BW, true>: RK_STORE 1 =
+// i kz u - i kx w and RK_STORE 3 = theta, and the mean mode's stores U, W, Theta
+// (initial_step.f90:139-179).  One thread per (mode, y).
+__global__ void __launch_bounds__(256) k_init_elem(InitArgs a) {
+  const int64_t nm = a.nmodes, ns = a.ns;
+  const int64_t m = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (m >= nm) return;
+  const int64_t o = (int64_t)blockIdx.y * nm + m;
+  const double2 u = a.S[o], w = a.S[2 * ns + o];
+  if (m == 0) {
+    a.RK[o] = u;
+    a.RK[ns + o] = w;
+  } else {
+    const int kzi = (int)(m / a.nxh), kxi = (int)(m - (int64_t)kzi * a.nxh);
+    const int kzint = (kzi <= a.nz / 2) ? kzi : kzi - a.nz;
+    const double kx = kxi * a.lmfxr, kz = kzint * a.lmfzr;
+    a.RK[o] = zsub(zmul(z2(0.0, kz), u), zmul(z2(0.0, kx), w));
+  }
+  a.RK[2 * ns + o] = a.S[3 * ns + o];
 }
 
 // Batched LABS kernels for the unit tests (row 18).
@@ -133,6 +158,13 @@ cudaError_t dispatch_bw(int bw, Args &&...args) {
 template <int BW> struct InitRun {
   static cudaError_t run(Handle &h, cudaStream_t st) { return init_bw<BW>(h, st); }
 };
+template <int BW> struct InitPhiRun {
+  static cudaError_t run(Handle &h, cudaStream_t st) {
+    const InitArgs a = make_init_args(h);
+    k_init_stores<BW, true><<<(unsigned)((h.nmodes + 127) / 128), 128, 0, st>>>(a);
+    return cudaGetLastError();
+  }
+};
 template <int BW> struct LuRun {
   static cudaError_t run(Handle &h, double *a, int nm, cudaStream_t st) {
     k_labs_lu<BW><<<(nm + 127) / 128, 128, 0, st>>>(a, h.ny, nm);
@@ -155,6 +187,13 @@ template <int BW> struct MmRun {
 }  // namespace
 
 cudaError_t launch_init_stores(Handle &h, cudaStream_t st) { return dispatch_bw<InitRun>(h.bw, h, st); }
+cudaError_t launch_init_phi(Handle &h, cudaStream_t st) { return dispatch_bw<InitPhiRun>(h.bw, h, st); }
+cudaError_t launch_init_elem(Handle &h, cudaStream_t st) {
+  const InitArgs a = make_init_args(h);
+  const dim3 grid((unsigned)((h.nmodes + 255) / 256), (unsigned)h.ny);
+  k_init_elem<<<grid, 256, 0, st>>>(a);
+  return cudaGetLastError();
+}
 cudaError_t launch_labs_lu(Handle &h, double *a, int nmodes, cudaStream_t st) {
   return dispatch_bw<LuRun>(h.bw, h, a, nmodes, st);
 }
