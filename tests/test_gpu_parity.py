@@ -396,3 +396,32 @@ def test_statistics_match_oracle(precision, tol):
     assert abs(g["U_c"] - o["u_center"]) <= 1e-12 * abs(o["u_center"])
     assert abs(g["T_c"] - o["t_center"]) <= 1e-12 * abs(o["t_center"])
     assert rel_l2(g["P"], o["P"]) < tol
+
+
+def test_statistics_other_shape_tanh_grid_fp64():
+    """kmm_get_statistics in FP64 on another shape (nx > nz, 41 tanh-mapped collocation points,
+    no control) against the oracle: all lines, both spectra, the centre-line values and p."""
+    from oracle import stats as ostats
+    cfg, p = make_pair(nx=24, ny=41, nz=16, stretch=2.0, grid=1)
+    p.grid = "tanh"
+    ops = okmm.make_operators(p)
+    U = seeded_state(cfg, ops.y)
+    with Channel(cfg) as ch:
+        np.testing.assert_allclose(ch.y, ops.y, rtol=0, atol=1e-14)
+        ch.set_initial_data_uvw(U, 0.01)
+        ch.step(1)
+        Us, _ = ch.download_state()
+        g = ch.get_statistics(pressure=True)
+    o = ostats.statistics(Us, ops, p)
+    for i, name in enumerate(ostats.LINE_NAMES):
+        ref = o["lines"][i]
+        if np.abs(ref).max() < 1e-14:
+            continue
+        err = np.abs(g["lines"][name] - ref).max() / np.abs(ref).max()
+        assert err < 1e-11, (name, err)
+    for i, name in enumerate(ostats.SPEC_NAMES):
+        assert rel_l2(g["spec_kx"][name], o["spec_kx"][i]) < 1e-11, ("kx", name)
+        assert rel_l2(g["spec_kz"][name], o["spec_kz"][i]) < 1e-11, ("kz", name)
+    assert abs(g["U_c"] - o["u_center"]) <= 1e-12 * abs(o["u_center"])
+    assert abs(g["T_c"] - o["t_center"]) <= 1e-12 * abs(o["t_center"])
+    assert rel_l2(g["P"], o["P"]) < 1e-11
