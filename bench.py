@@ -371,6 +371,76 @@ def cpu_baseline_quick(w):
             "sample": pool.sample_text() + "; best of substeps 1-3 after one warm-up"}
 
 
+# 16 independent channels of uneven sizes, mixed precision, Re_tau 180 (Lx 2 pi, Lz pi), CFL time
+# step, each with its own seeded IC, opposition amplitude A ~ U[-1, 0] and detection plane
+# y+ ~ U[10, 20].  Amplitudes below -1 give the opposition loop a gain above one: the FP64
+# restatement itself diverges from this IC (velmax 40 -> 4455 in 10 steps at A = -1.47,
+# y+ = 11.6, even under the CFL time step), so they are not drawn.
+ENSEMBLE_A = (-1.0, 0.0)
+ENSEMBLE_SHAPES = [(64, 65, 64)] * 6 + [(96, 97, 96)] * 6 + [(128, 97, 128)] * 4
+
+
+def run_ensemble(args, device, local, rank):
+    """Aggregate grid-point-steps/s of the 16-channel ensemble stepped through kmm_ensemble_step
+    (every channel's graph launches enqueued on its own stream before any wait) against the same
+    channels stepped one by one (kmm_step per channel, in turn).  Both arms are timed by CUDA
+    events recorded on an idle device right before and right after the host call."""
+    import torch
+
+    from channel_passive_b200 import Channel, Config, ensemble_step, ic
+    from channel_passive_b200 import _lib
+
+    rng = np.random.default_rng(SEED + 7 + rank)
+    chans, members = [], []
+    for i, (nx, ny, nz) in enumerate(ENSEMBLE_SHAPES):
+        amp = float(rng.uniform(*ENSEMBLE_A))
+        yplus = float(rng.uniform(10.0, 20.0))
+        ch = Channel(Config(nx=nx, ny=ny, nz=nz, lmfx=1.0, lmfz=0.5, stretch=0.9, nu=1.0 / 2800.0, pr=0.71,
+                            fixed_dt=0, control_amp=amp, control_yd=-1.0 + yplus / RE_TAU,
+                            precision=_lib.KMM_PREC_MIXED, device=local))
+        U = ic.seeded_ic(nx, ny, nz, ch.y, 1.0, 0.5, seed=SEED + 100 * rank + i)
+        chans.append((ch, U))
+        members.append({"shape": f"{nx}x{ny}x{nz}", "A": amp, "y_plus": yplus})
+    points = sum(nx * ny * nz for nx, ny, nz in ENSEMBLE_SHAPES)
+    k = args.ensemble_steps
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+
+    def reset():
+        for ch, U in chans:
+            ch.set_initial_data_uvw(U, 0.01)
+        torch.cuda.synchronize()
+
+    def clock(fn):
+        torch.cuda.synchronize()
+        e0.record()
+        fn()
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1)
+
+    hs = [ch for ch, _ in chans]
+    reset()
+    ensemble_step(hs, args.warmup)                 # graphs captured, clocks up
+    for ch in hs:
+        ch.step(1)
+    reset()
+    ms_one = clock(lambda: [ch.step(k) for ch in hs])
+    reset()
+    ms_ens = clock(lambda: ensemble_step(hs, k))
+    for ch in hs:
+        ch.close()
+    return {"channels": len(hs), "shapes": "6x 64x65x64, 6x 96x97x96, 4x 128x97x128 (Lx 2 pi, Lz pi)",
+            "precision": "mixed", "steps_per_channel": k, "dt": "CFL 1.0 per channel",
+            "control": "A ~ U[-1, 0], y+ ~ U[10, 20] per channel",
+            "grid_point_steps_per_s": points * k / (ms_ens * 1e-3),
+            "one_by_one_grid_point_steps_per_s": points * k / (ms_one * 1e-3),
+            "speedup_vs_one_by_one": ms_one / ms_ens, "ms": ms_ens, "one_by_one_ms": ms_one,
+            "members": members,
+            "api": "kmm_ensemble_step over 16 handles (stream-concurrent CUDA graphs); one by one = "
+                   "kmm_step(k) per handle in turn"}
+
+
 def run_kmm(args):
     import torch
 
@@ -479,6 +549,8 @@ def run_kmm(args):
     torch.cuda.synchronize()
     ms_stat = max_over_ranks(e0.elapsed_time(e1), dist, device) / args.stat_calls
 
+    ens = run_ensemble(args, device, local, rank) if args.ensemble_steps > 0 else None
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline_quick(w)
@@ -521,6 +593,7 @@ def run_kmm(args):
         "statistics": {"ms_per_call": ms_stat, "per_step_time": ms_stat / (ms_mixed / args.steps),
                        "api": "kmm_get_statistics: the 58 stat-file lines, 2 x 18 spectra, U_c, T_c "
                               "and the pressure of the current state (statistics step), on the device"},
+        "ensemble": ens,
         "gpu_launches": launches_per_step * args.steps,
         "clocks": clocks,
         "last_step": {"dt": out_m["dt"], "dpdx": out_m["phi_dpdx"][3], "tau_w": out_m["wall_shear_stress"],
@@ -548,6 +621,8 @@ def main(argv=None):
     ap.add_argument("--prof-steps", type=int, default=5)
     ap.add_argument("--e2e-steps", type=int, default=20)
     ap.add_argument("--stat-calls", type=int, default=5, help="statistics-step calls timed")
+    ap.add_argument("--ensemble-steps", type=int, default=50,
+                    help="RK3 steps per channel of the 16-channel ensemble (0: skip)")
     ap.add_argument("--ref-planes", type=int, default=4, help="y-planes per worker in a reference step")
     ap.add_argument("--ref-rows", type=int, default=4, help="kz rows per worker in a reference step")
     ap.add_argument("--no-cpu-baseline", action="store_true")

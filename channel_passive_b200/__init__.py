@@ -6,5 +6,5 @@ The compute path is libkmm.so (CUDA kernels + C++ operator builder); this packag
 the build recipe, the ctypes binding and a thin host-side mirror of the reference
 interface.
 """
-from .solver import Channel, Config, KmmError, NFIELD, labs_fill_full, read_input_file  # noqa: F401
+from .solver import Channel, Config, KmmError, NFIELD, ensemble_step, labs_fill_full, read_input_file  # noqa: F401
 from . import ic  # noqa: F401

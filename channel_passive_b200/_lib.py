@@ -90,6 +90,7 @@ SIGNATURES = {
     "kmm_step_host": (C.c_int, [_P, _D, C.c_int, _D, C.c_int, C.POINTER(KmmScalars)]),
     "kmm_get_stream": (C.c_int, [_P, C.POINTER(_P)]),
     "kmm_get_pressure": (C.c_int, [_P, C.POINTER(C.c_double)]),
+    "kmm_ensemble_step": (C.c_int, [C.POINTER(_P), C.c_int, C.c_int, C.POINTER(KmmScalars)]),
     "kmm_get_statistics": (C.c_int, [_P, C.POINTER(C.c_double), C.POINTER(C.c_double),
                                      C.POINTER(C.c_double), C.POINTER(C.c_double),
                                      C.POINTER(C.c_double)]),

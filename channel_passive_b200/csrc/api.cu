@@ -660,6 +660,39 @@ int kmm_step(kmm_handle *hh, int nsteps, kmm_scalars *out) {
   return kmm_sync(hh, out);
 }
 
+int kmm_ensemble_step(kmm_handle *const *hs, int n, int nsteps, kmm_scalars *outs) {
+  if (!hs || n < 0 || nsteps < 0) {
+    set_error("kmm_ensemble_step: null handle array or negative count");
+    return KMM_ERR_ARG;
+  }
+  for (int i = 0; i < n; ++i)
+    if (!hs[i]) {
+      set_error("kmm_ensemble_step: null handle " + std::to_string(i));
+      return KMM_ERR_ARG;
+    }
+  int first = KMM_OK;
+  std::string msg;
+  std::vector<char> queued((size_t)n, 0);
+  for (int i = 0; i < n; ++i) {  // enqueue every channel before waiting on any
+    const int rc = kmm_step_async(hs[i], nsteps);
+    if (rc == KMM_OK) queued[(size_t)i] = 1;
+    else if (first == KMM_OK) {
+      first = rc;
+      msg = kmm_last_error();
+    }
+  }
+  for (int i = 0; i < n; ++i) {
+    if (!queued[(size_t)i]) continue;
+    const int rc = kmm_sync(hs[i], outs ? &outs[i] : nullptr);
+    if (rc != KMM_OK && first == KMM_OK) {
+      first = rc;
+      msg = kmm_last_error();
+    }
+  }
+  if (first != KMM_OK) set_error("kmm_ensemble_step: " + msg);
+  return first;
+}
+
 // kmm_step_host without RK_STORE: the four fields cross the bus one at a time on h.copy while
 // h.stream lays out the ones already there, and the D0 solve that rebuilds RK_STORE 2 from v
 // (v goes first) runs under the copies of u, w, theta; on the way back each field's layout

@@ -322,4 +322,18 @@ class Channel:
                                              C.c_void_p(b.data_ptr()), x.shape[-1], self._stream()))
 
 
-__all__ = ["Config", "Channel", "KmmError", "read_input_file", "labs_fill_full", "NFIELD"]
+def ensemble_step(channels, nsteps: int = 1) -> list[dict]:
+    """kmm_ensemble_step: nsteps RK3 steps of every channel, each channel's graph launches
+    enqueued on its own stream before any is waited on, so independent channels of any sizes
+    run side by side on the GPU.  Returns each channel's diagnostics of its last step."""
+    chans = list(channels)
+    if len({id(c) for c in chans}) != len(chans):
+        raise ValueError("ensemble_step: a channel appears twice")
+    n = len(chans)
+    hs = (C.c_void_p * max(n, 1))(*[c._h for c in chans])
+    outs = (KmmScalars * max(n, 1))()
+    check(chans[0]._lib.kmm_ensemble_step(hs, n, int(nsteps), outs) if n else 0)
+    return [outs[i].as_dict() for i in range(n)]
+
+
+__all__ = ["Config", "Channel", "KmmError", "read_input_file", "labs_fill_full", "NFIELD", "ensemble_step"]

@@ -130,6 +130,14 @@ int kmm_time_march(kmm_handle *h, int rk_substep, kmm_scalars *out);
  * CUDA graph; out receives the diagnostics of the last step. */
 int kmm_step(kmm_handle *h, int nsteps, kmm_scalars *out);
 
+/* An ensemble of independent channels (one handle each; any sizes, precisions and control
+ * settings) stepped together: every handle's nsteps graph launches are enqueued on its own
+ * stream before any handle is waited on, so the channels run concurrently and small grids share
+ * the GPU.  outs (may be NULL) receives each handle's diagnostics of its last step.  Returns the
+ * status of the first handle that fails (all handles are still waited on).  No counterpart in
+ * the reference, which runs one channel per job.  Each handle must appear once. */
+int kmm_ensemble_step(kmm_handle *const *hs, int n, int nsteps, kmm_scalars *outs);
+
 /* Same as kmm_step but only enqueues the work on the handle's stream (no host sync,
  * no error check); kmm_sync then waits and reports. */
 int kmm_step_async(kmm_handle *h, int nsteps);

@@ -103,4 +103,8 @@ def test_null_arguments_return_status():
     assert lib.kmm_create(None, None) == _lib.KMM_ERR_ARG
     assert lib.kmm_time_march(None, 1, None) == _lib.KMM_ERR_ARG
     assert lib.kmm_step_host(None, None, 10, None, 1, None) == _lib.KMM_ERR_ARG
+    assert lib.kmm_ensemble_step(None, 1, 1, None) == _lib.KMM_ERR_ARG
+    hs = (C.c_void_p * 2)(None, None)
+    assert lib.kmm_ensemble_step(hs, 2, 1, None) == _lib.KMM_ERR_ARG
+    assert lib.kmm_ensemble_step(hs, 0, 1, None) == 0
     assert lib.kmm_destroy(None) == 0
