@@ -86,6 +86,8 @@ def test_read_input_file_rejects_malformed(tmp_path):
     (dict(nx=14), "factor"),
     (dict(nu=-1.0), "positive"),
     (dict(control_amp=-1.0, control_yd=0.5), "y_d"),
+    # the per-mode kernels' 32-bit line offsets: 2*bw*nxh*nz*ny must stay below 2^31
+    (dict(nx=2048, ny=129, nz=2048), "2^31"),
 ])
 def test_create_rejects_bad_config(override, msg):
     from channel_passive_b200 import Channel
