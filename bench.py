@@ -441,6 +441,60 @@ def run_ensemble(args, device, local, rank):
                    "kmm_step(k) per handle in turn"}
 
 
+def run_production(args, device, local, rank, dist):
+    """The Re_tau 590 production grid: 384x257x384, Lx 2 pi, Lz pi, tanh-mapped y, nu 1/10850,
+    CFL 0.8, opposition control A = -1 at y+ = 15 of Re_tau 590, one passive scalar (Pr 0.71).
+    Mixed-precision and FP64 RK3 steps/s through the CUDA graph, each timed by CUDA events on the
+    handle's stream, the step's HBM roofline fraction, and mixed vs FP64 after the timed steps."""
+    import torch
+
+    from channel_passive_b200 import Channel, Config, ic
+    from channel_passive_b200 import _lib
+
+    w = dict(nx=384, ny=257, nz=384)
+    common = dict(lmfx=1.0, lmfz=0.5, stretch=2.0, grid=_lib.KMM_GRID_TANH, nu=1.0 / 10850.0, pr=0.71,
+                  cfl=0.8, fixed_dt=0, control_amp=-1.0, control_yd=-1.0 + 15.0 / 590.0, device=local, **w)
+    k = args.production_steps
+    res, states = {}, {}
+    U0 = None
+    for name, prec in (("mixed", _lib.KMM_PREC_MIXED), ("fp64", _lib.KMM_PREC_FP64)):
+        ch = Channel(Config(precision=prec, **common))
+        if U0 is None:
+            U0 = ic.seeded_ic(w["nx"], w["ny"], w["nz"], ch.y, 1.0, 0.5, seed=SEED + rank)
+        ch.set_initial_data_uvw(U0, 1e-3)
+        ch.step(args.warmup)
+        ch.set_initial_data_uvw(U0, 1e-3)
+        stream = torch.cuda.ExternalStream(ch.stream_ptr, device=device)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        barrier(dist, device)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        ch.step_async(k)
+        e1.record(stream)
+        out = ch.sync()
+        torch.cuda.synchronize()
+        ms = max_over_ranks(e0.elapsed_time(e1), dist, device)
+        states[name], _ = ch.download_state(7)
+        ch.close()
+        s_nl = 8 if name == "mixed" else 16
+        peak, _kind = measured_peaks()
+        res[name] = {"steps_per_s": k / (ms * 1e-3), "ms_per_step": ms / k, "last_dt": out["dt"],
+                     "step_algorithmic_bytes": step_bytes(w, s_nl),
+                     "step_frac": step_bytes(w, s_nl) / (ms / k * 1e-3) / 1e9 / peak}
+    names = {0: "u", 1: "v", 2: "w", 6: "theta"}
+    Um, Ud = states["mixed"], states["fp64"]
+    rel = {names[f]: float(np.linalg.norm(Um[f] - Ud[f]) / np.linalg.norm(Ud[f])) for f in names}
+    return {"workload": "384x257x384 Re_tau 590 (Lx 2 pi, Lz pi, tanh y map), nu 1/10850, CFL 0.8, "
+                        "opposition control A=-1 at y+=15, one passive scalar Pr 0.71",
+            "steps": k, "warmup": args.warmup, "mixed": res["mixed"], "fp64": res["fp64"],
+            "mixed_over_fp64": res["mixed"]["steps_per_s"] / res["fp64"]["steps_per_s"],
+            "grid_point_steps_per_s": res["mixed"]["steps_per_s"] * w["nx"] * w["ny"] * w["nz"],
+            "rel_l2_mixed_vs_fp64": rel,
+            "roofline_peak": "of measured HBM copy bandwidth",
+            "second_scalar": "not run: the reference carries one passive scalar"}
+
+
 def run_kmm(args):
     import torch
 
@@ -550,6 +604,7 @@ def run_kmm(args):
     ms_stat = max_over_ranks(e0.elapsed_time(e1), dist, device) / args.stat_calls
 
     ens = run_ensemble(args, device, local, rank) if args.ensemble_steps > 0 else None
+    prod = run_production(args, device, local, rank, dist) if args.production_steps > 0 else None
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -594,6 +649,7 @@ def run_kmm(args):
                        "api": "kmm_get_statistics: the 58 stat-file lines, 2 x 18 spectra, U_c, T_c "
                               "and the pressure of the current state (statistics step), on the device"},
         "ensemble": ens,
+        "production": prod,
         "gpu_launches": launches_per_step * args.steps,
         "clocks": clocks,
         "last_step": {"dt": out_m["dt"], "dpdx": out_m["phi_dpdx"][3], "tau_w": out_m["wall_shear_stress"],
@@ -621,6 +677,8 @@ def main(argv=None):
     ap.add_argument("--prof-steps", type=int, default=5)
     ap.add_argument("--e2e-steps", type=int, default=20)
     ap.add_argument("--stat-calls", type=int, default=5, help="statistics-step calls timed")
+    ap.add_argument("--production-steps", type=int, default=20,
+                    help="RK3 steps timed on the 384x257x384 production grid (0: skip)")
     ap.add_argument("--ensemble-steps", type=int, default=50,
                     help="RK3 steps per channel of the 16-channel ensemble (0: skip)")
     ap.add_argument("--ref-planes", type=int, default=4, help="y-planes per worker in a reference step")
