@@ -476,12 +476,14 @@ def run_production(args, device, local, rank, dist):
         torch.cuda.synchronize()
         ms = max_over_ranks(e0.elapsed_time(e1), dist, device)
         states[name], _ = ch.download_state(7)
+        prof = ch.profile_step(2)
         ch.close()
         s_nl = 8 if name == "mixed" else 16
         peak, _kind = measured_peaks()
         res[name] = {"steps_per_s": k / (ms * 1e-3), "ms_per_step": ms / k, "last_dt": out["dt"],
                      "step_algorithmic_bytes": step_bytes(w, s_nl),
-                     "step_frac": step_bytes(w, s_nl) / (ms / k * 1e-3) / 1e9 / peak}
+                     "step_frac": step_bytes(w, s_nl) / (ms / k * 1e-3) / 1e9 / peak,
+                     "kernels_ms": {kn: v["ms"] for kn, v in prof.items()}}
     names = {0: "u", 1: "v", 2: "w", 6: "theta"}
     Um, Ud = states["mixed"], states["fp64"]
     rel = {names[f]: float(np.linalg.norm(Um[f] - Ud[f]) / np.linalg.norm(Ud[f])) for f in names}
