@@ -158,8 +158,19 @@ struct X2Args {
 // dft_x_realspace.f90:192-199): packed lines (f1, f2), (f3, f4), (f5, f6); no CFL, and only
 // slots 0..5 are written.  With a_.mom set, each block also writes the sums over its physical
 // points of the moments of dft_x_realspace.f90:128-155 (moment_terms), in FP64.
+#ifndef KMM_X576_MINB
+#define KMM_X576_MINB 5
+#endif
+// Resident blocks asked of the compiler: at N = 576 the FP32 step pass otherwise takes 140
+// registers a thread, 3 blocks (12 warps) an SM.  5 blocks (96 registers, a 200-byte spill) took
+// the pass from 2.35 to 2.01 ms on the 384x257x384 grid (4 blocks, no spill: 2.04 ms).  The
+// statistics variant keeps the default: a cap spills more there.
+template <typename R, int N, bool STAT> constexpr int x_min_blocks() {
+  return (sizeof(R) == 4 && N >= 576 && !STAT) ? KMM_X576_MINB : 1;
+}
+
 template <typename R, int N1, int N2, int ZB, int NT, bool STAT = false>
-__global__ void __launch_bounds__(NT) k_xphys2(typename Cpx<R>::T *__restrict__ mid, FftPlan pl, X2Args a_) {
+__global__ void __launch_bounds__(NT, (x_min_blocks<R, N1 * N2, STAT>())) k_xphys2(typename Cpx<R>::T *__restrict__ mid, FftPlan pl, X2Args a_) {
   using C = typename Cpx<R>::T;
   constexpr int N = N1 * N2, LD = ip_lda<N1, N2>();
   extern __shared__ __align__(16) unsigned char smem_raw[];
