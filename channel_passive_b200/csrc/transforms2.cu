@@ -165,8 +165,14 @@ struct X2Args {
 // registers a thread, 3 blocks (12 warps) an SM.  5 blocks (96 registers, a 200-byte spill) took
 // the pass from 2.35 to 2.01 ms on the 384x257x384 grid (4 blocks, no spill: 2.04 ms).  The
 // statistics variant keeps the default: a cap spills more there.
+// At N = 288 (16 x 18) the FP32 step pass took 80 registers, 6 blocks an SM; 8 blocks (64
+// registers, a 56-byte spill) took it from 0.2345 to 0.2155 ms on the 192x129x192 grid
+// (7 blocks: 0.2167 ms).
+#ifndef KMM_X288_MINB
+#define KMM_X288_MINB 8
+#endif
 template <typename R, int N, bool STAT> constexpr int x_min_blocks() {
-  return (sizeof(R) == 4 && N >= 576 && !STAT) ? KMM_X576_MINB : 1;
+  return (sizeof(R) != 4 || STAT) ? 1 : N >= 576 ? KMM_X576_MINB : N == 288 ? KMM_X288_MINB : 1;
 }
 
 template <typename R, int N1, int N2, int ZB, int NT, bool STAT = false>
