@@ -666,6 +666,22 @@ def run_kmm(args):
     return 0
 
 
+def free_port() -> int:
+    import socket
+    with socket.socket(socket.AF_INET, socket.SOCK_STREAM) as s:
+        s.bind(("127.0.0.1", 0))
+        return s.getsockname()[1]
+
+
+def relaunch_ranks(n: int, argv) -> int:
+    """`bench.py --gpus N` started without a launcher: run the same command as N ranks (one
+    process per GPU) under torch.distributed.run on this node, so N independent channels are
+    stepped and timed as max over ranks.  Rank 0's JSON line is the output."""
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", f"--nproc-per-node={n}",
+           "--master-addr=127.0.0.1", f"--master-port={free_port()}", os.path.abspath(__file__)] + list(argv)
+    return subprocess.call(cmd)
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -689,6 +705,8 @@ def main(argv=None):
     args = ap.parse_args(argv)
     if args.warmup < 3:
         args.warmup = 3
+    if args.gpus > 1 and "WORLD_SIZE" not in os.environ:
+        return relaunch_ranks(args.gpus, sys.argv[1:] if argv is None else list(argv))
     if args.impl == "reference":
         return run_reference(args)
     return run_kmm(args)

@@ -18,7 +18,7 @@ KMM_ERR_CUDA = 2
 KMM_ERR_DT = 3
 KMM_ERR_NONFINITE = 4
 KMM_ERR_ARG = 5
-KMM_ERR_TIMEOUT = 6
+KMM_ERR_TIMEOUT = 6  # reserved
 
 KMM_PREC_FP64 = 0
 KMM_PREC_MIXED = 1
@@ -100,6 +100,7 @@ SIGNATURES = {
     "kmm_get_dt": (C.c_int, [_P, _D]),
     "kmm_set_dt": (C.c_int, [_P, C.c_double]),
     "kmm_set_control_gains": (C.c_int, [_P, C.POINTER(C.c_float)]),
+    "kmm_set_control": (C.c_int, [_P, C.c_double, C.POINTER(C.c_float), C.c_double]),
     "kmm_dev_y_to_x": (C.c_int, [_P, _P, _P, _P]),
     "kmm_dev_x_to_y": (C.c_int, [_P, _P, _P, C.c_int, _P]),
     "kmm_dev_dft_x_realspace": (C.c_int, [_P, _P, C.c_int, _P, _P]),

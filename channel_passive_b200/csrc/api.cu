@@ -4,7 +4,7 @@
 //                    (module_labs.f90:77-238, module_runge_kutta.f90:28-54,
 //                    module_ppdfftw.f90:499-588)
 // kmm_time_march     time_march (time_march.f90:36-128), one substep
-// kmm_step           the main.f90:262-321 loop body (three substeps) from a CUDA graph
+// kmm_step           the main.f90:134-193 loop body (three substeps) from a CUDA graph
 // kmm_upload_state / kmm_download_state   the Y-pencil U / RK_STORE arrays
 #include <cuda_runtime.h>
 
@@ -41,7 +41,7 @@ OpsOffsets ops_offsets(int bw, int ny) {
 
 namespace {
 
-constexpr double kPiF = 3.14159265358979323;  // module_global_variable.f90:98
+constexpr double kPiF = 3.14159265358979323;  // module_global_variable.f90:28
 
 #define KMM_CUDA(call)                                                                   \
   do {                                                                                   \
@@ -302,8 +302,8 @@ int ensure_graph(Handle &h) {
 
 void finish_step_scalars(kmm_scalars *out) {
   if (!out) return;
-  out->phi_dpdx[3] = (out->phi_dpdx[0] + out->phi_dpdx[1] + out->phi_dpdx[2]) / out->dt;  // main.f90:275
-  out->phi_dtdx[3] = (out->phi_dtdx[0] + out->phi_dtdx[1] + out->phi_dtdx[2]) / out->dt;  // main.f90:276
+  out->phi_dpdx[3] = (out->phi_dpdx[0] + out->phi_dpdx[1] + out->phi_dpdx[2]) / out->dt;  // main.f90:147
+  out->phi_dtdx[3] = (out->phi_dtdx[0] + out->phi_dtdx[1] + out->phi_dtdx[2]) / out->dt;  // main.f90:148
 }
 
 }  // namespace
@@ -417,7 +417,7 @@ int kmm_create(const kmm_config *cfg, kmm_handle **out) {
   h->ns = (int64_t)h->ny * h->nmodes;
   h->nm = (int64_t)h->ny * h->nz32 * h->nxh;
   h->mixed = cfg->precision == KMM_PREC_MIXED;
-  // read_input_file.f90:199-221
+  // read_input_file.f90:94-116
   const double lx = cfg->lmfx * 2 * kPiF, lz = cfg->lmfz * 2 * kPiF;
   h->dxr = (double)cfg->nx / lx;
   h->dzr = (double)cfg->nz / lz;
@@ -455,7 +455,9 @@ int kmm_create(const kmm_config *cfg, kmm_handle **out) {
     delete h;
     return KMM_ERR_CUDA;
   }
-  if (cudaSetDevice(cfg->device) != cudaSuccess) {
+  // the handle's resources live on cfg->device; the caller's current device is restored on return
+  DeviceGuard dg(cfg->device);
+  if (!dg.ok) {
     set_error("cudaSetDevice failed");
     delete h;
     return KMM_ERR_CUDA;
@@ -534,6 +536,7 @@ int kmm_create(const kmm_config *cfg, kmm_handle **out) {
 int kmm_destroy(kmm_handle *hh) {
   if (!hh) return KMM_OK;
   Handle *h = reinterpret_cast<Handle *>(hh);
+  DeviceGuard dg(h->cfg.device);
   if (h->gexec) cudaGraphExecDestroy(h->gexec);
   if (h->graph) cudaGraphDestroy(h->graph);
   if (h->stream) cudaStreamSynchronize(h->stream);
@@ -590,6 +593,7 @@ int kmm_upload_state(kmm_handle *hh, const double *U, int nf, const double *rk, 
     return KMM_ERR_ARG;
   }
   Handle &h = *reinterpret_cast<Handle *>(hh);
+  DeviceGuard dg(h.cfg.device);
   int rc = upload_fields(h, U, nf, rk, h.stream);
   if (rc) return rc;
   KMM_CUDA(cudaStreamSynchronize(h.stream));
@@ -602,6 +606,7 @@ int kmm_download_state(kmm_handle *hh, double *U, int nf, double *rk) {
     return KMM_ERR_ARG;
   }
   Handle &h = *reinterpret_cast<Handle *>(hh);
+  DeviceGuard dg(h.cfg.device);
   int rc = download_fields(h, U, nf, rk, h.stream);
   if (rc) return rc;
   KMM_CUDA(cudaStreamSynchronize(h.stream));
@@ -614,6 +619,7 @@ int kmm_set_initial_data_uvw(kmm_handle *hh, const double *U, int nf, double dt)
     return KMM_ERR_ARG;
   }
   Handle &h = *reinterpret_cast<Handle *>(hh);
+  DeviceGuard dg(h.cfg.device);
   int rc = upload_fields(h, U, nf, nullptr, h.stream);
   if (rc) return rc;
   KMM_CUDA(launch_init_stores(h, h.stream));
@@ -627,6 +633,7 @@ int kmm_time_march(kmm_handle *hh, int s, kmm_scalars *out) {
     return KMM_ERR_ARG;
   }
   Handle &h = *reinterpret_cast<Handle *>(hh);
+  DeviceGuard dg(h.cfg.device);
   int rc = enqueue_substep(h, s, h.stream);
   if (rc) return rc;
   KMM_CUDA(cudaStreamSynchronize(h.stream));
@@ -638,6 +645,7 @@ int kmm_time_march(kmm_handle *hh, int s, kmm_scalars *out) {
 int kmm_step_async(kmm_handle *hh, int nsteps) {
   if (!hh || nsteps < 0) return KMM_ERR_ARG;
   Handle &h = *reinterpret_cast<Handle *>(hh);
+  DeviceGuard dg(h.cfg.device);
   int rc = ensure_graph(h);
   if (rc) return rc;
   for (int i = 0; i < nsteps; ++i) KMM_CUDA(cudaGraphLaunch(h.gexec, h.stream));
@@ -647,6 +655,7 @@ int kmm_step_async(kmm_handle *hh, int nsteps) {
 int kmm_sync(kmm_handle *hh, kmm_scalars *out) {
   if (!hh) return KMM_ERR_ARG;
   Handle &h = *reinterpret_cast<Handle *>(hh);
+  DeviceGuard dg(h.cfg.device);
   KMM_CUDA(cudaStreamSynchronize(h.stream));
   int err = 0, rc;
   if ((rc = read_scalars(h, out, &err))) return rc;
@@ -739,6 +748,7 @@ int kmm_step_host(kmm_handle *hh, double *U, int nf, double *rk, int nsteps, kmm
     return KMM_ERR_ARG;
   }
   Handle &h = *reinterpret_cast<Handle *>(hh);
+  DeviceGuard dg(h.cfg.device);
   if (!rk) return step_host_pipelined(h, U, nsteps, out);
   int rc = upload_fields(h, U, nf, rk, h.stream);
   if (rc) return rc;
@@ -756,6 +766,7 @@ int kmm_get_pressure(kmm_handle *hh, double *P) {
     return KMM_ERR_ARG;
   }
   Handle &h = *reinterpret_cast<Handle *>(hh);
+  DeviceGuard dg(h.cfg.device);
   double2 *planes = h.staging, *ref = h.staging + h.ns;
   // the wall values nu d2v/dy2 of the state's v into dvw (get_statistics_1's dv/dy call)
   KMM_CUDA(launch_ydiff(h, 2, h.stream));
@@ -778,6 +789,7 @@ int kmm_get_statistics(kmm_handle *hh, double *lines, double *spec_kx, double *s
     return KMM_ERR_ARG;
   }
   Handle &h = *reinterpret_cast<Handle *>(hh);
+  DeviceGuard dg(h.cfg.device);
   const StatLayout L = stat_layout(h);
   if (!h.stat) {
     int rc;
@@ -843,6 +855,7 @@ int kmm_get_stream(const kmm_handle *hh, void **stream) {
 int kmm_profile_step(kmm_handle *hh, int nsteps, double *ms, int *launches) {
   if (!hh || nsteps <= 0 || !ms || !launches) return KMM_ERR_ARG;
   Handle &h = *reinterpret_cast<Handle *>(hh);
+  DeviceGuard dg(h.cfg.device);
   const int per_step = 3 * KMM_NKERNEL;
   const int nmax = per_step * nsteps;
   std::vector<cudaEvent_t> ev(2 * nmax, nullptr);
@@ -878,6 +891,7 @@ int kmm_profile_step(kmm_handle *hh, int nsteps, double *ms, int *launches) {
 int kmm_get_dt(const kmm_handle *hh, double *dt) {
   if (!hh || !dt) return KMM_ERR_ARG;
   const Handle &h = *reinterpret_cast<const Handle *>(hh);
+  DeviceGuard dg(h.cfg.device);
   KMM_CUDA(cudaMemcpy(dt, &h.dsc->dt, sizeof(double), cudaMemcpyDeviceToHost));
   return KMM_OK;
 }
@@ -890,18 +904,60 @@ int kmm_set_dt(kmm_handle *hh, double dt) {
 int kmm_set_control_gains(kmm_handle *hh, const float *gains) {
   if (!hh) return KMM_ERR_ARG;
   Handle &h = *reinterpret_cast<Handle *>(hh);
+  DeviceGuard dg(h.cfg.device);
   std::vector<float> g((size_t)h.nmodes, 1.0f);
   if (gains) {
     // input (nxh, nz) Fortran order = mode index kz * nxh + kx, the device order
     std::memcpy(g.data(), gains, g.size() * sizeof(float));
   }
+  // steps already queued on the handle's stream read the gains: let them finish first
+  KMM_CUDA(cudaStreamSynchronize(h.stream));
   KMM_CUDA(cudaMemcpy(h.gains, g.data(), g.size() * sizeof(float), cudaMemcpyHostToDevice));
+  return KMM_OK;
+}
+
+int kmm_set_control(kmm_handle *hh, double amp, const float *gains, double yd) {
+  if (!hh) return KMM_ERR_ARG;
+  if (!std::isfinite(amp)) {
+    set_error("kmm_set_control: non-finite amplitude");
+    return KMM_ERR_ARG;
+  }
+  Handle &h = *reinterpret_cast<Handle *>(hh);
+  DeviceGuard dg(h.cfg.device);
+  if (amp != 0.0) {
+    std::string err;
+    HostOps ops = h.ops;  // the handle keeps its weights if the new plane is refused
+    const int rc = build_control_weights(ops, yd, err);
+    if (rc) {
+      set_error("kmm_set_control: " + err);
+      return rc;
+    }
+    const OpsOffsets off = ops_offsets(h.bw, h.ny);
+    KMM_CUDA(cudaStreamSynchronize(h.stream));
+    KMM_CUDA(cudaMemcpy(h.dops + off.wlo, ops.wlo.data(), sizeof(double) * (size_t)h.ny, cudaMemcpyHostToDevice));
+    KMM_CUDA(cudaMemcpy(h.dops + off.whi, ops.whi.data(), sizeof(double) * (size_t)h.ny, cudaMemcpyHostToDevice));
+    h.ops.wlo = ops.wlo;
+    h.ops.whi = ops.whi;
+    h.cfg.control_yd = yd;
+  }
+  const int rc = kmm_set_control_gains(hh, gains);
+  if (rc) return rc;
+  if (amp != h.cfg.control_amp) {
+    // the amplitude is a kernel argument captured in the step graph: capture it again
+    KMM_CUDA(cudaStreamSynchronize(h.stream));
+    if (h.gexec) cudaGraphExecDestroy(h.gexec);
+    if (h.graph) cudaGraphDestroy(h.graph);
+    h.gexec = nullptr;
+    h.graph = nullptr;
+    h.cfg.control_amp = amp;
+  }
   return KMM_OK;
 }
 
 int kmm_dev_y_to_x(kmm_handle *hh, const double *u, void *xp, void *stream) {
   if (!hh || !u || !xp) return KMM_ERR_ARG;
   Handle &h = *reinterpret_cast<Handle *>(hh);
+  DeviceGuard dg(h.cfg.device);
   cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
   KMM_CUDA(launch_ref_to_planes(reinterpret_cast<const double2 *>(u), h.staging, 1, h.nmodes, h.ny, st));
   KMM_CUDA(launch_zinv(h, h.staging, xp, 1, st));
@@ -911,6 +967,7 @@ int kmm_dev_y_to_x(kmm_handle *hh, const double *u, void *xp, void *stream) {
 int kmm_dev_x_to_y(kmm_handle *hh, const void *xp, double *u, int rescale, void *stream) {
   if (!hh || !u || !xp) return KMM_ERR_ARG;
   Handle &h = *reinterpret_cast<Handle *>(hh);
+  DeviceGuard dg(h.cfg.device);
   cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
   KMM_CUDA(launch_zfwd(h, xp, h.staging, 1, rescale ? h.rescale : 1.0, true, st));
   KMM_CUDA(launch_planes_to_ref(h.staging, reinterpret_cast<double2 *>(u), 1, h.nmodes, h.ny, st));
@@ -920,6 +977,7 @@ int kmm_dev_x_to_y(kmm_handle *hh, const void *xp, double *u, int rescale, void 
 int kmm_dev_dft_x_realspace(kmm_handle *hh, void *xp, int s, double *velmax_dev, void *stream) {
   if (!hh || !xp || s < 1 || s > 3) return KMM_ERR_ARG;
   Handle &h = *reinterpret_cast<Handle *>(hh);
+  DeviceGuard dg(h.cfg.device);
   cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
   const size_t r2 = h.mixed ? sizeof(float2) : sizeof(double2);
   const size_t fb = r2 * (size_t)h.nm;
@@ -942,6 +1000,7 @@ int kmm_dev_wavespace(kmm_handle *hh, double *U, double *rk, int s, double dt, k
                       void *stream) {
   if (!hh || !U || !rk || s < 1 || s > 3) return KMM_ERR_ARG;
   Handle &h = *reinterpret_cast<Handle *>(hh);
+  DeviceGuard dg(h.cfg.device);
   cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
   const double2 *Uc = reinterpret_cast<const double2 *>(U);
   const int pslots[8] = {0, 1, 2, 3, 4, 6, 7, 8};
@@ -968,6 +1027,7 @@ int kmm_dev_wavespace(kmm_handle *hh, double *U, double *rk, int s, double dt, k
 int kmm_dev_labs_lu(kmm_handle *hh, double *a, int nm, void *stream) {
   if (!hh || !a || nm <= 0) return KMM_ERR_ARG;
   Handle &h = *reinterpret_cast<Handle *>(hh);
+  DeviceGuard dg(h.cfg.device);
   KMM_CUDA(launch_labs_lu(h, a, nm, reinterpret_cast<cudaStream_t>(stream)));
   return KMM_OK;
 }
@@ -975,6 +1035,7 @@ int kmm_dev_labs_lu(kmm_handle *hh, double *a, int nm, void *stream) {
 int kmm_dev_labs_bs(kmm_handle *hh, const double *a, double *b, int nm, void *stream) {
   if (!hh || !a || !b || nm <= 0) return KMM_ERR_ARG;
   Handle &h = *reinterpret_cast<Handle *>(hh);
+  DeviceGuard dg(h.cfg.device);
   KMM_CUDA(launch_labs_bs(h, a, reinterpret_cast<double2 *>(b), nm, reinterpret_cast<cudaStream_t>(stream)));
   return KMM_OK;
 }
@@ -982,6 +1043,7 @@ int kmm_dev_labs_bs(kmm_handle *hh, const double *a, double *b, int nm, void *st
 int kmm_dev_labs_mat_mul(kmm_handle *hh, int which, const double *x, double *b, int nm, void *stream) {
   if (!hh || !x || !b || nm <= 0 || which < 0 || which > 2) return KMM_ERR_ARG;
   Handle &h = *reinterpret_cast<Handle *>(hh);
+  DeviceGuard dg(h.cfg.device);
   KMM_CUDA(launch_labs_mat_mul(h, which, reinterpret_cast<const double2 *>(x), reinterpret_cast<double2 *>(b), nm,
                                reinterpret_cast<cudaStream_t>(stream)));
   return KMM_OK;

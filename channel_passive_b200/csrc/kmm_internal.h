@@ -144,6 +144,26 @@ cudaError_t launch_labs_mat_mul(Handle &h, int which, const double2 *x, double2 
                                 cudaStream_t st);
 
 void set_error(const std::string &msg);
+
+// Makes a handle's device current for the lifetime of the guard and gives the caller's current
+// device back on destruction.  Every handle entry point holds one, so handles on several GPUs,
+// or a caller that changes the current device between calls, always launch on the handle's own
+// device (its streams, graph and buffers belong to it).
+struct DeviceGuard {
+  int prev = -1;
+  bool ok = true;
+  explicit DeviceGuard(int dev) {
+    if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
+    if (prev != dev) ok = cudaSetDevice(dev) == cudaSuccess;
+  }
+  ~DeviceGuard() {
+    int cur = -1;
+    if (prev >= 0 && cudaGetDevice(&cur) == cudaSuccess && cur != prev) cudaSetDevice(prev);
+  }
+  DeviceGuard(const DeviceGuard &) = delete;
+  DeviceGuard &operator=(const DeviceGuard &) = delete;
+};
+
 // Sets the dynamic shared-memory limits of every kernel instantiation the handle uses.
 void prepare_kernels(Handle &h);
 void convert_planes_d2f(const double2 *src, float2 *dst, int64_t n, cudaStream_t st);

@@ -17,6 +17,7 @@
 // A_m x = rhs_m in place (the kernels of labs.cuh).
 #include <cuda_runtime.h>
 
+#include <cstdint>
 #include <mutex>
 #include <string>
 
@@ -31,6 +32,9 @@ namespace {
 // contents, and calls that overlap on the GPU race on it.
 __device__ __align__(256) double g_noalloc_band[KMM_NOALLOC_MAX_DOUBLES];
 
+// The array's device address per device ordinal, looked up once.  A cudaDeviceReset unloads the
+// module and invalidates these addresses; a process that resets a device must not call this
+// entry point on that device again.
 constexpr int kMaxDevices = 64;
 std::mutex g_mutex;
 double *g_band_ptr[kMaxDevices] = {};
@@ -76,6 +80,10 @@ extern "C" int kmm_helmholtz_solve_noalloc(int ny, int bw, int nmodes, const dou
   }
   if (bw < kMinBw || bw > kMaxBw || ny < 4 * bw + 2 || nmodes <= 0) {
     set_error("kmm_helmholtz_solve_noalloc: need 2 <= bw <= 7, ny >= 4*bw+2 and nmodes > 0");
+    return KMM_ERR_ARG;
+  }
+  if ((reinterpret_cast<uintptr_t>(rhs) & 15u) != 0) {
+    set_error("kmm_helmholtz_solve_noalloc: rhs must be 16-byte aligned (it is read as complex doubles)");
     return KMM_ERR_ARG;
   }
   const long long need = (long long)(2 * bw + 1) * ny * nmodes;

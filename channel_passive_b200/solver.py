@@ -2,12 +2,12 @@
 
 The names follow the reference routines they stand in for:
 
-* ``read_input_file``  -> read_input_file.f90:119-353 (positional ``input`` file)
+* ``read_input_file``  -> read_input_file.f90:38-89 (positional ``input`` file)
 * ``labs_fill_full``   -> LABS_fill_full (labs_fill_full.cpp:35-195)
 * ``Channel``          -> the module state set up by LABS_initialize / RK3_initialize /
   ppdfftw_initialize, with ``time_march`` (time_march.f90:36-128),
   ``set_initial_data_uvw`` (initial_step.f90:139-179) and the main-loop step
-  (main.f90:262-321) as methods.
+  (main.f90:134-193) as methods.
 
 Arrays use the reference layout: complex128 numpy arrays of shape (nf, nz, nxh, ny)
 (= Fortran U(ny, nxh, nz, nf)); RK stores (3, nz, nxh, ny).  Errors raise
@@ -78,7 +78,7 @@ class Config:
 
 
 def read_input_file(path: str) -> Config:
-    """Parse the reference's positional ``input`` file (read_input_file.f90:144-193)."""
+    """Parse the reference's positional ``input`` file (read_input_file.f90:38-89)."""
     lib = _lib.load()
     c = KmmConfig()
     check(lib.kmm_read_input_file(str(path).encode(), C.byref(c)))
@@ -230,6 +230,21 @@ class Channel:
         if g.shape != (self.config.nz, self.config.nxh):
             raise ValueError("gains must have shape (nz, nxh)")
         check(self._lib.kmm_set_control_gains(self._h, g.ctypes.data_as(C.POINTER(C.c_float))))
+
+    def set_control(self, amp: float, gains: np.ndarray | None = None, y_d: float | None = None):
+        """kmm_set_control: opposition amplitude, per-mode gains (nz, nxh) or None (= 1), and the
+        detection plane y_d (default: the configured one)."""
+        yd = self.config.control_yd if y_d is None else float(y_d)
+        gp = None
+        if gains is not None:
+            g = np.ascontiguousarray(gains, dtype=np.float32)
+            if g.shape != (self.config.nz, self.config.nxh):
+                raise ValueError("gains must have shape (nz, nxh)")
+            gp = g.ctypes.data_as(C.POINTER(C.c_float))
+        check(self._lib.kmm_set_control(self._h, float(amp), gp, yd))
+        self.config.control_amp = float(amp)
+        if amp != 0.0:
+            self.config.control_yd = yd
 
     # -- time stepping ----------------------------------------------------------------
     def time_march(self, rk_substep: int) -> dict:

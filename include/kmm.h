@@ -16,7 +16,7 @@
  * Wavenumber order: kx = 0..nx/2-1; kz = 0..nz/2, -nz/2+1..-1 (module_ppdfftw.f90:347-384).
  *
  * Status codes: 0 = success; nonzero = failure with a message from kmm_last_error().  The
- * reference aborts through mpi_abort on the same conditions (read_input_file.f90:335-343,
+ * reference aborts through mpi_abort on the same conditions (read_input_file.f90:230-238,
  * dft_x_realspace.f90:494-497); a Fortran shim converts a nonzero status into mpi_abort.
  */
 #ifndef KMM_H
@@ -30,12 +30,12 @@ extern "C" {
 #endif
 
 #define KMM_OK 0
-#define KMM_ERR_CONFIG 1      /* invalid configuration (read_input_file.f90:251-333 checks) */
+#define KMM_ERR_CONFIG 1      /* invalid configuration (read_input_file.f90:146-228 checks) */
 #define KMM_ERR_CUDA 2        /* CUDA runtime error or no device */
 #define KMM_ERR_DT 3          /* dt <= 1e-14 or dt > 1e5 (dft_x_realspace.f90:494-497) */
 #define KMM_ERR_NONFINITE 4   /* NaN / Inf in the velocity maximum or in uploaded state */
 #define KMM_ERR_ARG 5         /* null pointer, bad substep, size mismatch */
-#define KMM_ERR_TIMEOUT 6     /* a bounded device wait gave up */
+#define KMM_ERR_TIMEOUT 6     /* reserved: no entry point waits on the device with a limit yet */
 
 #define KMM_PREC_FP64 0       /* every kernel in FP64 */
 #define KMM_PREC_MIXED 1      /* FP32 transforms/products, FP64 state, v-influence and mean modes */
@@ -43,12 +43,12 @@ extern "C" {
 #define KMM_GRID_SINE 0       /* the reference's breakpoint map (labs_fill_full.cpp:92) */
 #define KMM_GRID_TANH 1       /* the commented tanh map (labs_fill_full.cpp:89) */
 
-/* Mirrors the positional `input` file read by read_input_file.f90:144-193, plus the
+/* Mirrors the positional `input` file read by read_input_file.f90:38-89, plus the
  * switches this implementation adds (fixed dt, precision, opposition control). */
 typedef struct kmm_config {
   int32_t nx, ny, nz;         /* modes in x, collocation points in y, modes in z */
   int32_t no_of_field;        /* must be 10 (fields 1..10 are used, wavespace.f90:29) */
-  int32_t rk_scheme;          /* must be 3 (read_input_file.f90:295-300) */
+  int32_t rk_scheme;          /* must be 3 (read_input_file.f90:190-195) */
   int32_t labs_k;             /* B-spline order minus one (GSL order = labs_k+1) */
   double lmfx, lmfy, lmfz;    /* Lx = 2 pi lmfx, Ly = 2 lmfy, Lz = 2 pi lmfz */
   double stretch;             /* breakpoint stretching factor */
@@ -65,7 +65,7 @@ typedef struct kmm_config {
   int32_t reserved[7];
 } kmm_config;
 
-/* Per-step diagnostics printed by main.f90:278-280. */
+/* Per-step diagnostics printed by main.f90:147-151. */
 typedef struct kmm_scalars {
   double dt;                  /* time step used by the last substep */
   double velmax;              /* max(|u| dxr + |v| dyr + |w| dzr) of the last substep 1 */
@@ -92,7 +92,7 @@ const char *kmm_last_error(void);
 /* Fills the reference defaults (single rank, Re_tau 180 style channel). */
 int kmm_config_default(kmm_config *cfg);
 
-/* Parses the positional `input` text file (read_input_file.f90:119-193) into cfg. */
+/* Parses the positional `input` text file (read_input_file.f90:38-89) into cfg. */
 int kmm_read_input_file(const char *path, kmm_config *cfg);
 
 /* LABS_initialize + RK3_initialize + ppdfftw_initialize (module_labs.f90:77-238,
@@ -126,7 +126,7 @@ int kmm_set_initial_data_uvw(kmm_handle *h, const double *U, int nf, double dt);
  * out may be NULL. */
 int kmm_time_march(kmm_handle *h, int rk_substep, kmm_scalars *out);
 
-/* nsteps full RK3 steps (the main.f90:262-321 loop body without I/O), replayed from a
+/* nsteps full RK3 steps (the main.f90:134-193 loop body without I/O), replayed from a
  * CUDA graph; out receives the diagnostics of the last step. */
 int kmm_step(kmm_handle *h, int nsteps, kmm_scalars *out);
 
@@ -208,6 +208,14 @@ int kmm_set_dt(kmm_handle *h, double dt);
 /* Opposition-control gains per mode, (nxh, nz) Fortran order, float; NULL resets to 1. */
 int kmm_set_control_gains(kmm_handle *h, const float *gains);
 
+/* Opposition control at the wall rows of the v solve (the hook of solve_v_f.f90:251-257, whose
+ * commented lines read v at a fixed collocation row): v_wall(kx, kz) = amp * gains(kx, kz) *
+ * v(kx, kz, y_d) at the bottom wall and with v at -y_d at the top wall.  amp = 0 turns the
+ * control off (the reference's behaviour); otherwise y_d must lie in (-1, 0).  gains as in
+ * kmm_set_control_gains (NULL = 1).  Waits for the handle's queued steps; the next kmm_step
+ * captures its graph again when amp changes. */
+int kmm_set_control(kmm_handle *h, double amp, const float *gains, double y_d);
+
 /* ---- Device-level building blocks (caller device pointers, reference layouts, cudaStream_t
  * passed as void*).  Complex buffers are interleaved doubles. ---- */
 
@@ -244,16 +252,20 @@ int kmm_dev_labs_mat_mul(kmm_handle *h, int which, const double *x, double *b, i
  * callers that may not allocate device memory (code running while a stream is captured into a
  * CUDA graph, hosts whose device memory is reserved up front by another allocator, loops that
  * cannot afford cudaMalloc's device-wide synchronisation).  It needs no handle.
- * For every mode m it builds A_m = a[m] D0 - b[m] D2 with Dirichlet first and last rows (the
- * left-hand side of solve_g / solve_t), factors it and solves A_m x = rhs_m in place.
- *   d0_band, d2_band  device, real (2*bw+1, ny) packed bands (module_labs.f90:301-328)
+ * For every mode m it builds A_m = a[m] D0 - b[m] D2 with Dirichlet first and last rows,
+ * factors it and solves A_m x = rhs_m in place.
+ *   d0_band, d2_band  device, real (2*bw+1, ny) column-major bands: entry r (1..2bw+1) of
+ *                     column j (1..ny) at band[(j-1)*(2bw+1) + r-1]; column j holds row j of the
+ *                     operator, the near-boundary rows packed as kmm_get_operators returns them
  *   a, b              device, nmodes doubles
- *   rhs               device, complex (ny, nmodes), mode fastest; overwritten by x
+ *   rhs               device, complex (ny, nmodes), mode fastest, 16-byte aligned; overwritten
+ *                     by x
  * The per-mode scratch band is a fixed array inside the library of KMM_NOALLOC_MAX_DOUBLES
  * doubles (16 MiB), held by every GPU that loads the library until exit; calls with
- * (2*bw+1)*ny*nmodes above it are rejected with KMM_ERR_ARG.  The first call on each device
- * looks the array up (cudaGetSymbolAddress); make that call before any stream capture.  All
- * calls share the array: calls that overlap on the GPU race. */
+ * (2*bw+1)*ny*nmodes above it, or a misaligned rhs, are rejected with KMM_ERR_ARG.  The first
+ * call on each device looks the array up (cudaGetSymbolAddress); make that call before any
+ * stream capture.  A cudaDeviceReset invalidates that lookup: do not call this entry point on a
+ * device after resetting it.  All calls share the array: calls that overlap on the GPU race. */
 #define KMM_NOALLOC_MAX_DOUBLES 2097152
 int kmm_helmholtz_solve_noalloc(int ny, int bw, int nmodes, const double *d0_band,
                                 const double *d2_band, const double *a, const double *b,

@@ -19,7 +19,7 @@ import numpy as np
 
 from . import bspline, labs
 
-PI_F = 3.14159265358979323  # module_global_variable.f90:98
+PI_F = 3.14159265358979323  # module_global_variable.f90:28
 
 # module_runge_kutta.f90:33-48 (alpha, beta, gamma, zeta) per substep 1..3
 RK_ALPHA = (29.0 / 96.0, -3.0 / 40.0, 1.0 / 6.0)
@@ -62,7 +62,7 @@ class Params:
     re_tau: float = 180.0
     gains: np.ndarray | None = None  # per-(kz,kx) control gains, default 1
 
-    # derived, read_input_file.f90:199-221
+    # derived, read_input_file.f90:94-116
     @property
     def nxh(self):
         return self.nx // 2
@@ -605,7 +605,7 @@ def time_march(U, RK, ops: Operators, p: Params, s: int, dt: float, sc: Scalars,
 
 
 def rk3_step(U, RK, ops, p, dt, sc=None, dyr=None, ctrl=None):
-    """Three substeps of main.f90:134-156; phi_dpdx(4) = sum/dt (main.f90:275-276)."""
+    """Three substeps of main.f90:134-156; phi_dpdx(4) = sum/dt (main.f90:147-148)."""
     sc = sc or Scalars()
     for s in (1, 2, 3):
         dt = time_march(U, RK, ops, p, s, dt, sc, dyr, ctrl)

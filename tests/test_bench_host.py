@@ -81,3 +81,22 @@ def test_clock_parser(tmp_path):
 def test_measured_peaks_has_a_number():
     peak, kind = bench.measured_peaks()
     assert peak > 1000 and kind in ("measured", "fallback")
+
+
+def test_gpus_n_without_launcher_relaunches_n_ranks(monkeypatch):
+    """`bench.py --gpus 4` with no WORLD_SIZE in the environment runs itself as 4 ranks under
+    torch.distributed.run on 127.0.0.1 (one process per GPU), passing the arguments through."""
+    seen = {}
+
+    def fake_call(cmd):
+        seen["cmd"] = cmd
+        return 0
+
+    monkeypatch.delenv("WORLD_SIZE", raising=False)
+    monkeypatch.setattr(bench.subprocess, "call", fake_call)
+    assert bench.main(["--gpus", "4", "--steps", "7", "--warmup", "3"]) == 0
+    cmd = seen["cmd"]
+    assert cmd[1:3] == ["-m", "torch.distributed.run"]
+    assert "--nproc-per-node=4" in cmd and "--master-addr=127.0.0.1" in cmd
+    assert cmd[-6:] == ["--gpus", "4", "--steps", "7", "--warmup", "3"]
+    assert cmd[-7].endswith("bench.py")
