@@ -9,7 +9,8 @@ nu = 1/2800, Pr = 0.71, opposition control A = -1 at y+ = 15, fixed dt = 0.01, s
 divergence-free random-phase initial condition (synthetic data).
 
   python bench.py [--gpus N --steps K --warmup W]          our implementation
-  python bench.py --impl reference [...]                    the CPU restatement (oracle port)
+  python bench.py --impl reference [...]                    the C/OpenMP FP64 restatement of the
+                                                            step (oracle/kmm_cpu.c) on the host threads
 
 Multi-GPU: one independent channel per rank (replicas; the step has no data-path
 collective), weak scaling; value = all ranks' steps / max-over-ranks time.
@@ -198,45 +199,8 @@ def barrier(dist, device):
 
 
 # ------------------------------------------------------------------------------------------
-# CPU reference (oracle port), sampled
+# CPU reference: the compiled FP64 restatement (oracle/kmm_cpu.c) on every host thread
 # ------------------------------------------------------------------------------------------
-def _transform_planes(U, ops, p, s, lo, hi):
-    """The oracle's y_to_x, dft_x_realspace and x_to_y on the wall-normal planes lo..hi-1."""
-    from oracle import kmm as okmm
-    Usub = np.ascontiguousarray(U[:, :, :, lo:hi])
-    Up = np.zeros((10, hi - lo, p.nz32, p.nxh), dtype=np.complex128)
-    for f in (0, 1, 2, 6):
-        Up[f] = okmm.y_to_x(Usub[f], p.nz32)
-    dyr = okmm.dyr_vector(ops.y, p.dy_factor)[lo:hi]
-    okmm.dft_x_realspace(Up, p.nx, s, p.dxr, p.dzr, dyr)
-    for f in (0, 1, 2, 3, 4, 6, 7, 8, 9):
-        okmm.x_to_y(Up[f], p.nz)
-
-
-# Per-process copy of the CPU workload for the pool workers (built by _pool_init).
-_POOL_STATE = {}
-
-
-def _pool_init(w):
-    _POOL_STATE["w"] = cpu_reference_setup(w)
-
-
-def _pool_ready(_):
-    return os.getpid()
-
-
-def _pool_task(task):
-    kind, s, lo, hi = task
-    p, ops, U, RK, ctrl = _POOL_STATE["w"]
-    if kind == "planes":
-        _transform_planes(U, ops, p, s, lo, hi)
-    else:
-        Us = np.ascontiguousarray(U[:, lo:hi]) * p.rescale
-        RKs = np.ascontiguousarray(RK[:, lo:hi])
-        _wavespace_block(Us, RKs, ops, p, s, 0.01, ctrl, lo, hi)
-    return hi - lo
-
-
 def host_threads():
     try:
         return len(os.sched_getaffinity(0))
@@ -244,84 +208,40 @@ def host_threads():
         return os.cpu_count() or 1
 
 
-class OraclePool:
-    """The oracle port on every host core: one single-threaded worker process per core, each
-    holding the seeded workload.  A sampled substep gives each worker `planes` wall-normal planes
-    of transforms and then `rows` kz rows (all kx) of wavespace solves; each phase's wall time
-    is scaled to the whole substep (both phases are linear in the planes / modes they process)."""
+class CpuReference:
+    """The workload on the host: the C/OpenMP FP64 restatement of the step (the same algorithm as
+    the numpy oracle, checked against it in tests/test_oracle_cpu.py) on all host threads, from
+    the same seeded IC with the RK stores built by set_initial_data_uvw.  Every timed step is a
+    complete RK3 step (three substeps, all 129 planes and all modes, the mean lines and the CFL
+    update) on the state the previous step left."""
 
-    def __init__(self, w, nproc=None, planes=4, rows=4):
-        import multiprocessing as mp
-        for var in ("OMP_NUM_THREADS", "OPENBLAS_NUM_THREADS", "MKL_NUM_THREADS"):
-            os.environ[var] = "1"  # one thread per worker; the pool supplies the parallelism
-        self.nproc = nproc or host_threads()
+    def __init__(self, w, nthreads=0):
+        from channel_passive_b200 import ic
+        from oracle import cpu as ocpu
+        from oracle import kmm as okmm
+        ocpu.build()
+        p = okmm.Params(nx=w["nx"], ny=w["ny"], nz=w["nz"], lmfx=w["lmfx"], lmfz=w["lmfz"],
+                        stretch=w["stretch"], nu=w["nu"], pr=w["pr"], fixed_dt=True,
+                        control_amp=w["control_amp"], control_yplus=15.0, re_tau=RE_TAU)
+        ops = okmm.make_operators(p)
+        ctrl = (*okmm.control_weights(ops, p), p.control_amp, None)
+        self.prob = ocpu.Problem(p, ops, ctrl, nthreads=nthreads)
+        self.U = ic.seeded_ic(p.nx, p.ny, p.nz, ops.y, p.lmfx, p.lmfz, seed=SEED)
+        self.RK = self.prob.set_initial_data_uvw(self.U)
+        self.threads = nthreads or ocpu.threads()
         self.w = w
-        self.planes, self.rows = planes, rows
-        self.pool = mp.get_context("spawn").Pool(self.nproc, initializer=_pool_init, initargs=(w,))
-        self.pool.map(_pool_ready, range(self.nproc), chunksize=1)
 
-    def close(self):
-        self.pool.terminate()
-        self.pool.join()
-
-    def _phase(self, kind, s, per, total):
-        n = min(self.nproc, max(1, total // per))
-        tasks = [(kind, s, i * per, min(total, (i + 1) * per)) for i in range(n)]
+    def step_seconds(self) -> float:
         t0 = time.perf_counter()
-        done = sum(self.pool.map(_pool_task, tasks, chunksize=1))
-        return (time.perf_counter() - t0) * total / done
+        self.prob.rk3(self.U, self.RK, 0.01, 1)
+        return time.perf_counter() - t0
 
-    def substep_seconds(self, s):
-        return (self._phase("planes", s, self.planes, self.w["ny"]) +
-                self._phase("rows", s, self.rows, self.w["nz"]))
-
-    def sample_text(self):
+    def sample_text(self, nsteps):
         w = self.w
-        return (f"oracle port (numpy FP64) on {self.nproc} worker processes, one per host thread: each step "
-                f"times one substep with {self.planes} y-planes of transforms and {self.rows} kz rows of "
-                f"wavespace solves per worker, each phase scaled to a full RK3 step of "
-                f"{w['nx']}x{w['ny']}x{w['nz']}")
-
-
-def _wavespace_block(U, RK, ops, p, s, dt, ctrl, lo, hi):
-    """The oracle's per-mode solves on the modes lo <= kz_index < hi (all kx); U and RK hold
-    those kz rows."""
-    from oracle import kmm as okmm
-    kxi, kzi = okmm.wavenumbers(p.nx, p.nz)
-    kzi = kzi[lo:hi]
-    KZ, KX = np.meshgrid(kzi, kxi, indexing="ij")
-    mask = ~((KX == 0) & (KZ == 0))
-    kx = KX[mask] * (1.0 / p.lmfx)
-    kz = KZ[mask] * (1.0 / p.lmfz)
-
-    def lines(slot, arr=U):
-        return np.ascontiguousarray(arr[slot][mask].T)
-
-    u1, u2, u3, u4, u5, u7, u8, u9, u10 = (lines(i) for i in (0, 1, 2, 3, 4, 6, 7, 8, 9))
-    sg, sp, st = lines(0, RK), lines(1, RK), lines(2, RK)
-    hg, hv, ht = okmm.hvhg(u1, u2, u3, u4, u5, u7, u8, u9, ops, kx, kz)
-    g, sg, Dg = okmm.solve_scalar_helmholtz(hg, sg, ops, kx, kz, (p.nu, None), s, dt)
-    vwall = None
-    if ctrl is not None:
-        w_lo, w_hi, amp, _ = ctrl
-        vwall = np.stack([amp * (w_lo @ u10), amp * (w_hi @ u10)])
-    v, dv, sp = okmm.solve_v_f(hv, sp, u10, ops, Dg, kx, kz, p.nu, s, dt, vwall)
-    okmm.solve_u_w(g, dv, kx, kz)
-    okmm.solve_scalar_helmholtz(ht, st, ops, kx, kz, (p.nu, p.pr), s, dt)
-
-
-def cpu_reference_setup(w):
-    from channel_passive_b200 import ic
-    from oracle import kmm as okmm
-    p = okmm.Params(nx=w["nx"], ny=w["ny"], nz=w["nz"], lmfx=w["lmfx"], lmfz=w["lmfz"],
-                    stretch=w["stretch"], nu=w["nu"], pr=w["pr"], fixed_dt=True,
-                    control_amp=w["control_amp"], control_yplus=15.0, re_tau=RE_TAU)
-    ops = okmm.make_operators(p)
-    U = ic.seeded_ic(p.nx, p.ny, p.nz, ops.y, p.lmfx, p.lmfz, seed=SEED)
-    RK = np.zeros((3, p.nz, p.nxh, p.ny), dtype=np.complex128)
-    RK[:] = U[[0, 1, 6]] * 0.1
-    ctrl = (*okmm.control_weights(ops, p), p.control_amp, None)
-    return p, ops, U, RK, ctrl
+        return (f"C/OpenMP FP64 restatement of the step (oracle/kmm_cpu.c; restatement, not the reference "
+                f"binary, which needs gfortran, MPI, FFTW, GSL and HDF5) on {self.threads} host threads: "
+                f"{nsteps} complete RK3 steps of {w['nx']}x{w['ny']}x{w['nz']} from the seeded IC, timed "
+                f"one by one with the state carried from step to step")
 
 
 def run_reference(args):
@@ -329,28 +249,26 @@ def run_reference(args):
     if rank != 0:
         return 0
     w = workload()
-    pool = OraclePool(w, planes=args.ref_planes, rows=args.ref_rows)
-    try:
-        for i in range(args.warmup):
-            pool.substep_seconds(1 + i % 3)
-        times = []
-        for i in range(args.steps):
-            # one "step" = a sampled substep, scaled to the full substep; an RK3 step is 3 of them
-            times.append(3.0 * pool.substep_seconds(1 + i % 3))
-    finally:
-        pool.close()
+    ref = CpuReference(w)
+    for _ in range(args.warmup):
+        t_w = ref.step_seconds()
+    # complete steps only; if the requested count would run past the time cap, fewer are run and
+    # "steps" says how many
+    k = max(1, min(args.steps, int(args.ref_seconds / max(t_w, 1e-9))))
+    times = [ref.step_seconds() for _ in range(k)]
     sec_per_step = float(np.mean(times))
     value = 1.0 / sec_per_step
-    sample = pool.sample_text()
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": 0,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": sec_per_step * 1e3,
+        "steps": k, "requested_steps": args.steps, "warmup": args.warmup, "ms_per_step": sec_per_step * 1e3,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic (seeded random-phase IC)",
         "config": {"workload": workload_name(w), "nx": w["nx"], "ny": w["ny"], "nz": w["nz"],
-                   "precision": "fp64", "parallelism": "cpu"},
-        "cpu_baseline": {"value": value, "unit": "steps/s", "cores": pool.nproc, "kind": "port", "sample": sample},
+                   "precision": "fp64", "parallelism": f"cpu x{ref.threads} threads"},
+        "cpu_baseline": {"value": value, "unit": "steps/s", "cores": ref.threads, "kind": "port",
+                         "sample": ref.sample_text(k)},
         "e2e": {"value": value, "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "timed_seconds": float(np.sum(times)),
     }
     print(json.dumps(line), flush=True)
     return 0
@@ -359,16 +277,17 @@ def run_reference(args):
 # ------------------------------------------------------------------------------------------
 # our implementation
 # ------------------------------------------------------------------------------------------
-def cpu_baseline_quick(w):
-    """Rank 0, N = 1: the oracle port on every host core, on a bounded sample (a few seconds)."""
-    pool = OraclePool(w)
-    try:
-        pool.substep_seconds(2)
-        t = min(pool.substep_seconds(s) for s in (1, 2, 3))
-    finally:
-        pool.close()
-    return {"value": 1.0 / (3.0 * t), "unit": "steps/s", "cores": pool.nproc, "kind": "port",
-            "sample": pool.sample_text() + "; best of substeps 1-3 after one warm-up"}
+def cpu_baseline_quick(w, seconds=12.0):
+    """Rank 0, N = 1: the CPU restatement on every host thread, complete RK3 steps for about
+    `seconds` after one warm-up step."""
+    ref = CpuReference(w)
+    ref.step_seconds()
+    times = []
+    while sum(times) < seconds and len(times) < 20:
+        times.append(ref.step_seconds())
+    t = float(np.mean(times))
+    return {"value": 1.0 / t, "unit": "steps/s", "cores": ref.threads, "kind": "port",
+            "sample": ref.sample_text(len(times)) + "; after one warm-up step"}
 
 
 # 16 independent channels of uneven sizes, mixed precision, Re_tau 180 (Lx 2 pi, Lz pi), CFL time
@@ -699,8 +618,8 @@ def main(argv=None):
                     help="RK3 steps timed on the 384x257x384 production grid (0: skip)")
     ap.add_argument("--ensemble-steps", type=int, default=50,
                     help="RK3 steps per channel of the 16-channel ensemble (0: skip)")
-    ap.add_argument("--ref-planes", type=int, default=4, help="y-planes per worker in a reference step")
-    ap.add_argument("--ref-rows", type=int, default=4, help="kz rows per worker in a reference step")
+    ap.add_argument("--ref-seconds", type=float, default=150.0,
+                    help="cap on the reference arm's timed seconds (complete steps only)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args(argv)
     if args.warmup < 3:

@@ -12,6 +12,7 @@ import numpy as np
 import pytest
 
 from channel_passive_b200 import Channel
+from oracle import cpu as ocpu
 from oracle import kmm as okmm
 from oracle import labs
 
@@ -29,15 +30,15 @@ def test_small_channel_fp64_100_steps_match_oracle():
         ch.set_initial_data_uvw(U, 0.01)
         out = ch.step(100)
         Ug, _ = ch.download_state()
+    # the compiled FP64 restatement (held to the numpy oracle in tests/test_oracle_cpu.py)
+    prob = ocpu.Problem(p, ops)
     Uo = U.copy()
-    RKo = okmm.set_initial_data_uvw(Uo, ops, p)
-    dyr = okmm.dyr_vector(ops.y, p.dy_factor)
-    dt, sc = 0.01, None
-    for _ in range(100):
-        dt, sc = okmm.rk3_step(Uo, RKo, ops, p, dt, None, dyr)
+    RKo = prob.set_initial_data_uvw(Uo)
+    _, scs = prob.rk3(Uo, RKo, 0.01, 100)
+    sc = scs[-1]
     errs = {s: rel_l2(Ug[s], Uo[s]) for s in STATE_SLOTS}
     assert max(errs.values()) < 1e-10, errs
-    assert abs(out["phi_dpdx"][3] - sc.phi_dpdx[3]) <= 1e-10 * abs(sc.phi_dpdx[3])
+    assert abs(out["phi_dpdx"][3] - sc["phi_dpdx"][3]) <= 1e-10 * abs(sc["phi_dpdx"][3])
 
 
 def _divergence(U, ops, p, modes):
