@@ -108,6 +108,14 @@ SIGNATURES = {
     "kmm_dev_labs_lu": (C.c_int, [_P, _P, C.c_int, _P]),
     "kmm_dev_labs_bs": (C.c_int, [_P, _P, _P, C.c_int, _P]),
     "kmm_dev_labs_mat_mul": (C.c_int, [_P, C.c_int, _P, _P, C.c_int, _P]),
+    "kmm_dev_hvhg": (C.c_int, [_P] + [_P] * 8 + [_P] * 3 + [_P, _P, C.c_int64, C.c_int64, C.c_int, _P]),
+    "kmm_dev_solve_g": (C.c_int, [_P] + [_P] * 4 + [_P] * 4 + [_P, _P, C.c_double, C.c_int, C.c_int,
+                                                             C.c_double, C.c_int, _P]),
+    "kmm_dev_solve_t": (C.c_int, [_P] + [_P] * 4 + [_P] * 4 + [_P, _P, C.c_double, C.c_double, C.c_int,
+                                                             C.c_int, C.c_double, C.c_int, _P]),
+    "kmm_dev_solve_v_f": (C.c_int, [_P] + [_P] * 8 + [_P] * 5 + [_P, _P, C.c_double, C.c_int, C.c_int,
+                                                               C.c_double, _P, C.c_int, _P]),
+    "kmm_dev_solve_u_w": (C.c_int, [_P, _P, _P, _P, _P, C.c_int, _P]),
     "kmm_helmholtz_solve_noalloc": (C.c_int, [C.c_int, C.c_int, C.c_int, _P, _P, _P, _P, _P, _P]),
 }
 

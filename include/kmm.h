@@ -248,6 +248,57 @@ int kmm_dev_labs_bs(kmm_handle *h, const double *a_modes, double *b, int nmodes,
 int kmm_dev_labs_mat_mul(kmm_handle *h, int which, const double *x, double *b, int nmodes,
                          void *stream); /* which: 0 = D0, 1 = D1, 2 = D2 */
 
+/* ---- The reference's per-mode routines with their argument lists, batched over modes ----
+ * Each call applies one routine to nmodes independent (kx, kz) modes on the handle's device, one
+ * GPU thread per mode, in the routine's own statement order through the packed-band LU,
+ * substitution and mat-vec of module_labs.f90.  The caller's buffers are the routine's scratch,
+ * as in the Fortran; nothing is allocated.
+ *   line arguments   device, complex doubles, ny values per mode, mode fastest: value y (1..ny)
+ *                    of mode m at complex index (y-1)*nmodes + m; 16-byte aligned
+ *   D0_lu, D0..D2    device, (2*bw+1, ny) Fortran bands shared by all modes (kmm_get_operators)
+ *   D_buf            device, one (2*bw+1, ny) band per mode: entry (r, j) of mode m at
+ *                    ((j-1)*(2bw+1) + r-1)*nmodes + m
+ *   kx, kz           device, nmodes physical wavenumbers (kx_int / LMFx, kz_int / LMFz)
+ *   rk_substep, dt   the module globals RK_SUBSTEP and dt (module_runge_kutta.f90:14-21)
+ * ny must equal the handle's; bw is the handle's. */
+
+/* hvhg (hvhg.f90:28-163): on exit u1 = h_g, u5 = h_v, u7 = h_theta; u2, u3, u4, u8, u9 are
+ * overwritten as in the reference.  nx32 and nz32 are accepted as hvhg.f90:28 declares them
+ * (its body does not read them). */
+int kmm_dev_hvhg(kmm_handle *h, double *u1, double *u2, double *u3, double *u4, double *u5, double *u7,
+                 double *u8, double *u9, const double *D0_lu, const double *D1, const double *D2,
+                 const double *kx, const double *kz, int64_t nx32, int64_t nz32, int nmodes, void *stream);
+
+/* solve_g (solve_g.f90:28-201): u1 = h_g on entry, g on exit; store_g = RK_STORE 1 of the
+ * substep in and out; buf1, buf2 scratch; D_buf receives the factored (1 + beta k^2) D0 - beta D2
+ * with Dirichlet rows, which solve_v_f reads next. */
+int kmm_dev_solve_g(kmm_handle *h, double *u1, double *store_g, double *buf1, double *buf2,
+                    const double *D0_lu, const double *D0, const double *D2, double *D_buf,
+                    const double *kx, const double *kz, double nu, int ny, int rk_substep, double dt,
+                    int nmodes, void *stream);
+
+/* solve_t (solve_t.f90:28-201): solve_g with the diffusivity nu / pr, for the passive scalar. */
+int kmm_dev_solve_t(kmm_handle *h, double *u7, double *store_t, double *buf1, double *buf2,
+                    const double *D0_lu, const double *D0, const double *D2, double *D_buf,
+                    const double *kx, const double *kz, double nu, double pr, int ny, int rk_substep,
+                    double dt, int nmodes, void *stream);
+
+/* solve_v_f (solve_v_f.f90:38-375): hv = h_v on entry; v, dv = dv/dy and store_phi on exit;
+ * buf1..buf3 scratch; D_buf holds solve_g's factors on entry and the v operator's on exit.
+ * vwall (device, complex [2][nmodes], may be NULL) gives v at the bottom and top wall rows of
+ * the v solve (the opposition-control hook at solve_v_f.f90:251-257); NULL gives the reference's
+ * zero walls.  vold is accepted as the reference declares it; only its commented control lines
+ * read it. */
+int kmm_dev_solve_v_f(kmm_handle *h, double *v, double *dv, double *hv, double *store_phi,
+                      double *buf1, double *buf2, double *buf3, const double *vold,
+                      const double *D0_lu, const double *D0, const double *D1, const double *D2,
+                      double *D_buf, const double *kx, const double *kz, double nu, int ny,
+                      int rk_substep, double dt, const double *vwall, int nmodes, void *stream);
+
+/* solve_u_w (solve_u_w.f90:18-42): g -> u and f (= dv/dy) -> w, in place. */
+int kmm_dev_solve_u_w(kmm_handle *h, double *g, double *f, const double *kx, const double *kz,
+                      int nmodes, void *stream);
+
 /* Allocation-free batched Helmholtz solve.  No counterpart in the reference: it exists for
  * callers that may not allocate device memory (code running while a stream is captured into a
  * CUDA graph, hosts whose device memory is reserved up front by another allocator, loops that
