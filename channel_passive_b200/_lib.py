@@ -116,6 +116,9 @@ SIGNATURES = {
     "kmm_dev_solve_v_f": (C.c_int, [_P] + [_P] * 8 + [_P] * 5 + [_P, _P, C.c_double, C.c_int, C.c_int,
                                                                C.c_double, _P, C.c_int, _P]),
     "kmm_dev_solve_u_w": (C.c_int, [_P, _P, _P, _P, _P, C.c_int, _P]),
+    "kmm_adjoint_forward": (C.c_int, [_P, C.c_int, C.c_double, C.c_double, _D]),
+    "kmm_adjoint_backward": (C.c_int, [_P, _D, _D]),
+    "kmm_adjoint_release": (C.c_int, [_P]),
     "kmm_helmholtz_solve_noalloc": (C.c_int, [C.c_int, C.c_int, C.c_int, _P, _P, _P, _P, _P, _P]),
 }
 

@@ -308,6 +308,12 @@ void finish_step_scalars(kmm_scalars *out) {
 
 }  // namespace
 
+int run_substep(Handle &h, int substep, cudaStream_t st) { return enqueue_substep(h, substep, st); }
+
+int read_device_scalars(Handle &h, kmm_scalars *out, int *dev_err) { return read_scalars(h, out, dev_err); }
+
+int capture_step_graph(Handle &h) { return ensure_graph(h); }
+
 }  // namespace kmm
 
 using namespace kmm;
@@ -541,6 +547,7 @@ int kmm_destroy(kmm_handle *hh) {
   if (h->graph) cudaGraphDestroy(h->graph);
   if (h->stream) cudaStreamSynchronize(h->stream);
   if (h->side) cudaStreamSynchronize(h->side);
+  adjoint_free(*h);
   void *ptrs[] = {h->S, h->RK, h->P, h->MID, h->dops, h->gains, h->vwall, h->zc,
                   h->ec, h->xr, h->ub, h->vf, h->dvw, h->w00, h->staging, h->stat,
                   h->fftpos, h->tw64, h->tw32, h->dsc};

@@ -72,6 +72,9 @@ int build_host_ops(int k_order, int ny, double stretch, double ly, int grid, Hos
 int build_control_weights(HostOps &ops, double yd, std::string &err);
 void host_band_lu(std::vector<double> &a, int bw, int n);
 
+// The discrete adjoint's buffers (adjoint.cu), made by the first kmm_adjoint_forward.
+struct Adjoint;
+
 struct Handle {
   kmm_config cfg{};
   int nx = 0, ny = 0, nz = 0, nxh = 0, nx32 = 0, nz32 = 0, bw = 0;
@@ -111,6 +114,7 @@ struct Handle {
 
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t gexec = nullptr;
+  Adjoint *adj = nullptr;                  // discrete adjoint state (adjoint.cu), or null
 };
 
 // Offsets of the operator arrays inside dops (doubles).
@@ -175,6 +179,10 @@ cudaError_t launch_zinv2(Handle &h, const double2 *src_planes, void *mid, int nf
 cudaError_t launch_xphys2(Handle &h, void *mid, int substep, cudaStream_t st, bool stat = false,
                           double *mom = nullptr);
 int xphys2_row_blocks(const Handle &h);
+// The transpose of the x pass at a base state (FP64 handles, four-step lengths): base_mid slots
+// 0..3 hold u, v, w, theta; lmid slots 0..7 hold the lambda of the products (times scale) on entry
+// and slots 0..3 the lambda of u, v, w, theta on exit.
+cudaError_t launch_xadj2(Handle &h, const double2 *base_mid, double2 *lmid, double scale, cudaStream_t st);
 cudaError_t launch_zfwd2(Handle &h, const void *mid, void *dst_planes, int nfield, double scale,
                          bool dst_fp64, cudaStream_t st);
 // Per-mode solves of one substep (wavespace_split.cu): hvhg, Helmholtz and assembly kernels on
@@ -210,5 +218,14 @@ int64_t vop_factor_doubles(const Handle &h);
 cudaError_t launch_vop_factor(Handle &h, cudaStream_t st);
 // Doubles of U factor storage per solver role.
 int64_t split_ub_role(const Handle &h);
+
+// One time_march substep enqueued kernel by kernel on st (api.cu), the device scalars read back,
+// and the step graph captured if it is not yet.
+int run_substep(Handle &h, int substep, cudaStream_t st);
+int read_device_scalars(Handle &h, kmm_scalars *out, int *dev_err);
+int capture_step_graph(Handle &h);
+
+// Frees the discrete adjoint's buffers (adjoint.cu).
+void adjoint_free(Handle &h);
 
 }  // namespace kmm

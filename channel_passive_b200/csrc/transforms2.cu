@@ -300,6 +300,81 @@ __global__ void __launch_bounds__(NT, (x_min_blocks<R, N1 * N2, STAT>())) k_xphy
   }
 }
 
+// Transpose of the x pass at a base state (the discrete adjoint; FP64), one block per x-line
+// row (z, y).  With <a, b> = Re sum conj(a) b over the kept kx coefficients and the plain sum
+// over physical points, the pass's three parts transpose as
+//   r2c + truncate  ->  lambda_phys(x) = Re sum_{k < nxh} lambda_k e^{+ikx}: a c2r of
+//                       b_0 = lambda_0, b_k = lambda_k / 2 (the same packed c2r as the forward);
+//   products        ->  their linearisation at the base u, v, w, theta (a c2r of base_mid);
+//   pad + c2r       ->  an r2c with weight 1 at kx = 0 (its imaginary part dropped) and 2 above.
+// base_mid slots 0..3 = u, v, w, theta of the base state (x-spectral, z-physical); lmid slots
+// 0..7 = lambda of f1..f5, f7..f9 on entry, multiplied by `scale` (the rescale of x_to_y), and
+// lambda of u, v, w, theta in slots 0..3 on exit.
+template <int N1, int N2>
+__global__ void __launch_bounds__(128) k_xadj2(const double2 *__restrict__ base_mid, double2 *__restrict__ lmid,
+                                              FftPlan pl, int nz32, int nxh, float rnxh, int64_t nm, double scale) {
+  using C = double2;
+  constexpr int N = N1 * N2, LD = ip_lda<N1, N2>(), NT = 128;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C *a = reinterpret_cast<C *>(smem_raw);  // 6 lines: base (u,v) (w,t); lambda (f1,f2) (f3,f4) (f5,f7) (f8,f9)
+  const int z = blockIdx.x, y = blockIdx.y;
+  const int64_t row0 = ((int64_t)y * nz32 + z) * nxh;
+  for (int w = threadIdx.x; w < 6 * N; w += NT) a[(w / N) * LD + (w % N)] = make_double2(0.0, 0.0);
+  __syncthreads();
+  for (int w = threadIdx.x; w < 6 * nxh; w += NT) {
+    const int t = (int)(((float)w + 0.5f) * rnxh), k = w - t * nxh;  // line t = 0..5, exact split
+    C x1, x2;
+    if (t < 2) {
+      x1 = base_mid[(2 * t) * nm + row0 + k];
+      x2 = base_mid[(2 * t + 1) * nm + row0 + k];
+    } else {
+      const double f = (k == 0 ? 1.0 : 0.5) * scale;
+      const C l1 = lmid[(2 * (t - 2)) * nm + row0 + k], l2 = lmid[(2 * (t - 2) + 1) * nm + row0 + k];
+      x1 = make_double2(f * l1.x, f * l1.y);
+      x2 = make_double2(f * l2.x, f * l2.y);
+    }
+    C *line = a + t * LD;
+    if (k == 0) {
+      line[0] = make_double2(x1.x, x2.x);
+    } else {
+      line[k] = make_double2(x1.x - x2.y, x1.y + x2.x);
+      line[N - k] = make_double2(x1.x + x2.y, x2.x - x1.y);
+    }
+  }
+  __syncthreads();
+  fft4_ip<double, N1, N2, 6, NT>(a, LD, tw_of<double>(pl), +1);
+  for (int p = threadIdx.x; p < N; p += NT) {
+    const C uv = a[p], wt = a[LD + p];
+    const double u = uv.x, v = uv.y, w = wt.x, t = wt.y;
+    const C l12 = a[2 * LD + p], l34 = a[3 * LD + p], l57 = a[4 * LD + p], l89 = a[5 * LD + p];
+    // f1 = uu - vv, f2 = uv, f3 = ww - vv, f4 = vw, f5 = uw, f7 = u t, f8 = v t, f9 = w t
+    const double lu = 2.0 * u * l12.x + v * l12.y + w * l57.x + t * l57.y;
+    const double lv = -2.0 * v * l12.x + u * l12.y - 2.0 * v * l34.x + w * l34.y + t * l89.x;
+    const double lw = 2.0 * w * l34.x + v * l34.y + u * l57.x + t * l89.y;
+    const double lt = u * l57.y + v * l89.x + w * l89.y;
+    a[2 * LD + p] = make_double2(lu, lv);
+    a[3 * LD + p] = make_double2(lw, lt);
+  }
+  __syncthreads();
+  fft4_ip<double, N1, N2, 2, NT>(a + 2 * LD, LD, tw_of<double>(pl), -1);
+  for (int w = threadIdx.x; w < 2 * nxh; w += NT) {
+    const int t = (int)(((float)w + 0.5f) * rnxh), k = w - t * nxh;
+    const C *line = a + (2 + t) * LD;
+    const C zk = line[k], zm = line[k == 0 ? 0 : N - k];
+    C A = make_double2(0.5 * (zk.x + zm.x), 0.5 * (zk.y - zm.y));
+    C B = make_double2(0.5 * (zk.y + zm.y), 0.5 * (zm.x - zk.x));
+    if (k == 0) {
+      A.y = 0.0;
+      B.y = 0.0;
+    } else {
+      A = make_double2(2.0 * A.x, 2.0 * A.y);
+      B = make_double2(2.0 * B.x, 2.0 * B.y);
+    }
+    lmid[(2 * t) * nm + row0 + k] = A;
+    lmid[(2 * t + 1) * nm + row0 + k] = B;
+  }
+}
+
 // ---- dispatch over the supported lengths ------------------------------------------------
 template <typename F> bool with_shape(int N, F &&f) {
   switch (N) {
@@ -387,6 +462,7 @@ cudaError_t prepare_transforms2() {
       set_smem(k_xphys2<float, N1, N2, F::ZB, F::ZT>, optin);
       set_smem(k_xphys2<double, N1, N2, D::ZB, D::ZT, true>, optin);
       set_smem(k_xphys2<float, N1, N2, F::ZB, F::ZT, true>, optin);
+      set_smem(k_xadj2<N1, N2>, optin);
     });
   }
   return cudaSuccess;
@@ -429,6 +505,18 @@ cudaError_t launch_zfwd2(Handle &h, const void *mid, void *dst, int nfield, doub
   } else {
     go.template operator()<double, double2>();
   }
+  return err;
+}
+
+cudaError_t launch_xadj2(Handle &h, const double2 *base_mid, double2 *lmid, double scale, cudaStream_t st) {
+  cudaError_t err = cudaErrorNotSupported;
+  if (h.mixed) return err;
+  with_shape(h.nx32, [&]<int N1, int N2>() {
+    const dim3 grid((unsigned)h.nz32, (unsigned)h.ny);
+    const size_t smem = sizeof(double2) * 6 * (size_t)ip_lda<N1, N2>();
+    k_xadj2<N1, N2><<<grid, 128, smem, st>>>(base_mid, lmid, h.px, h.nz32, h.nxh, 1.0f / (float)h.nxh, h.nm, scale);
+    err = cudaGetLastError();
+  });
   return err;
 }
 

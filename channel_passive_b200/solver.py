@@ -246,6 +246,24 @@ class Channel:
         if amp != 0.0:
             self.config.control_yd = yd
 
+    # -- discrete adjoint of the control objective -------------------------------------
+    def adjoint_forward(self, nsteps: int, w_tau: float = 1.0, w_q: float = 0.0) -> float:
+        """kmm_adjoint_forward: nsteps RK3 steps from the current state with one checkpoint per
+        step; returns J = (w_tau tau_w + w_q q_w) averaged over the steps."""
+        J = C.c_double()
+        check(self._lib.kmm_adjoint_forward(self._h, int(nsteps), float(w_tau), float(w_q), C.byref(J)))
+        return J.value
+
+    def adjoint_backward(self):
+        """kmm_adjoint_backward: (dJ/dA, dJ/dgains of shape (nz, nxh)) for the recorded steps."""
+        dA = C.c_double()
+        dg = np.zeros((self.config.nz, self.config.nxh))
+        check(self._lib.kmm_adjoint_backward(self._h, C.byref(dA), _dptr(dg)))
+        return dA.value, dg
+
+    def adjoint_release(self):
+        check(self._lib.kmm_adjoint_release(self._h))
+
     # -- time stepping ----------------------------------------------------------------
     def time_march(self, rk_substep: int) -> dict:
         s = KmmScalars()

@@ -299,6 +299,26 @@ int kmm_dev_solve_v_f(kmm_handle *h, double *v, double *dv, double *hv, double *
 int kmm_dev_solve_u_w(kmm_handle *h, double *g, double *f, const double *kx, const double *kz,
                       int nmodes, void *stream);
 
+/* ---- Discrete adjoint of the RK3 step: gradients of the opposition control ----
+ * No counterpart in the reference (its control is commented out).  The control of
+ * kmm_set_control sets v at the wall rows of the v solve to v_wall(m) = A g(m) P(w . v_m): A the
+ * amplitude, g the per-mode gains, w . v the value of v at the detection plane, P the projection
+ * the physical round trip applies (kz Nyquist row zeroed, Hermitian part on kx = 0).  Objective
+ * over N steps at a fixed time step:
+ *   J = (w_tau / N) sum_n tau_w(n) + (w_q / N) sum_n q_w(n),
+ * tau_w and q_w the wall shear stress and wall scalar flux of each step (kmm_scalars).
+ * kmm_adjoint_forward runs nsteps RK3 steps from the current state (as kmm_step does) keeping one
+ * checkpoint per step in HBM (u, v, w, theta and the three stores: 7 ny nxh nz complex doubles
+ * each) and returns J.  kmm_adjoint_backward applies the transpose of the recorded steps,
+ * recomputing each step's substeps from its checkpoint, and returns dJ/dA and dJ/dg
+ * (dJ_dgains: (nxh, nz) Fortran order like kmm_set_control_gains, may be NULL); the state is left
+ * where kmm_adjoint_forward left it.  kmm_adjoint_release frees the checkpoints and buffers
+ * (kmm_destroy does too).  The adjoint is FP64: a mixed-precision handle, or one with the CFL
+ * time step, gets KMM_ERR_CONFIG. */
+int kmm_adjoint_forward(kmm_handle *h, int nsteps, double w_tau, double w_q, double *J);
+int kmm_adjoint_backward(kmm_handle *h, double *dJ_dA, double *dJ_dgains);
+int kmm_adjoint_release(kmm_handle *h);
+
 /* Allocation-free batched Helmholtz solve.  No counterpart in the reference: it exists for
  * callers that may not allocate device memory (code running while a stream is captured into a
  * CUDA graph, hosts whose device memory is reserved up front by another allocator, loops that
