@@ -205,7 +205,7 @@ __device__ void helm_t(const AdjArgs &a, double visc, double k2, DLine lf, DLine
 
 // Per-mode transpose of wavespace (modes other than (0,0)).
 template <int BW>
-__global__ void __launch_bounds__(128) k_adj_modes(AdjArgs a) {
+__global__ void __launch_bounds__(64) k_adj_modes(AdjArgs a) {
   const int64_t m = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (m == 0 || m >= a.nmodes) return;
   const int n = a.ny, s = a.substep;
@@ -564,8 +564,9 @@ cudaError_t adj_substep_bw(Handle &h, int s, const double2 *sbase, double dt, do
   a.mb = A.mb;
   a.w_tau = w_tau;
   a.w_q = w_q;
+  // one thread per mode; 64-thread blocks spread the few thousand modes over more SMs
+  k_adj_modes<BW><<<(unsigned)((h.nmodes + 63) / 64), 64, 0, st>>>(a);
   const unsigned blocks = (unsigned)((h.nmodes + 127) / 128);
-  k_adj_modes<BW><<<blocks, 128, 0, st>>>(a);
   k_adj_mean<BW><<<1, 32, 0, st>>>(a);
   ProbeArgs pa{};
   pa.ny = h.ny;
