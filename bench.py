@@ -50,16 +50,19 @@ def workload_name(w):
 # ------------------------------------------------------------------------------------------
 # algorithmic bytes per kernel launch (each kernel's own required HBM traffic)
 # ------------------------------------------------------------------------------------------
-def kernel_bytes(w, s_nl, control=True):
+def kernel_bytes(w, s_nl, control=True, scalars=1):
+    """Each kernel's required HBM traffic per launch; a second scalar adds one state field, one
+    store and three products."""
     nxh = w["nx"] // 2
     nspec = nxh * w["nz"] * w["ny"]
     nmid = nxh * (w["nz"] * 3 // 2) * w["ny"]
     s_st = 16
+    nf, npd, nst = 3 + scalars, 5 + 3 * scalars, 2 + scalars
     return {
-        "zinv": 4 * nspec * s_st + 4 * nmid * s_nl,
-        "xphys": 4 * nmid * s_nl + 8 * nmid * s_nl,
-        "zfwd": 8 * nmid * s_nl + 8 * nspec * s_nl,
-        "wavespace": 8 * nspec * s_nl + (3 + (1 if control else 0)) * nspec * s_st + 7 * nspec * s_st,
+        "zinv": nf * nspec * s_st + nf * nmid * s_nl,
+        "xphys": nf * nmid * s_nl + npd * nmid * s_nl,
+        "zfwd": npd * nmid * s_nl + npd * nspec * s_nl,
+        "wavespace": npd * nspec * s_nl + (nst + (1 if control else 0)) * nspec * s_st + (nf + nst) * nspec * s_st,
     }
 
 
@@ -74,8 +77,8 @@ def group_wavespace(prof):
     return g
 
 
-def step_bytes(w, s_nl, control=True):
-    kb = kernel_bytes(w, s_nl, control)
+def step_bytes(w, s_nl, control=True, scalars=1):
+    kb = kernel_bytes(w, s_nl, control, scalars)
     return 3 * sum(kb.values())
 
 
@@ -429,9 +432,10 @@ def run_adjoint(args, device, local, rank):
 
 def run_production(args, device, local, rank, dist):
     """The Re_tau 590 production grid: 384x257x384, Lx 2 pi, Lz pi, tanh-mapped y, nu 1/10850,
-    CFL 0.8, opposition control A = -1 at y+ = 15 of Re_tau 590, one passive scalar (Pr 0.71).
-    Mixed-precision and FP64 RK3 steps/s through the CUDA graph, each timed by CUDA events on the
-    handle's stream, the step's HBM roofline fraction, and mixed vs FP64 after the timed steps."""
+    CFL 0.8, opposition control A = -1 at y+ = 15 of Re_tau 590, two passive scalars (Pr 0.71 and
+    Pr 0.2; the second in field 11, started from the first's profile).  Mixed-precision and FP64
+    RK3 steps/s through the CUDA graph, each timed by CUDA events on the handle's stream, the
+    step's HBM roofline fraction, and mixed vs FP64 after the timed steps."""
     import torch
 
     from channel_passive_b200 import Channel, Config, ic
@@ -439,14 +443,18 @@ def run_production(args, device, local, rank, dist):
 
     w = dict(nx=384, ny=257, nz=384)
     common = dict(lmfx=1.0, lmfz=0.5, stretch=2.0, grid=_lib.KMM_GRID_TANH, nu=1.0 / 10850.0, pr=0.71,
-                  cfl=0.8, fixed_dt=0, control_amp=-1.0, control_yd=-1.0 + 15.0 / 590.0, device=local, **w)
+                  cfl=0.8, fixed_dt=0, control_amp=-1.0, control_yd=-1.0 + 15.0 / 590.0, device=local,
+                  n_scalar=2, pr2=0.2, bulk_t2=1.0, **w)
     k = args.production_steps
     res, states = {}, {}
     U0 = None
     for name, prec in (("mixed", _lib.KMM_PREC_MIXED), ("fp64", _lib.KMM_PREC_FP64)):
         ch = Channel(Config(precision=prec, **common))
         if U0 is None:
-            U0 = ic.seeded_ic(w["nx"], w["ny"], w["nz"], ch.y, 1.0, 0.5, seed=SEED + rank)
+            U10 = ic.seeded_ic(w["nx"], w["ny"], w["nz"], ch.y, 1.0, 0.5, seed=SEED + rank)
+            U0 = np.zeros((11,) + U10.shape[1:], dtype=np.complex128)
+            U0[:10] = U10
+            U0[10] = U10[6]
         ch.set_initial_data_uvw(U0, 1e-3)
         ch.step(args.warmup)
         ch.set_initial_data_uvw(U0, 1e-3)
@@ -461,26 +469,29 @@ def run_production(args, device, local, rank, dist):
         out = ch.sync()
         torch.cuda.synchronize()
         ms = max_over_ranks(e0.elapsed_time(e1), dist, device)
-        states[name], _ = ch.download_state(7)
+        states[name], _ = ch.download_state(11)
         prof = ch.profile_step(2)
         ch.close()
         s_nl = 8 if name == "mixed" else 16
         peak, _kind = measured_peaks()
+        sb = step_bytes(w, s_nl, scalars=2)
         res[name] = {"steps_per_s": k / (ms * 1e-3), "ms_per_step": ms / k, "last_dt": out["dt"],
-                     "step_algorithmic_bytes": step_bytes(w, s_nl),
-                     "step_frac": step_bytes(w, s_nl) / (ms / k * 1e-3) / 1e9 / peak,
+                     "step_algorithmic_bytes": sb,
+                     "step_frac": sb / (ms / k * 1e-3) / 1e9 / peak,
+                     "q_w": [out["wall_theta_stress"], out["wall_theta_stress2"]],
                      "kernels_ms": {kn: v["ms"] for kn, v in prof.items()}}
-    names = {0: "u", 1: "v", 2: "w", 6: "theta"}
+    names = {0: "u", 1: "v", 2: "w", 6: "theta", 10: "theta2"}
     Um, Ud = states["mixed"], states["fp64"]
     rel = {names[f]: float(np.linalg.norm(Um[f] - Ud[f]) / np.linalg.norm(Ud[f])) for f in names}
     return {"workload": "384x257x384 Re_tau 590 (Lx 2 pi, Lz pi, tanh y map), nu 1/10850, CFL 0.8, "
-                        "opposition control A=-1 at y+=15, one passive scalar Pr 0.71",
+                        "opposition control A=-1 at y+=15, two passive scalars Pr 0.71 and Pr 0.2",
             "steps": k, "warmup": args.warmup, "mixed": res["mixed"], "fp64": res["fp64"],
             "mixed_over_fp64": res["mixed"]["steps_per_s"] / res["fp64"]["steps_per_s"],
             "grid_point_steps_per_s": res["mixed"]["steps_per_s"] * w["nx"] * w["ny"] * w["nz"],
             "rel_l2_mixed_vs_fp64": rel,
             "roofline_peak": "of measured HBM copy bandwidth",
-            "second_scalar": "not run: the reference carries one passive scalar"}
+            "scalars": "Pr 0.71 and Pr 0.2 (the reference carries one; the second is checked against the "
+                       "build's own FP64 oracle)"}
 
 
 def run_kmm(args):

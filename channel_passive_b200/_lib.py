@@ -42,7 +42,8 @@ class KmmConfig(C.Structure):
         ("u_gal", C.c_double), ("cfl", C.c_double), ("dt_factor", C.c_double),
         ("dy_factor", C.c_double), ("fixed_dt", C.c_int32), ("precision", C.c_int32),
         ("control_amp", C.c_double), ("control_yd", C.c_double), ("device", C.c_int32),
-        ("reserved", C.c_int32 * 7),
+        ("n_scalar", C.c_int32), ("pr2", C.c_double), ("bulk_t2", C.c_double),
+        ("reserved", C.c_int32 * 2),
     ]
 
 
@@ -51,12 +52,14 @@ class KmmScalars(C.Structure):
         ("dt", C.c_double), ("velmax", C.c_double),
         ("phi_dpdx", C.c_double * 4), ("phi_dtdx", C.c_double * 4),
         ("wall_shear_stress", C.c_double), ("wall_theta_stress", C.c_double),
+        ("phi_dtdx2", C.c_double * 4), ("wall_theta_stress2", C.c_double),
     ]
 
     def as_dict(self):
         return {"dt": self.dt, "velmax": self.velmax, "phi_dpdx": list(self.phi_dpdx),
                 "phi_dtdx": list(self.phi_dtdx), "wall_shear_stress": self.wall_shear_stress,
-                "wall_theta_stress": self.wall_theta_stress}
+                "wall_theta_stress": self.wall_theta_stress, "phi_dtdx2": list(self.phi_dtdx2),
+                "wall_theta_stress2": self.wall_theta_stress2}
 
 
 class KmmInfo(C.Structure):

@@ -617,6 +617,10 @@ int adjoint_checks(Handle &h, const char *name) {
     set_error(std::string(name) + ": the adjoint needs a fixed time step (fixed_dt = 1)");
     return KMM_ERR_CONFIG;
   }
+  if (h.nsc != 1) {
+    set_error(std::string(name) + ": the adjoint covers one passive scalar");
+    return KMM_ERR_CONFIG;
+  }
   return KMM_OK;
 }
 

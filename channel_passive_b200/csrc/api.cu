@@ -101,6 +101,8 @@ int validate(const kmm_config &c) {
   if (c.grid != KMM_GRID_SINE && c.grid != KMM_GRID_TANH) return bad("unknown grid map");
   if (c.control_amp != 0.0 && !(c.control_yd > -1.0 && c.control_yd < 0.0))
     return bad("control detection plane y_d must lie in (-1, 0)");
+  if (c.n_scalar < 0 || c.n_scalar > 2) return bad("n_scalar must be 1 or 2");
+  if (c.n_scalar == 2 && !(c.pr2 > 0.0)) return bad("pr2 (the second scalar's Prandtl number) must be positive");
   std::vector<int> rs;
   if (!factor_radices(c.nx * 3 / 2, rs) || !factor_radices(c.nz * 3 / 2, rs))
     return bad("3/2-padded lengths must factor into 2, 3, 5 with at most 8 passes");
@@ -203,11 +205,12 @@ int enqueue_substep(Handle &h, int s, cudaStream_t st, cudaEvent_t *ev = nullptr
   };
   int rc;
   if ((rc = rec(KMM_K_BEGIN, [&] { return launch_begin_substep(h, s, st); }))) return rc;
-  if ((rc = rec(KMM_K_ZINV, [&] { return launch_zinv(h, h.S, h.MID, 4, st); }))) return rc;
+  if ((rc = rec(KMM_K_ZINV, [&] { return launch_zinv(h, h.S, h.MID, 3 + h.nsc, st); }))) return rc;
   if ((rc = rec(KMM_K_XPHYS, [&] { return launch_xphys(h, h.MID, s, st); }))) return rc;
   if (s == 1)
     if ((rc = rec(KMM_K_DT, [&] { return launch_update_dt(h, s, st); }))) return rc;
-  if ((rc = rec(KMM_K_ZFWD, [&] { return launch_zfwd(h, h.MID, h.P, 8, h.rescale, !h.mixed, st); }))) return rc;
+  if ((rc = rec(KMM_K_ZFWD, [&] { return launch_zfwd(h, h.MID, h.P, 5 + 3 * h.nsc, h.rescale, !h.mixed, st); })))
+    return rc;
   if ((rc = rec(KMM_K_HVHG, [&] { return launch_ws_hvhg(h, s, nullptr, st); }))) return rc;
   if ((rc = rec(KMM_K_HELMHOLTZ, [&] { return launch_ws_helmholtz(h, s, nullptr, st); }))) return rc;
   if ((rc = rec(KMM_K_ASSEMBLE, [&] { return launch_ws_assemble(h, s, nullptr, st); }))) return rc;
@@ -229,6 +232,8 @@ int read_scalars(Handle &h, kmm_scalars *out, int *dev_err) {
     }
     out->wall_shear_stress = d.wall_shear_stress;
     out->wall_theta_stress = d.wall_theta_stress;
+    for (int i = 0; i < 4; ++i) out->phi_dtdx2[i] = d.phi_dtdx2[i];
+    out->wall_theta_stress2 = d.wall_theta_stress2;
   }
   return KMM_OK;
 }
@@ -244,15 +249,18 @@ int check_device_error(Handle &h, int err) {
   return err;
 }
 
+// U slots of the state fields S 0..4: u, v, w, theta (fields 1, 2, 3, 7) and theta2 (field 11).
+constexpr int kStateSlots[5] = {0, 1, 2, 6, 10};
+
 int upload_fields(Handle &h, const double *U, int nf, const double *rk, cudaStream_t st) {
   const size_t fb = sizeof(double2) * (size_t)h.ns;
-  const int slots[4] = {0, 1, 2, 6};
-  for (int i = 0; i < 4; ++i)
-    KMM_CUDA(cudaMemcpyAsync(h.staging + i * h.ns, U + 2 * (size_t)slots[i] * h.ns, fb, cudaMemcpyHostToDevice, st));
-  KMM_CUDA(launch_ref_to_planes(h.staging, h.S, 4, h.nmodes, h.ny, st));
+  const int nfld = 3 + h.nsc, nst = 2 + h.nsc;
+  for (int i = 0; i < nfld; ++i)
+    KMM_CUDA(cudaMemcpyAsync(h.staging + i * h.ns, U + 2 * (size_t)kStateSlots[i] * h.ns, fb, cudaMemcpyHostToDevice, st));
+  KMM_CUDA(launch_ref_to_planes(h.staging, h.S, nfld, h.nmodes, h.ny, st));
   if (rk) {
-    KMM_CUDA(cudaMemcpyAsync(h.staging + 4 * h.ns, rk, 3 * fb, cudaMemcpyHostToDevice, st));
-    KMM_CUDA(launch_ref_to_planes(h.staging + 4 * h.ns, h.RK, 3, h.nmodes, h.ny, st));
+    KMM_CUDA(cudaMemcpyAsync(h.staging + nfld * h.ns, rk, nst * fb, cudaMemcpyHostToDevice, st));
+    KMM_CUDA(launch_ref_to_planes(h.staging + nfld * h.ns, h.RK, nst, h.nmodes, h.ny, st));
   }
   (void)nf;
   return KMM_OK;
@@ -260,16 +268,19 @@ int upload_fields(Handle &h, const double *U, int nf, const double *rk, cudaStre
 
 int download_fields(Handle &h, double *U, int nf, double *rk, cudaStream_t st) {
   const size_t fb = sizeof(double2) * (size_t)h.ns;
-  const int slots[4] = {0, 1, 2, 6};
-  KMM_CUDA(launch_planes_to_ref(h.S, h.staging, 4, h.nmodes, h.ny, st));
-  if (rk) KMM_CUDA(launch_planes_to_ref(h.RK, h.staging + 4 * h.ns, 3, h.nmodes, h.ny, st));
+  const int nfld = 3 + h.nsc, nst = 2 + h.nsc;
+  KMM_CUDA(launch_planes_to_ref(h.S, h.staging, nfld, h.nmodes, h.ny, st));
+  if (rk) KMM_CUDA(launch_planes_to_ref(h.RK, h.staging + nfld * h.ns, nst, h.nmodes, h.ny, st));
   if (U)
-    for (int i = 0; i < 4; ++i)
-      KMM_CUDA(cudaMemcpyAsync(U + 2 * (size_t)slots[i] * h.ns, h.staging + i * h.ns, fb, cudaMemcpyDeviceToHost, st));
-  if (rk) KMM_CUDA(cudaMemcpyAsync(rk, h.staging + 4 * h.ns, 3 * fb, cudaMemcpyDeviceToHost, st));
+    for (int i = 0; i < nfld; ++i)
+      KMM_CUDA(cudaMemcpyAsync(U + 2 * (size_t)kStateSlots[i] * h.ns, h.staging + i * h.ns, fb, cudaMemcpyDeviceToHost, st));
+  if (rk) KMM_CUDA(cudaMemcpyAsync(rk, h.staging + nfld * h.ns, nst * fb, cudaMemcpyDeviceToHost, st));
   (void)nf;
   return KMM_OK;
 }
+
+// Fields a caller's U must hold: 7 (theta is field 7), 11 with a second scalar (field 11).
+int min_fields(const Handle &h) { return h.nsc == 2 ? 11 : 7; }
 
 int set_dt_device(Handle &h, double dt) {
   DevScalars d;
@@ -304,6 +315,7 @@ void finish_step_scalars(kmm_scalars *out) {
   if (!out) return;
   out->phi_dpdx[3] = (out->phi_dpdx[0] + out->phi_dpdx[1] + out->phi_dpdx[2]) / out->dt;  // main.f90:147
   out->phi_dtdx[3] = (out->phi_dtdx[0] + out->phi_dtdx[1] + out->phi_dtdx[2]) / out->dt;  // main.f90:148
+  out->phi_dtdx2[3] = (out->phi_dtdx2[0] + out->phi_dtdx2[1] + out->phi_dtdx2[2]) / out->dt;
 }
 
 }  // namespace
@@ -350,6 +362,9 @@ int kmm_config_default(kmm_config *c) {
   c->control_amp = 0.0;
   c->control_yd = -1.0 + 15.0 / 180.0;
   c->device = 0;
+  c->n_scalar = 1;
+  c->pr2 = 0.2;
+  c->bulk_t2 = 1.0;
   return KMM_OK;
 }
 
@@ -423,6 +438,7 @@ int kmm_create(const kmm_config *cfg, kmm_handle **out) {
   h->ns = (int64_t)h->ny * h->nmodes;
   h->nm = (int64_t)h->ny * h->nz32 * h->nxh;
   h->mixed = cfg->precision == KMM_PREC_MIXED;
+  h->nsc = cfg->n_scalar == 2 ? 2 : 1;
   // read_input_file.f90:94-116
   const double lx = cfg->lmfx * 2 * kPiF, lz = cfg->lmfz * 2 * kPiF;
   h->dxr = (double)cfg->nx / lx;
@@ -440,6 +456,11 @@ int kmm_create(const kmm_config *cfg, kmm_handle **out) {
     return rc;
   }
   h->bw = h->ops.bw;
+  if (h->nsc == 2 && !fft4_supported(h->nx32)) {
+    set_error("a second scalar needs nx*3/2 among the four-step lengths (12 ... 576)");
+    delete h;
+    return KMM_ERR_CONFIG;
+  }
   if (h->bw < kMinBw || h->bw > kMaxBw) {
     set_error("detected band width " + std::to_string(h->bw) + " outside the compiled range 2..7");
     delete h;
@@ -483,24 +504,25 @@ int kmm_create(const kmm_config *cfg, kmm_handle **out) {
     }
   const size_t r2 = h->mixed ? sizeof(float2) : sizeof(double2);
   OpsOffsets off = ops_offsets(h->bw, h->ny);
-  if ((rc = dalloc(*h, &h->S, 4 * h->ns))) return fail(rc);
-  if ((rc = dalloc(*h, &h->RK, 3 * h->ns))) return fail(rc);
-  if ((rc = dalloc(*h, reinterpret_cast<char **>(&h->P), 8 * h->ns * r2))) return fail(rc);
-  if ((rc = dalloc(*h, reinterpret_cast<char **>(&h->MID), 8 * h->nm * r2))) return fail(rc);
+  const int nfld = 3 + h->nsc, nst = 2 + h->nsc, nprod = 5 + 3 * h->nsc, x2 = h->nsc - 1;
+  if ((rc = dalloc(*h, &h->S, nfld * h->ns))) return fail(rc);
+  if ((rc = dalloc(*h, &h->RK, nst * h->ns))) return fail(rc);
+  if ((rc = dalloc(*h, reinterpret_cast<char **>(&h->P), nprod * h->ns * r2))) return fail(rc);
+  if ((rc = dalloc(*h, reinterpret_cast<char **>(&h->MID), nprod * h->nm * r2))) return fail(rc);
   if ((rc = dalloc(*h, &h->dops, (size_t)off.total))) return fail(rc);
   if ((rc = dalloc(*h, &h->gains, (size_t)h->nmodes))) return fail(rc);
   if ((rc = dalloc(*h, &h->vwall, 2 * (size_t)h->nmodes))) return fail(rc);
-  if ((rc = dalloc(*h, &h->zc, 8 * (size_t)h->ns))) return fail(rc);
-  if ((rc = dalloc(*h, &h->ec, 9 * (size_t)h->ns))) return fail(rc);
+  if ((rc = dalloc(*h, &h->zc, (8 + 2 * x2) * (size_t)h->ns))) return fail(rc);
+  if ((rc = dalloc(*h, &h->ec, (9 + 2 * x2) * (size_t)h->ns))) return fail(rc);
   if ((rc = dalloc(*h, &h->xr, 6 * (size_t)h->ns))) return fail(rc);
-  if ((rc = dalloc(*h, &h->ub, 3 * (size_t)split_ub_role(*h)))) return fail(rc);
+  if ((rc = dalloc(*h, &h->ub, (3 + x2) * (size_t)split_ub_role(*h)))) return fail(rc);
   if ((rc = dalloc(*h, &h->vf, (size_t)vop_factor_doubles(*h)))) return fail(rc);
   if ((rc = dalloc(*h, &h->dvw, 3 * (size_t)h->nmodes))) return fail(rc);
-  if ((rc = dalloc(*h, &h->w00, 3 * (size_t)h->ny * (8 + 2 * h->bw)))) return fail(rc);
+  if ((rc = dalloc(*h, &h->w00, (3 + x2) * (size_t)h->ny * (8 + 2 * h->bw)))) return fail(rc);
   if ((rc = dalloc(*h, &h->staging, 10 * h->ns))) return fail(rc);
   if ((rc = dalloc(*h, &h->dsc, 1))) return fail(rc);
-  if (cudaMemset(h->S, 0, sizeof(double2) * 4 * h->ns) != cudaSuccess ||
-      cudaMemset(h->RK, 0, sizeof(double2) * 3 * h->ns) != cudaSuccess ||
+  if (cudaMemset(h->S, 0, sizeof(double2) * nfld * h->ns) != cudaSuccess ||
+      cudaMemset(h->RK, 0, sizeof(double2) * nst * h->ns) != cudaSuccess ||
       cudaMemset(h->dsc, 0, sizeof(DevScalars)) != cudaSuccess) {
     set_error("cudaMemset failed");
     return fail(KMM_ERR_CUDA);
@@ -600,6 +622,10 @@ int kmm_upload_state(kmm_handle *hh, const double *U, int nf, const double *rk, 
     return KMM_ERR_ARG;
   }
   Handle &h = *reinterpret_cast<Handle *>(hh);
+  if (nf < min_fields(h)) {
+    set_error("kmm_upload_state: a second scalar needs nf >= 11 (it is field 11)");
+    return KMM_ERR_ARG;
+  }
   DeviceGuard dg(h.cfg.device);
   int rc = upload_fields(h, U, nf, rk, h.stream);
   if (rc) return rc;
@@ -613,6 +639,10 @@ int kmm_download_state(kmm_handle *hh, double *U, int nf, double *rk) {
     return KMM_ERR_ARG;
   }
   Handle &h = *reinterpret_cast<Handle *>(hh);
+  if (U && nf < min_fields(h)) {
+    set_error("kmm_download_state: a second scalar needs nf >= 11 (it is field 11)");
+    return KMM_ERR_ARG;
+  }
   DeviceGuard dg(h.cfg.device);
   int rc = download_fields(h, U, nf, rk, h.stream);
   if (rc) return rc;
@@ -626,6 +656,10 @@ int kmm_set_initial_data_uvw(kmm_handle *hh, const double *U, int nf, double dt)
     return KMM_ERR_ARG;
   }
   Handle &h = *reinterpret_cast<Handle *>(hh);
+  if (nf < min_fields(h)) {
+    set_error("kmm_set_initial_data_uvw: a second scalar needs nf >= 11 (it is field 11)");
+    return KMM_ERR_ARG;
+  }
   DeviceGuard dg(h.cfg.device);
   int rc = upload_fields(h, U, nf, nullptr, h.stream);
   if (rc) return rc;
@@ -756,7 +790,11 @@ int kmm_step_host(kmm_handle *hh, double *U, int nf, double *rk, int nsteps, kmm
   }
   Handle &h = *reinterpret_cast<Handle *>(hh);
   DeviceGuard dg(h.cfg.device);
-  if (!rk) return step_host_pipelined(h, U, nsteps, out);
+  if (nf < min_fields(h)) {
+    set_error("kmm_step_host: a second scalar needs nf >= 11 (it is field 11)");
+    return KMM_ERR_ARG;
+  }
+  if (!rk && h.nsc == 1) return step_host_pipelined(h, U, nsteps, out);
   int rc = upload_fields(h, U, nf, rk, h.stream);
   if (rc) return rc;
   // Without rk the stores are rebuilt from U, as the reference's restart option 1 does
@@ -984,6 +1022,10 @@ int kmm_dev_x_to_y(kmm_handle *hh, const void *xp, double *u, int rescale, void 
 int kmm_dev_dft_x_realspace(kmm_handle *hh, void *xp, int s, double *velmax_dev, void *stream) {
   if (!hh || !xp || s < 1 || s > 3) return KMM_ERR_ARG;
   Handle &h = *reinterpret_cast<Handle *>(hh);
+  if (h.nsc != 1) {
+    set_error("kmm_dev_dft_x_realspace: the reference's 10-slot X-pencil carries one scalar");
+    return KMM_ERR_CONFIG;
+  }
   DeviceGuard dg(h.cfg.device);
   cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
   const size_t r2 = h.mixed ? sizeof(float2) : sizeof(double2);
@@ -1007,6 +1049,10 @@ int kmm_dev_wavespace(kmm_handle *hh, double *U, double *rk, int s, double dt, k
                       void *stream) {
   if (!hh || !U || !rk || s < 1 || s > 3) return KMM_ERR_ARG;
   Handle &h = *reinterpret_cast<Handle *>(hh);
+  if (h.nsc != 1) {
+    set_error("kmm_dev_wavespace: the reference's 10-slot U carries one scalar");
+    return KMM_ERR_CONFIG;
+  }
   DeviceGuard dg(h.cfg.device);
   cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
   const double2 *Uc = reinterpret_cast<const double2 *>(U);

@@ -5,6 +5,8 @@
 //   RK  [3][ny][nz][nxh]    double2   low-storage RK terms           (RK_STORE 1..3)
 //   P   [8][ny][nz][nxh]    R2        spectral products f1..f5, f7..f9 (fields 1-5, 7-9)
 //   MID [8][ny][nz32][nxh]  R2        x-spectral / z-physical slab = the reference X-pencil
+// With a second passive scalar theta2 (Handle::nsc = 2): S field 4 = theta2, RK store 3 = its
+// RK term, P and MID fields 8..10 = u theta2, v theta2, w theta2 (MID field 4 = theta2 in).
 //                                     Up(nxh, nz32, ny) (dft_x_realspace.f90:31)
 // A (kx, kz) mode m = kz_index * nxh + kx owns the strided line S[f][.][m]: a warp of 32
 // consecutive modes reads one 32-element contiguous run per y, so the per-mode solver is
@@ -49,6 +51,8 @@ struct DevScalars {
   double phi_dtdx[4];
   double wall_shear_stress;
   double wall_theta_stress;
+  double phi_dtdx2[4];          // the second passive scalar's forcing (n_scalar = 2)
+  double wall_theta_stress2;
   int err;                      // KMM_ERR_* raised on the device, 0 if none
   int nonfinite;                // set when a non-finite velocity was seen
 };
@@ -82,6 +86,8 @@ struct Handle {
   int64_t ns = 0;               // ny * nmodes            (spectral plane stack per field)
   int64_t nm = 0;               // ny * nz32 * nxh        (mid slab per field)
   bool mixed = false;
+  int nsc = 1;                  // passive scalars (1 or 2): S holds 3 + nsc fields, RK 2 + nsc stores,
+                                // P and MID 8 + 3 (nsc - 1) product fields
   double dxr = 0, dzr = 0, cflx = 0, rescale = 0, lmfxr = 0, lmfzr = 0;
   HostOps ops;
   std::vector<int> radix_x, radix_z;
@@ -172,6 +178,8 @@ struct DeviceGuard {
 void prepare_kernels(Handle &h);
 void convert_planes_d2f(const double2 *src, float2 *dst, int64_t n, cudaStream_t st);
 cudaError_t prepare_transforms2();
+// Whether a padded line length has a compile-time four-step shape (transforms2.cu).
+bool fft4_supported(int N);
 // Four-step transforms (transforms2.cu); return cudaErrorNotSupported for other lengths.
 cudaError_t launch_zinv2(Handle &h, const double2 *src_planes, void *mid, int nfield, cudaStream_t st);
 // stat: the statistics-step variant (f6 = v v, no CFL); mom (stat only, may be null) receives

@@ -13,7 +13,7 @@ namespace kmm {
 namespace {
 
 struct InitArgs {
-  int ny, nxh, nz;
+  int ny, nxh, nz, nsc;
   int64_t nmodes, ns;
   double2 *S, *RK, *scratch;
   const double *tabs;  // offset tables T0, T1, T2, L0, U0
@@ -45,6 +45,10 @@ __global__ void __launch_bounds__(128) k_init_stores(InitArgs a) {
       R2.st(i, Sw.ld(i));
       R3.st(i, St.ld(i));
     }
+    if (a.nsc == 2) {  // the second scalar's store is the scalar, as RK_STORE 3 is theta
+      const DLine S4 = dline(a.S, 4 * a.ns, m, nm), R4 = dline(a.RK, 3 * a.ns, m, nm);
+      for (int i = 1; i <= n; ++i) R4.st(i, S4.ld(i));
+    }
     return;
   }
   const int kzi = (int)(m / a.nxh), kxi = (int)(m - (int64_t)kzi * a.nxh);
@@ -63,6 +67,7 @@ __global__ void __launch_bounds__(128) k_init_stores(InitArgs a) {
         if constexpr (!PHI_ONLY) {
           R1.st(q, zsub(zmul(z2(0.0, kz), Su.ld(q)), zmul(z2(0.0, kx), Sw.ld(q))));
           R3.st(q, St.ld(q));
+          if (a.nsc == 2) a.RK[3 * a.ns + (q - 1) * nm + m] = a.S[4 * a.ns + (q - 1) * nm + m];
         }
       },
       [&](int r) {
@@ -97,6 +102,7 @@ __global__ void __launch_bounds__(256) k_init_elem(InitArgs a) {
     a.RK[o] = zsub(zmul(z2(0.0, kz), u), zmul(z2(0.0, kx), w));
   }
   a.RK[2 * ns + o] = a.S[3 * ns + o];
+  if (a.nsc == 2) a.RK[3 * ns + o] = a.S[4 * ns + o];
 }
 
 // Batched LABS kernels for the unit tests (row 18).
@@ -123,6 +129,7 @@ InitArgs make_init_args(Handle &h) {
   a.ny = h.ny;
   a.nxh = h.nxh;
   a.nz = h.nz;
+  a.nsc = h.nsc;
   a.nmodes = h.nmodes;
   a.ns = h.ns;
   a.S = h.S;

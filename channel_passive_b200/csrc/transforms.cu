@@ -355,7 +355,7 @@ static cudaError_t xphys_impl(Handle &h, void *mid, int substep, cudaStream_t st
 
 cudaError_t launch_xphys(Handle &h, void *mid, int substep, cudaStream_t st) {
   const cudaError_t e = launch_xphys2(h, mid, substep, st);
-  if (e != cudaErrorNotSupported) return e;
+  if (e != cudaErrorNotSupported || h.nsc != 1) return e;  // a second scalar needs a four-step length
   return h.mixed ? xphys_impl<float>(h, mid, substep, st) : xphys_impl<double>(h, mid, substep, st);
 }
 

@@ -182,28 +182,33 @@ template <typename R, int N, bool STAT> constexpr int x_min_blocks() {
   return N >= 576 ? KMM_X576_MINB : N == 288 ? KMM_X288_MINB : 1;
 }
 
-template <typename R, int N1, int N2, int ZB, int NT, bool STAT = false>
+// NS = 2: a second passive scalar theta2 in MID slot 4; its products u theta2, v theta2, w theta2
+// go to slots 8, 9, 10, formed like f7..f9 (a third packed input line (theta2, 0) and two packed
+// output lines (u theta2, v theta2), (w theta2, 0)).
+template <typename R, int N1, int N2, int ZB, int NT, bool STAT = false, int NS = 1>
 __global__ void __launch_bounds__(NT, (x_min_blocks<R, N1 * N2, STAT>())) k_xphys2(typename Cpx<R>::T *__restrict__ mid, FftPlan pl, X2Args a_) {
   using C = typename Cpx<R>::T;
   constexpr int N = N1 * N2, LD = ip_lda<N1, N2>();
+  constexpr int NIN = 1 + NS, NOUT = 2 + 2 * NS;  // packed input and output lines per row
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  C *a = reinterpret_cast<C *>(smem_raw);  // 4*ZB lines: (u,v) ZB, (w,theta) ZB, then f57, f89
+  C *a = reinterpret_cast<C *>(smem_raw);  // NOUT*ZB lines: (u,v) ZB, (w,theta) ZB, [(theta2,0) ZB,] then outputs
   const int nxh = a_.nxh;
   const int z0 = blockIdx.x * ZB, y = blockIdx.y;
   const int64_t row0 = ((int64_t)y * a_.nz32 + z0) * nxh;
-  for (int w = threadIdx.x; w < 2 * ZB * N; w += NT) {
+  for (int w = threadIdx.x; w < NIN * ZB * N; w += NT) {
     const int L = w / N, p = w - L * N;
     a[L * LD + p] = cmake<C>(0.0, 0.0);
   }
   __syncthreads();
   // Z_k = X1_k + i X2_k and its Hermitian mirror at N - k; DC imaginary parts dropped (c2r)
-  for (int w = threadIdx.x; w < 2 * ZB * nxh; w += NT) {
+  for (int w = threadIdx.x; w < NIN * ZB * nxh; w += NT) {
     // exact: (w + 0.5) / nxh stays at least 0.5 / nxh away from an integer, far above float rounding
     const int t = (int)(((float)w + 0.5f) * a_.rnxh), k = w - t * nxh, l = t % ZB, bsel = t / ZB;
     if (z0 + l >= a_.nz32) continue;
     const int64_t off = row0 + (int64_t)l * nxh + k;
-    const int fa = bsel ? 2 : 0, fb = bsel ? 3 : 1;
-    const C x1 = mid[fa * a_.nm + off], x2 = mid[fb * a_.nm + off];
+    const int fa = bsel == 0 ? 0 : bsel == 1 ? 2 : 4, fb = bsel == 0 ? 1 : 3;
+    const C x1 = mid[fa * a_.nm + off];
+    const C x2 = bsel < 2 ? mid[fb * a_.nm + off] : cmake<C>(0.0, 0.0);
     C *line = a + (bsel * ZB + l) * LD;
     if (k == 0) {
       line[0] = cmake<C>(x1.x, x2.x);
@@ -216,7 +221,7 @@ __global__ void __launch_bounds__(NT, (x_min_blocks<R, N1 * N2, STAT>())) k_xphy
     }
   }
   __syncthreads();
-  fft4_ip<R, N1, N2, 2 * ZB, NT>(a, LD, tw_of<R>(pl), +1);
+  fft4_ip<R, N1, N2, NIN * ZB, NT>(a, LD, tw_of<R>(pl), +1);
   const double dyr = a_.dyr[y];
   double vmax = 0.0;
   int bad = 0;
@@ -225,6 +230,8 @@ __global__ void __launch_bounds__(NT, (x_min_blocks<R, N1 * N2, STAT>())) k_xphy
     const int l = w / N, p = w - l * N;
     const C uv = a[l * LD + p], wt = a[(ZB + l) * LD + p];
     const R u = uv.x, v = uv.y, ww = wt.x, t = wt.y;
+    R t2 = 0;
+    if constexpr (NS == 2) t2 = a[(2 * ZB + l) * LD + p].x;
     if constexpr (STAT) {
       if (a_.mom && z0 + l < a_.nz32) moment_terms(ms, (double)u, (double)v, (double)ww);
     }
@@ -243,6 +250,13 @@ __global__ void __launch_bounds__(NT, (x_min_blocks<R, N1 * N2, STAT>())) k_xphy
     a[(ZB + l) * LD + p] = f34;
     a[(2 * ZB + l) * LD + p] = f57;
     a[(3 * ZB + l) * LD + p] = f89;
+    if constexpr (NS == 2) {
+      C g12, g3;
+      g12.x = u * t2; g12.y = v * t2;
+      g3.x = ww * t2; g3.y = 0;
+      a[(4 * ZB + l) * LD + p] = g12;
+      a[(5 * ZB + l) * LD + p] = g3;
+    }
     if (!STAT && a_.substep == 1 && z0 + l < a_.nz32) {
       const double vel = (fabs((double)u) * a_.dxr) + (fabs((double)v) * dyr) + (fabs((double)ww) * a_.dzr);
       if (!isfinite(vel)) bad = 1;
@@ -250,8 +264,8 @@ __global__ void __launch_bounds__(NT, (x_min_blocks<R, N1 * N2, STAT>())) k_xphy
     }
   }
   __syncthreads();
-  fft4_ip<R, N1, N2, 4 * ZB, NT>(a, LD, tw_of<R>(pl), -1);
-  for (int w = threadIdx.x; w < (STAT ? 3 : 4) * ZB * nxh; w += NT) {
+  fft4_ip<R, N1, N2, NOUT * ZB, NT>(a, LD, tw_of<R>(pl), -1);
+  for (int w = threadIdx.x; w < (STAT ? 3 : NOUT) * ZB * nxh; w += NT) {
     // exact: (w + 0.5) / nxh stays at least 0.5 / nxh away from an integer, far above float rounding
     const int t = (int)(((float)w + 0.5f) * a_.rnxh), k = w - t * nxh, l = t % ZB, bsel = t / ZB;
     if (z0 + l >= a_.nz32) continue;
@@ -262,7 +276,7 @@ __global__ void __launch_bounds__(NT, (x_min_blocks<R, N1 * N2, STAT>())) k_xphy
     B.x = (R)0.5 * (zk.y + zm.y); B.y = (R)0.5 * (zm.x - zk.x);
     const int64_t off = row0 + (int64_t)l * nxh + k;
     mid[(2 * bsel) * a_.nm + off] = A;
-    mid[(2 * bsel + 1) * a_.nm + off] = B;
+    if (2 * bsel + 1 < 11) mid[(2 * bsel + 1) * a_.nm + off] = B;  // slot 11 would be the zero partner
   }
   if constexpr (STAT) {
     if (a_.mom) {
@@ -414,9 +428,9 @@ template <typename R, int N1, int N2>
 constexpr size_t z_smem() {
   return sizeof(typename Cpx<R>::T) * (size_t)TCfg<R>::KB * ip_lda<N1, N2>();
 }
-template <typename R, int N1, int N2>
+template <typename R, int N1, int N2, int NS = 1>
 constexpr size_t x_smem() {
-  return sizeof(typename Cpx<R>::T) * (size_t)4 * TCfg<R>::ZB * ip_lda<N1, N2>();
+  return sizeof(typename Cpx<R>::T) * (size_t)(2 + 2 * NS) * TCfg<R>::ZB * ip_lda<N1, N2>();
 }
 
 }  // namespace
@@ -462,6 +476,8 @@ cudaError_t prepare_transforms2() {
       set_smem(k_xphys2<float, N1, N2, F::ZB, F::ZT>, optin);
       set_smem(k_xphys2<double, N1, N2, D::ZB, D::ZT, true>, optin);
       set_smem(k_xphys2<float, N1, N2, F::ZB, F::ZT, true>, optin);
+      set_smem(k_xphys2<double, N1, N2, D::ZB, D::ZT, false, 2>, optin);
+      set_smem(k_xphys2<float, N1, N2, F::ZB, F::ZT, false, 2>, optin);
       set_smem(k_xadj2<N1, N2>, optin);
     });
   }
@@ -546,6 +562,9 @@ cudaError_t launch_xphys2(Handle &h, void *mid, int substep, cudaStream_t st, bo
       dim3 grid((unsigned)((h.nz32 + T::ZB - 1) / T::ZB), (unsigned)h.ny);
       if (stat)
         k_xphys2<R, N1, N2, T::ZB, T::ZT, true><<<grid, T::ZT, x_smem<R, N1, N2>(), st>>>(reinterpret_cast<C *>(mid), h.px, a);
+      else if (h.nsc == 2)
+        k_xphys2<R, N1, N2, T::ZB, T::ZT, false, 2><<<grid, T::ZT, x_smem<R, N1, N2, 2>(), st>>>(
+            reinterpret_cast<C *>(mid), h.px, a);
       else
         k_xphys2<R, N1, N2, T::ZB, T::ZT><<<grid, T::ZT, x_smem<R, N1, N2>(), st>>>(reinterpret_cast<C *>(mid), h.px, a);
       err = cudaGetLastError();

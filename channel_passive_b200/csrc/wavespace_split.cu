@@ -42,7 +42,9 @@ constexpr int kRoles = 4;
 // of the products and are stored at the products' precision PT (float2 in the mixed path, packed
 // at (PT *)hl + i * ns); the substep-1 lines H_DP, H_DT, H_DG (D2 D0^{-1} of the FP64 RK stores)
 // stay double2 at hl + i * ns.
-enum HLine { H_HV0 = 0, H_HT, H_G2, H_V2, H_G3, H_V3, H_DP, H_DT, H_DG, H_COUNT };
+// A second passive scalar adds H_HT2 (its nonlinear term, at PT like H_HT) and H_DT2 (substep 1,
+// double2 like H_DT).
+enum HLine { H_HV0 = 0, H_HT, H_G2, H_V2, H_G3, H_V3, H_DP, H_DT, H_DG, H_HT2, H_DT2, H_COUNT };
 
 // Low-storage RK3 coefficients alpha, beta, gamma, zeta of substeps 1-3
 // (RK3_initialize, module_runge_kutta.f90:34-45).
@@ -68,7 +70,7 @@ struct SplitArgs {
   const double *wlo, *whi;  // control weights: v(y_d) = w . v
   const float *gains;       // control gain per mode
   double control_amp;
-  double nu, pr, lmfxr, lmfzr;
+  double nu, pr, pr2, lmfxr, lmfzr;
   DevScalars *dsc;
   const double *dt_ptr;
   double *vf;        // the v operator's profile LU per mode: LBand, then UBand at vf + vf_l
@@ -151,8 +153,11 @@ __device__ __forceinline__ void hvhg_role(const SplitArgs &a, const Tabs<BW> &tb
   // (substep 1, FP64 state) in double2
   const Line<PT> Z0{reinterpret_cast<PT *>(a.zl + (2 * ROLE) * ns) + m, nm};
   const DLine Z1{a.zl + (2 * ROLE + 1) * ns + m, nm};
-  constexpr int store_slot = ROLE == 0 ? 1 : ROLE == 1 ? 2 : 0;  // RK_STORE 2, 3, 1
-  constexpr int d2_line = ROLE == 0 ? H_DP : ROLE == 1 ? H_DT : H_DG;
+  // role 4 is a second scalar: products u, v, w theta2 in P slots 8, 9, 10, store 4
+  constexpr bool SCAL = ROLE == 1 || ROLE == 4;
+  constexpr int s7 = ROLE == 4 ? 8 : 5, s8 = ROLE == 4 ? 9 : 6, s9 = ROLE == 4 ? 10 : 7;
+  constexpr int store_slot = ROLE == 0 ? 1 : ROLE == 1 ? 2 : ROLE == 4 ? 3 : 0;  // RK_STORE 2, 3, (4), 1
+  constexpr int d2_line = ROLE == 0 ? H_DP : ROLE == 1 ? H_DT : ROLE == 4 ? H_DT2 : H_DG;
   const DLine Rs{a.RK + store_slot * ns + m, nm};
   auto hl = [&](int i) { return DLine{a.hl + i * ns + m, nm}; };
   auto hv = [&](int i) { return Line<PT>{reinterpret_cast<PT *>(a.hl) + i * ns + m, nm}; };
@@ -169,8 +174,8 @@ __device__ __forceinline__ void hvhg_role(const SplitArgs &a, const Tabs<BW> &tb
         if constexpr (ROLE == 0) {
           const double2 f1 = prod(0, r), f3 = prod(2, r), f5 = prod(4, r);
           b[0] = zsub(zsub(zscale(-kx2, f1), zscale(2.0 * kxkz, f5)), zscale(kz2, f3));
-        } else if constexpr (ROLE == 1) {
-          b[0] = prod(6, r);
+        } else if constexpr (SCAL) {
+          b[0] = prod(s8, r);
         } else if constexpr (ROLE == 2) {
           b[0] = prod(1, r);
         } else {
@@ -189,7 +194,7 @@ __device__ __forceinline__ void hvhg_role(const SplitArgs &a, const Tabs<BW> &tb
       },
       [&](int r) {
         if constexpr (ROLE == 0) { pfp(0, r); pfp(2, r); pfp(4, r); }
-        else pfp(ROLE == 1 ? 6 : ROLE == 2 ? 1 : 3, r);
+        else pfp(SCAL ? s8 : ROLE == 2 ? 1 : 3, r);
         if constexpr (NC == 2) pf_l1(Rs.p + (r - 1) * (int)nm);
         if (probe) pf_l1(Sv.p + (r - 1) * (int)nm);
       });
@@ -209,11 +214,11 @@ __device__ __forceinline__ void hvhg_role(const SplitArgs &a, const Tabs<BW> &tb
           const double2 f2 = prod(1, q), f4 = prod(3, q);
           const double2 ehv = z2(-c2i * f2.y - c4i * f4.y, c2i * f2.x + c4i * f4.x);
           hv(H_HV0).st(q, zadd(ehv, mvc<BW>(tb.t1, q, r, wc[0])));
-        } else if constexpr (ROLE == 1) {
-          const double2 f7 = prod(5, q), f9 = prod(7, q);
+        } else if constexpr (SCAL) {
+          const double2 f7 = prod(s7, q), f9 = prod(s9, q);
           const double2 t7 = z2(-kx * f7.y - kz * f9.y, kx * f7.x + kz * f9.x);
           const double2 t = zadd(t7, mvc<BW>(tb.t1, q, r, wc[0]));
-          hv(H_HT).st(q, z2(-t.x, -t.y));
+          hv(ROLE == 4 ? H_HT2 : H_HT).st(q, z2(-t.x, -t.y));
         } else if constexpr (ROLE == 2) {
           const double2 f1 = prod(0, q), f3 = prod(2, q), f5 = prod(4, q);
           const double2 a1 = zadd(zscale(kxkz, zsub(f1, f3)), zscale(kz2 - kx2, f5));
@@ -233,14 +238,15 @@ __device__ __forceinline__ void hvhg_role(const SplitArgs &a, const Tabs<BW> &tb
         if (r <= n - 2 * BW) {
           const int q = r + BW;
           if constexpr (ROLE == 0) { pfp(1, q); pfp(3, q); }
-          else if constexpr (ROLE == 1) { pfp(5, q); pfp(7, q); }
+          else if constexpr (SCAL) { pfp(s7, q); pfp(s9, q); }
           else if constexpr (ROLE == 2) { pfp(0, q); pfp(2, q); pfp(4, q); }
         }
       });
 }
 
-template <int BW, typename PT>
-__global__ void __launch_bounds__(kLanes * kRoles, 4) k_hvhg(SplitArgs a) {
+// NS passive scalars: roles 0..3 as above, role 4 the second scalar's h_theta2.
+template <int BW, typename PT, int NS>
+__global__ void __launch_bounds__(kLanes * (kRoles + NS - 1), 4) k_hvhg(SplitArgs a) {
   if (a.dsc->err) return;
   const int role = threadIdx.x / kLanes;
   const int64_t m = (int64_t)blockIdx.x * kLanes + (threadIdx.x % kLanes);
@@ -251,7 +257,10 @@ __global__ void __launch_bounds__(kLanes * kRoles, 4) k_hvhg(SplitArgs a) {
     case 0: s1 ? hvhg_role<BW, PT, 0, 2>(a, tb, m) : hvhg_role<BW, PT, 0, 1>(a, tb, m); break;
     case 1: s1 ? hvhg_role<BW, PT, 1, 2>(a, tb, m) : hvhg_role<BW, PT, 1, 1>(a, tb, m); break;
     case 2: s1 ? hvhg_role<BW, PT, 2, 2>(a, tb, m) : hvhg_role<BW, PT, 2, 1>(a, tb, m); break;
-    default: hvhg_role<BW, PT, 3, 1>(a, tb, m); break;
+    case 3: hvhg_role<BW, PT, 3, 1>(a, tb, m); break;
+    default:
+      if constexpr (NS == 2) s1 ? hvhg_role<BW, PT, 4, 2>(a, tb, m) : hvhg_role<BW, PT, 4, 1>(a, tb, m);
+      break;
   }
 }
 
@@ -297,24 +306,27 @@ __device__ __forceinline__ void helmholtz_role(const SplitArgs &a, const Tabs<BW
     return zadd(zadd(zscale(zeta, h), zscale(1.0 - alpha * k2, f)), zscale(alpha, d2f));
   };
 
-  // one complex Helmholtz solve: theta (role 0, h = HT), g (role 1, h = G2 + G3)
-  const double visc = ROLE == 0 ? nu / a.pr : nu;
+  // one complex Helmholtz solve: theta (role 0, h = HT), g (role 1, h = G2 + G3), and a second
+  // scalar theta2 (role 3, h = HT2, nu / pr2)
+  constexpr bool SCAL = ROLE == 0 || ROLE == 3;
+  const double visc = ROLE == 0 ? nu / a.pr : ROLE == 3 ? nu / a.pr2 : nu;
   const double beta = dt * rkc(2, s) * visc;
   const double dummy = 1.0 + beta * k2;
-  const int sslot = ROLE == 0 ? 2 : 0;
+  const int sslot = ROLE == 0 ? 2 : ROLE == 3 ? 3 : 0;
   const DLine store{a.RK + sslot * ns + m, nm};
-  const DLine d2l = hl(ROLE == 0 ? H_DT : H_DG);
+  const DLine d2l = hl(ROLE == 0 ? H_DT : ROLE == 3 ? H_DT2 : H_DG);
   auto hv = [&](int i) { return Line<PT>{reinterpret_cast<PT *>(a.hl) + i * ns + m, nm}; };
-  const PT *hA = hv(ROLE == 0 ? H_HT : H_G2).p, *hB = hv(H_G3).p;
+  constexpr int hline = ROLE == 0 ? H_HT : ROLE == 3 ? H_HT2 : H_G2;
+  const PT *hA = hv(hline).p, *hB = hv(H_G3).p;
   auto hsum = [&](int r) {
-    if constexpr (ROLE == 0) return hv(H_HT).ld(r);
+    if constexpr (SCAL) return hv(hline).ld(r);
     else return zadd(hv(H_G2).ld(r), hv(H_G3).ld(r));
   };
   auto rh = [&](int step, int k) { return ring_hv<PT>(ring, step, k); };
   // forward units: 0 store, 1 hA, 2 hB, 3 D2 store (substep 1)
   lu_fwd<BW, 1, 0, kStageAhead, true>(n, [&](int r, double *rw, bool c) { helm_row<BW>(tb, r, n, dummy, beta, rw, c); },
       [&](int r, double2 *bc, double *) {
-        const double2 h = ROLE == 0 ? rh(r, 1) : zadd(rh(r, 1), rh(r, 2));
+        const double2 h = SCAL ? rh(r, 1) : zadd(rh(r, 1), rh(r, 2));
         bc[0] = rhs(ring.c(r, 0), h, s == 1 ? ring.c(r, 3) : z2(0.0, 0.0), visc, r);
       },
       [&](int r, const double2 *zc, const double *) { Zr.st(r, zc[0]); }, ub,
@@ -325,14 +337,14 @@ __device__ __forceinline__ void helmholtz_role(const SplitArgs &a, const Tabs<BW
         if (s == 1) ring.get(r, 3, row(d2l.p, r));
       });
   // backward units: 0 Z(r), 1..BW U(r, e), BW+1 hA(q), BW+2 hB(q) with q = r + BW
-  const DLine out{ROLE == 0 ? a.S + 3 * ns + m : a.S + m, nm};
+  const DLine out{ROLE == 0 ? a.S + 3 * ns + m : ROLE == 3 ? a.S + 4 * ns + m : a.S + m, nm};
   bwd_emit<BW, 1, 0, kStageAhead, true>(n, [&](int r, int e) { return e <= BW ? ring.d(r, e) : ub.get(r, e); },
       [&](int r, double2 *zc, double *) { zc[0] = ring.c(r, 0); },
       [&](int q, int r, const double2 (&wc)[1][2 * BW + 1], const double (&)[1][2 * BW + 1]) {
         const double2 f = mvc<BW>(tb.t0, q, r, wc[0]), d2f = mvc<BW>(tb.t2, q, r, wc[0]);
         out.st(q, f);
         double2 h;
-        if (q == r + BW) h = ROLE == 0 ? rh(r, BW + 1) : zadd(rh(r, BW + 1), rh(r, BW + 2));
+        if (q == r + BW) h = SCAL ? rh(r, BW + 1) : zadd(rh(r, BW + 1), rh(r, BW + 2));
         else h = hsum(q);
         store.st(q, store_new(h, f, d2f, visc));
       },
@@ -530,16 +542,16 @@ __global__ void __launch_bounds__(128) k_vop_factor(SplitArgs a) {
   }
 }
 
-// Three roles per mode: theta, g, and phi with v (helmholtz_phi_v).
+// Three roles per mode: theta, g, and phi with v (helmholtz_phi_v); a fourth for a second scalar.
 constexpr int kHelmRoles = 3;
 
-template <int BW>
+template <int BW, int NS = 1>
 constexpr size_t helm_smem() {
-  return sizeof(double2) * (size_t)kStageSlots * kHelmUnits<BW> * kLanes * kHelmRoles;
+  return sizeof(double2) * (size_t)kStageSlots * kHelmUnits<BW> * kLanes * (kHelmRoles + NS - 1);
 }
 
-template <int BW, typename PT>
-__global__ void __launch_bounds__(kLanes * kHelmRoles, 4) k_helmholtz(SplitArgs a) {
+template <int BW, typename PT, int NS>
+__global__ void __launch_bounds__(kLanes * (kHelmRoles + NS - 1), 4) k_helmholtz(SplitArgs a) {
   extern __shared__ double2 helm_ring[];
   if (a.dsc->err) return;  // a failed dt update leaves the state untouched
   const int role = threadIdx.x / kLanes;
@@ -550,7 +562,10 @@ __global__ void __launch_bounds__(kLanes * kHelmRoles, 4) k_helmholtz(SplitArgs 
   switch (role) {
     case 0: helmholtz_role<BW, 0, PT>(a, tb, m, ring); break;
     case 1: helmholtz_role<BW, 1, PT>(a, tb, m, ring); break;
-    default: helmholtz_phi_v<BW, PT>(a, tb, m, ring); break;
+    case 2: helmholtz_phi_v<BW, PT>(a, tb, m, ring); break;
+    default:
+      if constexpr (NS == 2) helmholtz_role<BW, 3, PT>(a, tb, m, ring);
+      break;
   }
 }
 
@@ -603,13 +618,14 @@ __global__ void __launch_bounds__(256) k_assemble(SplitArgs a) {
 // k_mean: wave00.f90 for one mean line per thread: U (line 0: forced, Galilean shift),
 // W (line 1: phi = 0), Theta (line 2: nu/pr, forced to the bulk value).
 struct MeanArgs {
-  int ny, substep;
+  int ny, substep, nsc;
   int64_t nmodes, ns;
   double2 *S, *RK;
   const void *P;
   double *w00;
   const double *tabs, *integ;
   double nu, pr, bulk_u, bulk_w, bulk_t, u_gal;
+  double pr2, bulk_t2;  // a second passive scalar (line 3)
   DevScalars *dsc;
   const double *dt_ptr;
 };
@@ -617,18 +633,19 @@ struct MeanArgs {
 template <int BW, typename PT>
 __global__ void k_mean(MeanArgs a) {
   const int line = threadIdx.x;
-  if (line >= 3 || a.dsc->err) return;
+  if (line >= 2 + a.nsc || a.dsc->err) return;
   const Tabs<BW> tb = tabs_at<BW>(a.tabs, a.ny);
   const int n = a.ny, s = a.substep;
   const int64_t ns = a.ns;
   const double dt = *a.dt_ptr;
-  const double visc = (line == 2) ? a.nu / a.pr : a.nu;
+  // line 3: a second passive scalar, the theta block with its own Prandtl number and bulk value
+  const double visc = (line == 2) ? a.nu / a.pr : (line == 3) ? a.nu / a.pr2 : a.nu;
   const double gal = (line == 0) ? a.u_gal : 0.0;
-  const double bulk = (line == 0) ? a.bulk_u : (line == 1) ? a.bulk_w : a.bulk_t;
-  const int pslot = (line == 0) ? 1 : (line == 1) ? 3 : 6;  // uv, vw, v theta
+  const double bulk = (line == 0) ? a.bulk_u : (line == 1) ? a.bulk_w : (line == 2) ? a.bulk_t : a.bulk_t2;
+  const int pslot = (line == 0) ? 1 : (line == 1) ? 3 : (line == 2) ? 6 : 9;  // uv, vw, v theta, v theta2
   const PT *P = reinterpret_cast<const PT *>(a.P) + pslot * ns;
   const DLine store{a.RK + line * ns, a.nmodes};
-  const DLine out{a.S + (line == 0 ? 0 : line == 1 ? 2 : 3) * ns, a.nmodes};
+  const DLine out{a.S + (line == 0 ? 0 : line == 1 ? 2 : line == 2 ? 3 : 4) * ns, a.nmodes};
   const int64_t per = 8 * (int64_t)n + 2 * BW * (int64_t)n;  // doubles per line thread
   double *base = a.w00 + line * per;
   const DLine Zf{reinterpret_cast<double2 *>(base), 1}, Zs{reinterpret_cast<double2 *>(base) + n, 1};
@@ -712,9 +729,11 @@ __global__ void k_mean(MeanArgs a) {
     const double wall = r1[0] * creal(1) + r1[1] * creal(2) - rn[-1] * creal(n - 1) - rn[0] * creal(n);
     if (line == 0) a.dsc->wall_shear_stress = 0.5 * a.nu * wall;
     if (line == 2) a.dsc->wall_theta_stress = 0.5 * a.nu / a.pr * wall;
+    if (line == 3) a.dsc->wall_theta_stress2 = 0.5 * a.nu / a.pr2 * wall;
   }
   if (line == 0) a.dsc->phi_dpdx[s - 1] = phi;
   if (line == 2) a.dsc->phi_dtdx[s - 1] = phi;
+  if (line == 3) a.dsc->phi_dtdx2[s - 1] = phi;
   bwd_emit<BW, 1, 0>(n, [&](int, int) { return 0.0; },
       [&](int r, double2 *zc, double *) { zc[0] = z2(creal(r), 0.0); },
       [&](int q, int r, const double2 (&wc)[1][2 * BW + 1], const double (&)[1][2 * BW + 1]) {
@@ -768,6 +787,7 @@ cudaError_t split_bw(Handle &h, int part, int substep, const double *dt_ptr, cud
   a.control_amp = h.cfg.control_amp;
   a.nu = h.cfg.nu;
   a.pr = h.cfg.pr;
+  a.pr2 = h.cfg.pr2;
   a.lmfxr = h.lmfxr;
   a.lmfzr = h.lmfzr;
   a.dsc = h.dsc;
@@ -778,6 +798,9 @@ cudaError_t split_bw(Handle &h, int part, int substep, const double *dt_ptr, cud
   MeanArgs ma;
   ma.ny = h.ny;
   ma.substep = substep;
+  ma.nsc = h.nsc;
+  ma.pr2 = h.cfg.pr2;
+  ma.bulk_t2 = h.cfg.bulk_t2;
   ma.nmodes = h.nmodes;
   ma.ns = h.ns;
   ma.S = h.S;
@@ -805,13 +828,24 @@ cudaError_t split_bw(Handle &h, int part, int substep, const double *dt_ptr, cud
     else k_mean<BW, double2><<<1, 32, 0, h.side>>>(ma);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
     if ((e = cudaEventRecord(h.ev_join, h.side)) != cudaSuccess) return e;
-    if (h.mixed) k_hvhg<BW, float2><<<blocks, kLanes * kRoles, 0, st>>>(a);
-    else k_hvhg<BW, double2><<<blocks, kLanes * kRoles, 0, st>>>(a);
+    if (h.nsc == 2) {
+      if (h.mixed) k_hvhg<BW, float2, 2><<<blocks, kLanes * (kRoles + 1), 0, st>>>(a);
+      else k_hvhg<BW, double2, 2><<<blocks, kLanes * (kRoles + 1), 0, st>>>(a);
+    } else {
+      if (h.mixed) k_hvhg<BW, float2, 1><<<blocks, kLanes * kRoles, 0, st>>>(a);
+      else k_hvhg<BW, double2, 1><<<blocks, kLanes * kRoles, 0, st>>>(a);
+    }
     return cudaGetLastError();
   }
   if (part == 1) {
-    if (h.mixed) k_helmholtz<BW, float2><<<blocks, kLanes * kHelmRoles, helm_smem<BW>(), st>>>(a);
-    else k_helmholtz<BW, double2><<<blocks, kLanes * kHelmRoles, helm_smem<BW>(), st>>>(a);
+    if (h.nsc == 2) {
+      constexpr int nt = kLanes * (kHelmRoles + 1);
+      if (h.mixed) k_helmholtz<BW, float2, 2><<<blocks, nt, helm_smem<BW, 2>(), st>>>(a);
+      else k_helmholtz<BW, double2, 2><<<blocks, nt, helm_smem<BW, 2>(), st>>>(a);
+    } else {
+      if (h.mixed) k_helmholtz<BW, float2, 1><<<blocks, kLanes * kHelmRoles, helm_smem<BW>(), st>>>(a);
+      else k_helmholtz<BW, double2, 1><<<blocks, kLanes * kHelmRoles, helm_smem<BW>(), st>>>(a);
+    }
     return cudaGetLastError();
   }
   const dim3 agrid((unsigned)((h.nmodes + 255) / 256), (unsigned)h.ny);
@@ -864,28 +898,40 @@ cudaError_t launch_vop_factor(Handle &h, cudaStream_t st) {
   cudaError_t e = cudaSuccess;
   switch (h.bw) {
     case 2:
-      e = ring_smem(k_helmholtz<2, float2>, helm_smem<2>());
-      if (e == cudaSuccess) e = ring_smem(k_helmholtz<2, double2>, helm_smem<2>());
+      e = ring_smem(k_helmholtz<2, float2, 1>, helm_smem<2>());
+      if (e == cudaSuccess) e = ring_smem(k_helmholtz<2, double2, 1>, helm_smem<2>());
+      if (e == cudaSuccess) e = ring_smem(k_helmholtz<2, float2, 2>, helm_smem<2, 2>());
+      if (e == cudaSuccess) e = ring_smem(k_helmholtz<2, double2, 2>, helm_smem<2, 2>());
       break;
     case 3:
-      e = ring_smem(k_helmholtz<3, float2>, helm_smem<3>());
-      if (e == cudaSuccess) e = ring_smem(k_helmholtz<3, double2>, helm_smem<3>());
+      e = ring_smem(k_helmholtz<3, float2, 1>, helm_smem<3>());
+      if (e == cudaSuccess) e = ring_smem(k_helmholtz<3, double2, 1>, helm_smem<3>());
+      if (e == cudaSuccess) e = ring_smem(k_helmholtz<3, float2, 2>, helm_smem<3, 2>());
+      if (e == cudaSuccess) e = ring_smem(k_helmholtz<3, double2, 2>, helm_smem<3, 2>());
       break;
     case 4:
-      e = ring_smem(k_helmholtz<4, float2>, helm_smem<4>());
-      if (e == cudaSuccess) e = ring_smem(k_helmholtz<4, double2>, helm_smem<4>());
+      e = ring_smem(k_helmholtz<4, float2, 1>, helm_smem<4>());
+      if (e == cudaSuccess) e = ring_smem(k_helmholtz<4, double2, 1>, helm_smem<4>());
+      if (e == cudaSuccess) e = ring_smem(k_helmholtz<4, float2, 2>, helm_smem<4, 2>());
+      if (e == cudaSuccess) e = ring_smem(k_helmholtz<4, double2, 2>, helm_smem<4, 2>());
       break;
     case 5:
-      e = ring_smem(k_helmholtz<5, float2>, helm_smem<5>());
-      if (e == cudaSuccess) e = ring_smem(k_helmholtz<5, double2>, helm_smem<5>());
+      e = ring_smem(k_helmholtz<5, float2, 1>, helm_smem<5>());
+      if (e == cudaSuccess) e = ring_smem(k_helmholtz<5, double2, 1>, helm_smem<5>());
+      if (e == cudaSuccess) e = ring_smem(k_helmholtz<5, float2, 2>, helm_smem<5, 2>());
+      if (e == cudaSuccess) e = ring_smem(k_helmholtz<5, double2, 2>, helm_smem<5, 2>());
       break;
     case 6:
-      e = ring_smem(k_helmholtz<6, float2>, helm_smem<6>());
-      if (e == cudaSuccess) e = ring_smem(k_helmholtz<6, double2>, helm_smem<6>());
+      e = ring_smem(k_helmholtz<6, float2, 1>, helm_smem<6>());
+      if (e == cudaSuccess) e = ring_smem(k_helmholtz<6, double2, 1>, helm_smem<6>());
+      if (e == cudaSuccess) e = ring_smem(k_helmholtz<6, float2, 2>, helm_smem<6, 2>());
+      if (e == cudaSuccess) e = ring_smem(k_helmholtz<6, double2, 2>, helm_smem<6, 2>());
       break;
     case 7:
-      e = ring_smem(k_helmholtz<7, float2>, helm_smem<7>());
-      if (e == cudaSuccess) e = ring_smem(k_helmholtz<7, double2>, helm_smem<7>());
+      e = ring_smem(k_helmholtz<7, float2, 1>, helm_smem<7>());
+      if (e == cudaSuccess) e = ring_smem(k_helmholtz<7, double2, 1>, helm_smem<7>());
+      if (e == cudaSuccess) e = ring_smem(k_helmholtz<7, float2, 2>, helm_smem<7, 2>());
+      if (e == cudaSuccess) e = ring_smem(k_helmholtz<7, double2, 2>, helm_smem<7, 2>());
       break;
     default: break;
   }

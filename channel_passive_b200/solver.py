@@ -53,6 +53,9 @@ class Config:
     control_amp: float = 0.0
     control_yd: float = -1.0 + 15.0 / 180.0
     device: int = 0
+    n_scalar: int = 1
+    pr2: float = 0.2
+    bulk_t2: float = 1.0
 
     def to_c(self) -> KmmConfig:
         c = KmmConfig()
@@ -170,10 +173,17 @@ class Channel:
         RK = _as_state(RK, self.config, "RK")
         check(self._lib.kmm_upload_state(self._h, _dptr(U), U.shape[0], _dptr(RK), dt))
 
-    def download_state(self, nf: int = NFIELD):
+    @property
+    def nstores(self) -> int:
+        """RK stores: 3, plus one for a second passive scalar."""
+        return 3 + (1 if self.config.n_scalar == 2 else 0)
+
+    def download_state(self, nf: int | None = None):
         cfg = self.config
+        if nf is None:
+            nf = NFIELD if cfg.n_scalar != 2 else 11
         U = np.zeros((nf, cfg.nz, cfg.nxh, cfg.ny), dtype=np.complex128)
-        RK = np.zeros((3, cfg.nz, cfg.nxh, cfg.ny), dtype=np.complex128)
+        RK = np.zeros((self.nstores, cfg.nz, cfg.nxh, cfg.ny), dtype=np.complex128)
         check(self._lib.kmm_download_state(self._h, _dptr(U), nf, _dptr(RK)))
         return U, RK
 

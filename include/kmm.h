@@ -62,7 +62,10 @@ typedef struct kmm_config {
   double control_amp;         /* opposition control amplitude A; 0 = no control (reference) */
   double control_yd;          /* detection plane y_d (-1 < y_d < 0); mirrored at the top wall */
   int32_t device;             /* CUDA device ordinal */
-  int32_t reserved[7];
+  int32_t n_scalar;           /* passive scalars: 1 (the reference; 0 reads as 1) or 2 */
+  double pr2;                 /* Prandtl number of the second scalar */
+  double bulk_t2;             /* target bulk value of the second scalar */
+  int32_t reserved[2];
 } kmm_config;
 
 /* Per-step diagnostics printed by main.f90:147-151. */
@@ -73,6 +76,8 @@ typedef struct kmm_scalars {
   double phi_dtdx[4];         /* scalar forcing per substep; [3] = sum/dt after a full step */
   double wall_shear_stress;   /* 0.5 nu (dU/dy|bottom - dU/dy|top), substep 3 */
   double wall_theta_stress;   /* 0.5 nu/pr (dT/dy|bottom - dT/dy|top), substep 3 */
+  double phi_dtdx2[4];        /* the second scalar's forcing (n_scalar = 2), as phi_dtdx */
+  double wall_theta_stress2;  /* the second scalar's wall flux, 0.5 nu/pr2 (dT2/dy|bottom - top) */
 } kmm_scalars;
 
 typedef struct kmm_info {
@@ -114,6 +119,9 @@ void kmm_labs_fill_full(double *M0, double *M1, double *M2, double *M3, double *
 
 /* State exchange in the reference layout (module_ppdfftw.f90:298-335 allocations).
  * U holds nf >= 7 fields; fields 1,2,3,7 (u, v, w, theta) are used.  rk holds the 3 stores.
+ * With a second passive scalar (n_scalar = 2, no counterpart in the reference, which carries one
+ * scalar) U needs nf >= 11 and holds it in field 11, and rk holds a fourth store (its RK term,
+ * which between steps is the scalar itself, as RK_STORE 3 is theta).
  * Host pointers; pinned memory makes the copies asynchronous-capable. */
 int kmm_upload_state(kmm_handle *h, const double *U, int nf, const double *rk, double dt);
 int kmm_download_state(kmm_handle *h, double *U, int nf, double *rk);

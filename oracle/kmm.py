@@ -61,6 +61,15 @@ class Params:
     control_yplus: float = 15.0
     re_tau: float = 180.0
     gains: np.ndarray | None = None  # per-(kz,kx) control gains, default 1
+    n_scalar: int = 1                # passive scalars: 1 (the reference) or 2
+    pr2: float = 0.2                 # Prandtl number of the second scalar
+    bulk_t2: float = 1.0             # target bulk value of the second scalar
+
+    @property
+    def nslots(self):
+        """Field slots of U: the reference's 10, plus theta2 and its three products (u, v, w
+        times theta2) in slots 10..13 when a second scalar runs."""
+        return 10 if self.n_scalar == 1 else 14
 
     # derived, read_input_file.f90:94-116
     @property
@@ -213,6 +222,11 @@ def dft_x_realspace(Up: np.ndarray, nx: int, substep: int, dxr: float, dzr: floa
     bv2 = v * v
     prods = {8: w * t, 7: v * t, 6: u * t, 4: u * w, 3: v * w, 2: w * w - bv2,
              1: u * v, 0: u * u - bv2, 9: v}
+    if Up.shape[0] > 10:
+        # a second passive scalar theta2 (slot 10): its products u, v, w theta2 in slots 11..13,
+        # formed like f7..f9 (dft_x_realspace.f90:119-121)
+        t2 = c2r(Up[10])
+        prods.update({11: u * t2, 12: v * t2, 13: w * t2})
     if stat:
         prods[5] = bv2
     velmax = 0.0
@@ -423,7 +437,7 @@ def calculate_phi(bulk, integral):
     return (bulk - 0.5 * integral.real) / (0.5 * integral.imag)
 
 
-def wave00(u2, u4, u8, store1, store2, store3, ops: Operators, p: Params, s, dt):
+def wave00(u2, u4, u8, store1, store2, store3, ops: Operators, p: Params, s, dt, theta2=None):
     """wave00.f90:41-685 for the kx = kz = 0 mode (1-D complex lines of ny).
 
     Returns dict with u, w, theta (new mean profiles), the stores, phi_dpdx,
@@ -500,6 +514,16 @@ def wave00(u2, u4, u8, store1, store2, store3, ops: Operators, p: Params, s, dt)
         out["wall_theta_stress"] = 0.5 * nu / pr * wall_grad(buf1)
     out["store3"] = upd(u7) if upd else u7.copy()
     out["theta"] = u7
+    if theta2 is not None:
+        # the second scalar's mean line, same block with nu/pr2 and its own bulk value
+        u12, store4 = theta2
+        visc_t2 = nu / p.pr2
+        buf1, u11, phi_t2, upd = mean_line(store4, u12, visc_t2, p.bulk_t2, 0.0, True)
+        out["phi_dtdx2"] = phi_t2
+        if s == 3:
+            out["wall_theta_stress2"] = 0.5 * nu / p.pr2 * wall_grad(buf1)
+        out["store4"] = upd(u11) if upd else u11.copy()
+        out["theta2"] = u11
     return out
 
 
@@ -531,6 +555,8 @@ class Scalars:
     wall_theta_stress: float = 0.0
     velmax: float = 0.0
     dt: float = 0.0
+    phi_dtdx2: list = field(default_factory=lambda: [0.0] * 4)
+    wall_theta_stress2: float = 0.0
 
 
 def wavespace(U, RK, ops: Operators, p: Params, s: int, dt: float, sc: Scalars, ctrl=None):
@@ -549,8 +575,10 @@ def wavespace(U, RK, ops: Operators, p: Params, s: int, dt: float, sc: Scalars, 
     sg, sp, st = lines(0, RK), lines(1, RK), lines(2, RK)
     # (0,0) first: it reads the unmodified product lines
     i0 = np.argwhere((KX == 0) & (KZ == 0))[0]
+    two = p.n_scalar == 2
     m00 = wave00(U[1][tuple(i0)], U[3][tuple(i0)], U[7][tuple(i0)],
-                 RK[0][tuple(i0)], RK[1][tuple(i0)], RK[2][tuple(i0)], ops, p, s, dt)
+                 RK[0][tuple(i0)], RK[1][tuple(i0)], RK[2][tuple(i0)], ops, p, s, dt,
+                 (U[12][tuple(i0)], RK[3][tuple(i0)]) if two else None)
     hg, hv, ht = hvhg(u1, u2, u3, u4, u5, u7, u8, u9, ops, kx, kz)
     g, sg, D_buf_g = solve_scalar_helmholtz(hg, sg, ops, kx, kz, (p.nu, None), s, dt)
     vwall = None
@@ -565,6 +593,14 @@ def wavespace(U, RK, ops: Operators, p: Params, s: int, dt: float, sc: Scalars, 
         U[slot][mask] = val.T
     for slot, val in ((0, sg), (1, sp), (2, st)):
         RK[slot][mask] = val.T
+    if two:
+        # theta2: h = -(i kx (u theta2) + i kz (w theta2) + D1 D0^-1 (v theta2)) as hvhg forms h_theta
+        # (hvhg.f90:146-159), then solve_t with pr2
+        u11, u12, u13, s4 = lines(11), lines(12), lines(13), lines(3, RK)
+        ht2 = -((1j * kx) * u11 + (1j * kz) * u13 + labs.mat_mul(ops.D1, labs.bs(ops.D0_lu, u12)))
+        th2, s4, _ = solve_scalar_helmholtz(ht2, s4, ops, kx, kz, (p.nu, p.pr2), s, dt)
+        U[10][mask] = th2.T
+        RK[3][mask] = s4.T
     idx = tuple(i0)
     U[0][idx], U[1][idx], U[2][idx], U[6][idx] = m00["u"], m00["v"], m00["w"], m00["theta"]
     RK[0][idx], RK[1][idx], RK[2][idx] = m00["store1"], m00["store2"], m00["store3"]
@@ -573,6 +609,12 @@ def wavespace(U, RK, ops: Operators, p: Params, s: int, dt: float, sc: Scalars, 
     if s == 3:
         sc.wall_shear_stress = m00["wall_shear_stress"]
         sc.wall_theta_stress = m00["wall_theta_stress"]
+    if two:
+        U[10][idx] = m00["theta2"]
+        RK[3][idx] = m00["store4"]
+        sc.phi_dtdx2[s - 1] = m00["phi_dtdx2"]
+        if s == 3:
+            sc.wall_theta_stress2 = m00["wall_theta_stress2"]
 
 
 class DtError(RuntimeError):
@@ -586,8 +628,9 @@ def time_march(U, RK, ops: Operators, p: Params, s: int, dt: float, sc: Scalars,
     """
     if dyr is None:
         dyr = dyr_vector(ops.y, p.dy_factor)
-    Up = np.zeros((10, p.ny, p.nz32, p.nxh), dtype=np.complex128)
-    for f in (0, 1, 2, 6):
+    two = p.n_scalar == 2
+    Up = np.zeros((p.nslots, p.ny, p.nz32, p.nxh), dtype=np.complex128)
+    for f in (0, 1, 2, 6) + ((10,) if two else ()):
         Up[f] = y_to_x(U[f], p.nz32)
     velmax = dft_x_realspace(Up, p.nx, s, p.dxr, p.dzr, dyr)
     if s == 1:
@@ -596,9 +639,14 @@ def time_march(U, RK, ops: Operators, p: Params, s: int, dt: float, sc: Scalars,
             dt = p.dt_factor * dt + (1.0 - p.dt_factor) * p.cflx / velmax
         if dt <= 1e-14 or dt > 1e5:
             raise DtError(f"ABORT due to timestep dt = {dt}")
-    for f in (0, 1, 2, 3, 4, 6, 7, 8, 9):
+    for f in (0, 1, 2, 3, 4, 6, 7, 8, 9) + ((11, 12, 13) if two else ()):
         U[f] = x_to_y(Up[f], p.nz)
-    U *= p.rescale
+    if two:
+        theta2 = U[10].copy()
+        U *= p.rescale
+        U[10] = theta2  # the scalar itself is not a transformed product
+    else:
+        U *= p.rescale
     wavespace(U, RK, ops, p, s, dt, sc, ctrl)
     sc.dt = dt
     return dt
@@ -611,13 +659,16 @@ def rk3_step(U, RK, ops, p, dt, sc=None, dyr=None, ctrl=None):
         dt = time_march(U, RK, ops, p, s, dt, sc, dyr, ctrl)
     sc.phi_dpdx[3] = (sc.phi_dpdx[0] + sc.phi_dpdx[1] + sc.phi_dpdx[2]) / dt
     sc.phi_dtdx[3] = (sc.phi_dtdx[0] + sc.phi_dtdx[1] + sc.phi_dtdx[2]) / dt
+    sc.phi_dtdx2[3] = (sc.phi_dtdx2[0] + sc.phi_dtdx2[1] + sc.phi_dtdx2[2]) / dt
     return dt, sc
 
 
 def set_initial_data_uvw(U, ops: Operators, p: Params):
     """initial_step.f90:139-179: RK stores from u, v, w, theta (returns RK)."""
     kxi, kzi = wavenumbers(p.nx, p.nz)
-    RK = np.zeros((3, p.nz, p.nxh, p.ny), dtype=np.complex128)
+    RK = np.zeros((3 + (p.n_scalar - 1), p.nz, p.nxh, p.ny), dtype=np.complex128)
+    if p.n_scalar == 2:
+        RK[3] = U[10]  # the second scalar's store is the scalar (as RK_STORE 3 is theta)
     lmfxr, lmfzr = 1.0 / p.lmfx, 1.0 / p.lmfz
     for j, kzv in enumerate(kzi):
         for k, kxv in enumerate(kxi):

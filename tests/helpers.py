@@ -19,8 +19,18 @@ def make_pair(nx=16, ny=33, nz=16, lmfx=1.0, lmfz=0.5, stretch=0.9, control_amp=
                     stretch=stretch, nu=cfg.nu, pr=cfg.pr, bulk_u=cfg.bulk_vel_u,
                     bulk_w=cfg.bulk_vel_w, bulk_t=cfg.bulk_t, u_gal=cfg.u_gal, cfl=cfg.cfl,
                     dt_factor=cfg.dt_factor, dy_factor=cfg.dy_factor, fixed_dt=bool(fixed_dt),
-                    control_amp=control_amp, control_yplus=control_yplus, re_tau=RE_TAU)
+                    control_amp=control_amp, control_yplus=control_yplus, re_tau=RE_TAU,
+                    n_scalar=max(1, cfg.n_scalar), pr2=cfg.pr2, bulk_t2=cfg.bulk_t2)
     return cfg, p
+
+
+def with_scalar2(U, theta2=None):
+    """U (10, ...) -> (14, ...) with theta2 in slot 10 (the oracle's two-scalar layout; the C ABI
+    reads field 11 of nf >= 11).  theta2 defaults to theta (slot 6)."""
+    out = np.zeros((14,) + U.shape[1:], dtype=U.dtype)
+    out[:10] = U[:10]
+    out[10] = U[6] if theta2 is None else theta2
+    return out
 
 
 def oracle_ctrl(ops, p, gains=None):
@@ -41,3 +51,4 @@ def rel_l2(a, b):
 
 
 STATE_SLOTS = (0, 1, 2, 6)
+STATE_SLOTS2 = (0, 1, 2, 6, 10)
