@@ -176,8 +176,11 @@ struct X2Args {
 #ifndef KMM_X288_MINB_FP64
 #define KMM_X288_MINB_FP64 8
 #endif
-template <typename R, int N, bool STAT> constexpr int x_min_blocks() {
+template <typename R, int N, bool STAT, int NS = 1> constexpr int x_min_blocks() {
   if (STAT) return 1;
+  // two scalars, FP32 at N = 576: 210 registers uncapped (2 blocks an SM); 3 blocks fit the
+  // shared memory of the six packed lines per row
+  if (NS != 1) return (sizeof(R) == 4 && N >= 576) ? 3 : 1;
   if (sizeof(R) != 4) return N == 288 ? KMM_X288_MINB_FP64 : 1;
   return N >= 576 ? KMM_X576_MINB : N == 288 ? KMM_X288_MINB : 1;
 }
@@ -186,7 +189,7 @@ template <typename R, int N, bool STAT> constexpr int x_min_blocks() {
 // go to slots 8, 9, 10, formed like f7..f9 (a third packed input line (theta2, 0) and two packed
 // output lines (u theta2, v theta2), (w theta2, 0)).
 template <typename R, int N1, int N2, int ZB, int NT, bool STAT = false, int NS = 1>
-__global__ void __launch_bounds__(NT, (x_min_blocks<R, N1 * N2, STAT>())) k_xphys2(typename Cpx<R>::T *__restrict__ mid, FftPlan pl, X2Args a_) {
+__global__ void __launch_bounds__(NT, (x_min_blocks<R, N1 * N2, STAT, NS>())) k_xphys2(typename Cpx<R>::T *__restrict__ mid, FftPlan pl, X2Args a_) {
   using C = typename Cpx<R>::T;
   constexpr int N = N1 * N2, LD = ip_lda<N1, N2>();
   constexpr int NIN = 1 + NS, NOUT = 2 + 2 * NS;  // packed input and output lines per row

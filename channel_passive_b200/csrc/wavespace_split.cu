@@ -244,9 +244,11 @@ __device__ __forceinline__ void hvhg_role(const SplitArgs &a, const Tabs<BW> &tb
       });
 }
 
-// NS passive scalars: roles 0..3 as above, role 4 the second scalar's h_theta2.
+// NS passive scalars: roles 0..3 as above, role 4 the second scalar's h_theta2.  Four resident
+// blocks of one scalar's 128 threads keep 128 registers a thread; with a fifth role three blocks
+// keep 136 (four would cap it at 96 and spill about 1 KB a thread).
 template <int BW, typename PT, int NS>
-__global__ void __launch_bounds__(kLanes * (kRoles + NS - 1), 4) k_hvhg(SplitArgs a) {
+__global__ void __launch_bounds__(kLanes * (kRoles + NS - 1), NS == 1 ? 4 : 3) k_hvhg(SplitArgs a) {
   if (a.dsc->err) return;
   const int role = threadIdx.x / kLanes;
   const int64_t m = (int64_t)blockIdx.x * kLanes + (threadIdx.x % kLanes);
@@ -550,8 +552,10 @@ constexpr size_t helm_smem() {
   return sizeof(double2) * (size_t)kStageSlots * kHelmUnits<BW> * kLanes * (kHelmRoles + NS - 1);
 }
 
+// With a fourth role (a second scalar) three resident blocks keep the 168 registers of one
+// scalar's kernel; four would cap it at 128 and spill.
 template <int BW, typename PT, int NS>
-__global__ void __launch_bounds__(kLanes * (kHelmRoles + NS - 1), 4) k_helmholtz(SplitArgs a) {
+__global__ void __launch_bounds__(kLanes * (kHelmRoles + NS - 1), NS == 1 ? 4 : 3) k_helmholtz(SplitArgs a) {
   extern __shared__ double2 helm_ring[];
   if (a.dsc->err) return;  // a failed dt update leaves the state untouched
   const int role = threadIdx.x / kLanes;
