@@ -508,8 +508,9 @@ def run_kmm(args):
     common = dict(nx=w["nx"], ny=w["ny"], nz=w["nz"], lmfx=w["lmfx"], lmfz=w["lmfz"], stretch=w["stretch"],
                   nu=w["nu"], pr=w["pr"], fixed_dt=1, control_amp=w["control_amp"],
                   control_yd=w["control_yd"], device=local)
-    mixed = Channel(Config(precision=_lib.KMM_PREC_MIXED, **common))
-    fp64 = Channel(Config(precision=_lib.KMM_PREC_FP64, **common))
+    # both handles run the autotuner at creation (kmm_autotune: launch shapes timed on this grid)
+    mixed = Channel(Config(precision=_lib.KMM_PREC_MIXED, autotune=1, **common))
+    fp64 = Channel(Config(precision=_lib.KMM_PREC_FP64, autotune=1, **common))
     U0 = ic.seeded_ic(w["nx"], w["ny"], w["nz"], mixed.y, w["lmfx"], w["lmfz"], seed=SEED + rank)
     dt = 0.01
     # accuracy: 100 steps from the same IC, mixed vs FP64 (the FP64 GPU path matches the oracle
@@ -631,7 +632,9 @@ def run_kmm(args):
                    "graph": True, "parallelism": f"replicas x{world}",
                    "l2": "no flush: the resident state and slabs (>1 GB) exceed the 126 MB L2 every step"},
         "grid_point_steps_per_s": value * w["nx"] * w["ny"] * w["nz"],
-        "fp64": {"value": fp64_value, "ms_per_step": ms_fp64 / args.steps, "kernels": kernels64},
+        "fp64": {"value": fp64_value, "ms_per_step": ms_fp64 / args.steps, "kernels": kernels64,
+                 "tuning": fp64.tuning},
+        "tuning": mixed.tuning,
         "mixed_over_fp64": value / fp64_value,
         "rel_l2_mixed_vs_fp64": rel,
         "rel_l2_steps": args.acc_steps,

@@ -43,7 +43,7 @@ class KmmConfig(C.Structure):
         ("dy_factor", C.c_double), ("fixed_dt", C.c_int32), ("precision", C.c_int32),
         ("control_amp", C.c_double), ("control_yd", C.c_double), ("device", C.c_int32),
         ("n_scalar", C.c_int32), ("pr2", C.c_double), ("bulk_t2", C.c_double),
-        ("reserved", C.c_int32 * 2),
+        ("autotune", C.c_int32), ("reserved", C.c_int32),
     ]
 
 
@@ -68,6 +68,23 @@ class KmmInfo(C.Structure):
         ("nmodes", C.c_int64), ("device_bytes", C.c_int64),
         ("fft_radix_x", C.c_int32 * 8), ("fft_radix_z", C.c_int32 * 8),
     ]
+
+
+class KmmTuning(C.Structure):
+    _fields_ = [
+        ("z_lines_per_block", C.c_int32), ("x_rows_per_block", C.c_int32), ("x_threads", C.c_int32),
+        ("modes_per_block", C.c_int32), ("u_layout", C.c_int32), ("assemble_threads", C.c_int32),
+        ("tuned", C.c_int32), ("reserved", C.c_int32),
+        ("ms_z", C.c_double * 3), ("ms_x", C.c_double * 3), ("ms_modes", C.c_double * 2),
+        ("ms_layout", C.c_double * 2), ("ms_assemble", C.c_double * 3),
+    ]
+
+    def as_dict(self):
+        d = {f: getattr(self, f) for f, _ in self._fields_ if f != "reserved"}
+        for k, v in d.items():
+            if not isinstance(v, (int, float)):
+                d[k] = list(v)
+        return d
 
 
 # every symbol include/kmm.h declares, with its ctypes signature
@@ -122,6 +139,9 @@ SIGNATURES = {
     "kmm_adjoint_forward": (C.c_int, [_P, C.c_int, C.c_double, C.c_double, _D]),
     "kmm_adjoint_backward": (C.c_int, [_P, _D, _D]),
     "kmm_adjoint_release": (C.c_int, [_P]),
+    "kmm_autotune": (C.c_int, [_P, C.POINTER(KmmTuning)]),
+    "kmm_get_tuning": (C.c_int, [_P, C.POINTER(KmmTuning)]),
+    "kmm_set_tuning": (C.c_int, [_P, C.POINTER(KmmTuning)]),
     "kmm_helmholtz_solve_noalloc": (C.c_int, [C.c_int, C.c_int, C.c_int, _P, _P, _P, _P, _P, _P]),
 }
 

@@ -557,6 +557,7 @@ int kmm_create(const kmm_config *cfg, kmm_handle **out) {
       return fail(KMM_ERR_CUDA);
     }
   }
+  if (cfg->autotune && (rc = autotune(*h, nullptr))) return fail(rc);
   *out = reinterpret_cast<kmm_handle *>(h);
   return KMM_OK;
 }

@@ -79,6 +79,16 @@ void host_band_lu(std::vector<double> &a, int bw, int n);
 // The discrete adjoint's buffers (adjoint.cu), made by the first kmm_adjoint_forward.
 struct Adjoint;
 
+// Launch shapes the autotuner (kmm_autotune, tune.cu) chooses; the defaults are the hand-tuned ones.
+struct Tuning {
+  int z = 0;              // z-transform variant (lines per block, transforms2.cu ZVar)
+  int x = 0;              // x-pass variant (rows per block and threads, XVar)
+  int groups = 1;         // 32-mode groups per block of the hvhg and Helmholtz kernels (1 or 2)
+  int ulayout = 0;        // U factor storage: 0 = [offset][y][mode], 1 = [y][offset][mode]
+  int asm_threads = 256;  // threads per block of the assembly kernel
+  bool tuned = false;
+};
+
 struct Handle {
   kmm_config cfg{};
   int nx = 0, ny = 0, nz = 0, nxh = 0, nx32 = 0, nz32 = 0, bw = 0;
@@ -121,6 +131,7 @@ struct Handle {
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t gexec = nullptr;
   Adjoint *adj = nullptr;                  // discrete adjoint state (adjoint.cu), or null
+  Tuning tune;                             // launch shapes (kmm_autotune)
 };
 
 // Offsets of the operator arrays inside dops (doubles).
@@ -180,6 +191,11 @@ void convert_planes_d2f(const double2 *src, float2 *dst, int64_t n, cudaStream_t
 cudaError_t prepare_transforms2();
 // Whether a padded line length has a compile-time four-step shape (transforms2.cu).
 bool fft4_supported(int N);
+// The z lines per block and x rows / threads per block of tile variants zvar, xvar on h's grid
+// (0 where the length has no four-step shape).
+void tile_shapes(const Handle &h, int zvar, int xvar, int *z_lines, int *x_rows, int *x_threads);
+// Runs the autotuner (tune.cu) on h's grid and buffers; the state is left unchanged.
+int autotune(Handle &h, kmm_tuning *out);
 // Four-step transforms (transforms2.cu); return cudaErrorNotSupported for other lengths.
 cudaError_t launch_zinv2(Handle &h, const double2 *src_planes, void *mid, int nfield, cudaStream_t st);
 // stat: the statistics-step variant (f6 = v v, no CFL); mom (stat only, may be null) receives

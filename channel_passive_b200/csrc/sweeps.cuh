@@ -119,6 +119,12 @@ template <int BW>
 __device__ __forceinline__ UBand<BW> make_uband(double *base, int64_t s, int64_t es) {
   return UBand<BW>{base, base + BW * es, s, es};
 }
+// The same with the first rows' extra entries at base + px_off, for layouts whose row and offset
+// strides are not (modes, ny * modes).
+template <int BW>
+__device__ __forceinline__ UBand<BW> make_uband(double *base, int64_t s, int64_t es, int64_t px_off) {
+  return UBand<BW>{base, base + px_off, s, es};
+}
 
 // Per-mode L factor of a profile LU kept for later forward sweeps, the UBand idea for L:
 // L(r, r-d) for d = 0..BW (d = 0 holds 1 / L(r, r)) as [BW+1][ny][mode], plus d = BW+1..2BW of

@@ -176,8 +176,8 @@ struct X2Args {
 #ifndef KMM_X288_MINB_FP64
 #define KMM_X288_MINB_FP64 8
 #endif
-template <typename R, int N, bool STAT, int NS = 1> constexpr int x_min_blocks() {
-  if (STAT) return 1;
+template <typename R, int N, bool STAT, int NS = 1, int V = 0> constexpr int x_min_blocks() {
+  if (STAT || V != 0) return 1;  // the caps below were measured for the default shape
   // two scalars, FP32 at N = 576: 210 registers uncapped (2 blocks an SM); 3 blocks fit the
   // shared memory of the six packed lines per row
   if (NS != 1) return (sizeof(R) == 4 && N >= 576) ? 3 : 1;
@@ -188,8 +188,8 @@ template <typename R, int N, bool STAT, int NS = 1> constexpr int x_min_blocks()
 // NS = 2: a second passive scalar theta2 in MID slot 4; its products u theta2, v theta2, w theta2
 // go to slots 8, 9, 10, formed like f7..f9 (a third packed input line (theta2, 0) and two packed
 // output lines (u theta2, v theta2), (w theta2, 0)).
-template <typename R, int N1, int N2, int ZB, int NT, bool STAT = false, int NS = 1>
-__global__ void __launch_bounds__(NT, (x_min_blocks<R, N1 * N2, STAT, NS>())) k_xphys2(typename Cpx<R>::T *__restrict__ mid, FftPlan pl, X2Args a_) {
+template <typename R, int N1, int N2, int ZB, int NT, bool STAT = false, int NS = 1, int V = 0>
+__global__ void __launch_bounds__(NT, (x_min_blocks<R, N1 * N2, STAT, NS, V>())) k_xphys2(typename Cpx<R>::T *__restrict__ mid, FftPlan pl, X2Args a_) {
   using C = typename Cpx<R>::T;
   constexpr int N = N1 * N2, LD = ip_lda<N1, N2>();
   constexpr int NIN = 1 + NS, NOUT = 2 + 2 * NS;  // packed input and output lines per row
@@ -427,13 +427,42 @@ template <> struct TCfg<double> {
   static constexpr int KB = 8, ZB = 1, ZT = 64;
 };
 
-template <typename R, int N1, int N2>
-constexpr size_t z_smem() {
-  return sizeof(typename Cpx<R>::T) * (size_t)TCfg<R>::KB * ip_lda<N1, N2>();
+// Tile-shape variants the autotuner (kmm_autotune) times on the handle's grid; variant 0 is the
+// hand-tuned TCfg.  The others are built for lengths of kMinTunedLength points and more only
+// (shorter lines fall back to variant 0 at compile time).
+constexpr int kMinTunedLength = 96;
+template <typename R, int V> struct ZVar;  // z transforms: lines per block
+template <> struct ZVar<float, 0> { static constexpr int KB = TCfg<float>::KB; };
+template <> struct ZVar<float, 1> { static constexpr int KB = 8; };
+template <> struct ZVar<float, 2> { static constexpr int KB = 32; };
+template <> struct ZVar<double, 0> { static constexpr int KB = TCfg<double>::KB; };
+template <> struct ZVar<double, 1> { static constexpr int KB = 4; };
+template <> struct ZVar<double, 2> { static constexpr int KB = 16; };
+template <typename R, int V> struct XVar;  // x pass: rows per block and threads
+template <> struct XVar<float, 0> { static constexpr int ZB = TCfg<float>::ZB, ZT = TCfg<float>::ZT; };
+template <> struct XVar<float, 1> { static constexpr int ZB = 1, ZT = 128; };
+template <> struct XVar<float, 2> { static constexpr int ZB = 4, ZT = 256; };
+template <> struct XVar<double, 0> { static constexpr int ZB = TCfg<double>::ZB, ZT = TCfg<double>::ZT; };
+template <> struct XVar<double, 1> { static constexpr int ZB = 1, ZT = 128; };
+template <> struct XVar<double, 2> { static constexpr int ZB = 2, ZT = 128; };
+template <int N, int V> constexpr int tuned_variant() { return N < kMinTunedLength ? 0 : V; }
+
+// Runs f.template operator()<V>() for the runtime variant v (0..2).
+template <typename F> void with_variant(int v, F &&f) {
+  switch (v) {
+    case 1: f.template operator()<1>(); break;
+    case 2: f.template operator()<2>(); break;
+    default: f.template operator()<0>(); break;
+  }
 }
-template <typename R, int N1, int N2, int NS = 1>
+
+template <typename R, int N1, int N2, int KB = TCfg<R>::KB>
+constexpr size_t z_smem() {
+  return sizeof(typename Cpx<R>::T) * (size_t)KB * ip_lda<N1, N2>();
+}
+template <typename R, int N1, int N2, int NS = 1, int ZB = TCfg<R>::ZB>
 constexpr size_t x_smem() {
-  return sizeof(typename Cpx<R>::T) * (size_t)(2 + 2 * NS) * TCfg<R>::ZB * ip_lda<N1, N2>();
+  return sizeof(typename Cpx<R>::T) * (size_t)(2 + 2 * NS) * ZB * ip_lda<N1, N2>();
 }
 
 }  // namespace
@@ -470,18 +499,26 @@ cudaError_t prepare_transforms2() {
     with_shape(N, [&]<int N1, int N2>() {
       using F = TCfg<float>;
       using D = TCfg<double>;
-      set_smem(k_zinv2<double, N1, N2, D::KB>, optin);
-      set_smem(k_zinv2<float, N1, N2, F::KB>, optin);
-      set_smem(k_zfwd2<double, N1, N2, D::KB, double2>, optin);
-      set_smem(k_zfwd2<float, N1, N2, F::KB, float2>, optin);
-      set_smem(k_zfwd2<float, N1, N2, F::KB, double2>, optin);
-      set_smem(k_xphys2<double, N1, N2, D::ZB, D::ZT>, optin);
-      set_smem(k_xphys2<float, N1, N2, F::ZB, F::ZT>, optin);
       set_smem(k_xphys2<double, N1, N2, D::ZB, D::ZT, true>, optin);
       set_smem(k_xphys2<float, N1, N2, F::ZB, F::ZT, true>, optin);
-      set_smem(k_xphys2<double, N1, N2, D::ZB, D::ZT, false, 2>, optin);
-      set_smem(k_xphys2<float, N1, N2, F::ZB, F::ZT, false, 2>, optin);
       set_smem(k_xadj2<N1, N2>, optin);
+      for (int v = 0; v < 3; ++v)
+        with_variant(v, [&]<int V>() {
+          constexpr int VV = tuned_variant<N1 * N2, V>();
+          using ZF = ZVar<float, VV>;
+          using ZD = ZVar<double, VV>;
+          using XF = XVar<float, VV>;
+          using XD = XVar<double, VV>;
+          set_smem(k_zinv2<double, N1, N2, ZD::KB>, optin);
+          set_smem(k_zinv2<float, N1, N2, ZF::KB>, optin);
+          set_smem(k_zfwd2<double, N1, N2, ZD::KB, double2>, optin);
+          set_smem(k_zfwd2<float, N1, N2, ZF::KB, float2>, optin);
+          set_smem(k_zfwd2<float, N1, N2, ZF::KB, double2>, optin);
+          set_smem(k_xphys2<double, N1, N2, XD::ZB, XD::ZT, false, 1, VV>, optin);
+          set_smem(k_xphys2<float, N1, N2, XF::ZB, XF::ZT, false, 1, VV>, optin);
+          set_smem(k_xphys2<double, N1, N2, XD::ZB, XD::ZT, false, 2, VV>, optin);
+          set_smem(k_xphys2<float, N1, N2, XF::ZB, XF::ZT, false, 2, VV>, optin);
+        });
     });
   }
   return cudaSuccess;
@@ -492,12 +529,14 @@ cudaError_t launch_zinv2(Handle &h, const double2 *src, void *mid, int nfield, c
   cudaError_t err = cudaErrorNotSupported;
   auto go = [&]<typename R>() {
     with_shape(h.nz32, [&]<int N1, int N2>() {
-      using C = typename Cpx<R>::T;
-      using T = TCfg<R>;
-      dim3 grid((unsigned)((h.nxh + T::KB - 1) / T::KB), (unsigned)h.ny, (unsigned)nfield);
-      k_zinv2<R, N1, N2, T::KB><<<grid, z_threads<N1, N2, T::KB>(), z_smem<R, N1, N2>(), st>>>(
-          src, reinterpret_cast<C *>(mid), h.pz, h.nz, h.nxh, h.ns, h.nm);
-      err = cudaGetLastError();
+      with_variant(h.tune.z, [&]<int V>() {
+        using C = typename Cpx<R>::T;
+        constexpr int KB = ZVar<R, tuned_variant<N1 * N2, V>()>::KB;
+        dim3 grid((unsigned)((h.nxh + KB - 1) / KB), (unsigned)h.ny, (unsigned)nfield);
+        k_zinv2<R, N1, N2, KB><<<grid, z_threads<N1, N2, KB>(), z_smem<R, N1, N2, KB>(), st>>>(
+            src, reinterpret_cast<C *>(mid), h.pz, h.nz, h.nxh, h.ns, h.nm);
+        err = cudaGetLastError();
+      });
     });
   };
   if (h.mixed) go.template operator()<float>();
@@ -510,12 +549,14 @@ cudaError_t launch_zfwd2(Handle &h, const void *mid, void *dst, int nfield, doub
   cudaError_t err = cudaErrorNotSupported;
   auto go = [&]<typename R, typename D>() {
     with_shape(h.nz32, [&]<int N1, int N2>() {
-      using C = typename Cpx<R>::T;
-      using T = TCfg<R>;
-      dim3 grid((unsigned)((h.nxh + T::KB - 1) / T::KB), (unsigned)h.ny, (unsigned)nfield);
-      k_zfwd2<R, N1, N2, T::KB, D><<<grid, z_threads<N1, N2, T::KB>(), z_smem<R, N1, N2>(), st>>>(
-          reinterpret_cast<const C *>(mid), reinterpret_cast<D *>(dst), h.pz, h.nz, h.nxh, h.ns, h.nm, scale);
-      err = cudaGetLastError();
+      with_variant(h.tune.z, [&]<int V>() {
+        using C = typename Cpx<R>::T;
+        constexpr int KB = ZVar<R, tuned_variant<N1 * N2, V>()>::KB;
+        dim3 grid((unsigned)((h.nxh + KB - 1) / KB), (unsigned)h.ny, (unsigned)nfield);
+        k_zfwd2<R, N1, N2, KB, D><<<grid, z_threads<N1, N2, KB>(), z_smem<R, N1, N2, KB>(), st>>>(
+            reinterpret_cast<const C *>(mid), reinterpret_cast<D *>(dst), h.pz, h.nz, h.nxh, h.ns, h.nm, scale);
+        err = cudaGetLastError();
+      });
     });
   };
   if (h.mixed) {
@@ -537,6 +578,24 @@ cudaError_t launch_xadj2(Handle &h, const double2 *base_mid, double2 *lmid, doub
     err = cudaGetLastError();
   });
   return err;
+}
+
+void tile_shapes(const Handle &h, int zvar, int xvar, int *z_lines, int *x_rows, int *x_threads) {
+  *z_lines = *x_rows = *x_threads = 0;
+  auto zf = [&]<typename R>() {
+    with_shape(h.nz32, [&]<int N1, int N2>() {
+      with_variant(zvar, [&]<int V>() { *z_lines = ZVar<R, tuned_variant<N1 * N2, V>()>::KB; });
+    });
+    with_shape(h.nx32, [&]<int N1, int N2>() {
+      with_variant(xvar, [&]<int V>() {
+        using T = XVar<R, tuned_variant<N1 * N2, V>()>;
+        *x_rows = T::ZB;
+        *x_threads = T::ZT;
+      });
+    });
+  };
+  if (h.mixed) zf.template operator()<float>();
+  else zf.template operator()<double>();
 }
 
 int xphys2_row_blocks(const Handle &h) {
@@ -561,16 +620,26 @@ cudaError_t launch_xphys2(Handle &h, void *mid, int substep, cudaStream_t st, bo
   auto go = [&]<typename R>() {
     with_shape(h.nx32, [&]<int N1, int N2>() {
       using C = typename Cpx<R>::T;
-      using T = TCfg<R>;
-      dim3 grid((unsigned)((h.nz32 + T::ZB - 1) / T::ZB), (unsigned)h.ny);
-      if (stat)
+      if (stat) {
+        // the statistics variant keeps the default shape: its moment sums are laid out per row block
+        using T = TCfg<R>;
+        dim3 grid((unsigned)((h.nz32 + T::ZB - 1) / T::ZB), (unsigned)h.ny);
         k_xphys2<R, N1, N2, T::ZB, T::ZT, true><<<grid, T::ZT, x_smem<R, N1, N2>(), st>>>(reinterpret_cast<C *>(mid), h.px, a);
-      else if (h.nsc == 2)
-        k_xphys2<R, N1, N2, T::ZB, T::ZT, false, 2><<<grid, T::ZT, x_smem<R, N1, N2, 2>(), st>>>(
-            reinterpret_cast<C *>(mid), h.px, a);
-      else
-        k_xphys2<R, N1, N2, T::ZB, T::ZT><<<grid, T::ZT, x_smem<R, N1, N2>(), st>>>(reinterpret_cast<C *>(mid), h.px, a);
-      err = cudaGetLastError();
+        err = cudaGetLastError();
+        return;
+      }
+      with_variant(h.tune.x, [&]<int V>() {
+        constexpr int VV = tuned_variant<N1 * N2, V>();
+        using T = XVar<R, VV>;
+        dim3 grid((unsigned)((h.nz32 + T::ZB - 1) / T::ZB), (unsigned)h.ny);
+        if (h.nsc == 2)
+          k_xphys2<R, N1, N2, T::ZB, T::ZT, false, 2, VV><<<grid, T::ZT, x_smem<R, N1, N2, 2, T::ZB>(), st>>>(
+              reinterpret_cast<C *>(mid), h.px, a);
+        else
+          k_xphys2<R, N1, N2, T::ZB, T::ZT, false, 1, VV><<<grid, T::ZT, x_smem<R, N1, N2, 1, T::ZB>(), st>>>(
+              reinterpret_cast<C *>(mid), h.px, a);
+        err = cudaGetLastError();
+      });
     });
   };
   if (h.mixed) go.template operator()<float>();

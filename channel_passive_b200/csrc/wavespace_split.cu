@@ -75,7 +75,19 @@ struct SplitArgs {
   const double *dt_ptr;
   double *vf;        // the v operator's profile LU per mode: LBand, then UBand at vf + vf_l
   int64_t vf_l;
+  int groups;        // 32-mode groups per block of k_hvhg and k_helmholtz (Tuning::groups)
+  int ulayout;       // U factor layout of the per-role regions (Tuning::ulayout)
 };
+
+// A solver role's U factors for mode m: [offset][y][mode] (layout 0) or [y][offset][mode]
+// (layout 1, the BW offsets of one row next to each other); the first rows' extra entries follow
+// at BW * ns in both.
+template <int BW>
+__device__ __forceinline__ UBand<BW> role_uband(const SplitArgs &a, int role, int64_t m) {
+  double *base = a.ub + role * a.ub_role + m;
+  return a.ulayout == 0 ? make_uband<BW>(base, a.nmodes, a.ns, BW * a.ns)
+                        : make_uband<BW>(base, BW * a.nmodes, a.nmodes, BW * a.ns);
+}
 
 template <typename PT> __device__ __forceinline__ double2 ldp(const PT *p);
 template <> __device__ __forceinline__ double2 ldp<double2>(const double2 *p) { return *p; }
@@ -247,11 +259,14 @@ __device__ __forceinline__ void hvhg_role(const SplitArgs &a, const Tabs<BW> &tb
 // NS passive scalars: roles 0..3 as above, role 4 the second scalar's h_theta2.  Four resident
 // blocks of one scalar's 128 threads keep 128 registers a thread; with a fifth role three blocks
 // keep 136 (four would cap it at 96 and spill about 1 KB a thread).
+// One scalar: up to two 32-mode groups per block (Tuning::groups); the bound keeps 128 registers.
 template <int BW, typename PT, int NS>
-__global__ void __launch_bounds__(kLanes * (kRoles + NS - 1), NS == 1 ? 4 : 3) k_hvhg(SplitArgs a) {
+__global__ void __launch_bounds__(NS == 1 ? 2 * kLanes * kRoles : kLanes * (kRoles + 1), NS == 1 ? 2 : 3)
+k_hvhg(SplitArgs a) {
   if (a.dsc->err) return;
-  const int role = threadIdx.x / kLanes;
-  const int64_t m = (int64_t)blockIdx.x * kLanes + (threadIdx.x % kLanes);
+  constexpr int R = kRoles + NS - 1;
+  const int role = (threadIdx.x / kLanes) % R, grp = threadIdx.x / (kLanes * R);
+  const int64_t m = ((int64_t)blockIdx.x * a.groups + grp) * kLanes + (threadIdx.x % kLanes);
   if (m == 0 || m >= a.nmodes) return;
   const Tabs<BW> tb = tabs_at<BW>(a.tabs, a.ny);
   const bool s1 = a.substep == 1;
@@ -289,7 +304,7 @@ __device__ __forceinline__ void helmholtz_role(const SplitArgs &a, const Tabs<BW
   const double k2 = mode_k(a, m).k2;
   auto hl = [&](int i) { return DLine{a.hl + i * ns + m, nm}; };
   auto row = [&](const auto *base, int r) { return base + (r - 1) * (int)nm; };
-  const UBand<BW> ub = make_uband<BW>(a.ub + ROLE * a.ub_role + m, nm, ns);
+  const UBand<BW> ub = role_uband<BW>(a, ROLE, m);
   const DLine Zr{a.zl + ROLE * ns + m, nm};
 
   // RK right-hand side (solve_g.f90:84-123): rows 1 and n are the Dirichlet rows (zero)
@@ -353,7 +368,7 @@ __device__ __forceinline__ void helmholtz_role(const SplitArgs &a, const Tabs<BW
       [&](int r) {
         ring.get(r, 0, row(Zr.p, r));
 #pragma unroll
-        for (int e = 1; e <= BW; ++e) ring.get(r, e, ub.p + (e - 1) * (int)ns + (r - 1) * (int)nm);
+        for (int e = 1; e <= BW; ++e) ring.get(r, e, ub.p + (e - 1) * (int)ub.es + (r - 1) * (int)ub.s);
         if (r <= n - 2 * BW) {
           ring.get(r, BW + 1, row(hA, r + BW));
           if (ROLE == 1) ring.get(r, BW + 2, row(hB, r + BW));
@@ -378,7 +393,7 @@ __device__ __forceinline__ void helmholtz_phi_v(const SplitArgs &a, const Tabs<B
   const double k2 = mode_k(a, m).k2;
   auto hl = [&](int i) { return DLine{a.hl + i * ns + m, nm}; };
   auto row = [&](const auto *base, int r) { return base + (r - 1) * (int)nm; };
-  const UBand<BW> ub = make_uband<BW>(a.ub + 2 * a.ub_role + m, nm, ns);
+  const UBand<BW> ub = role_uband<BW>(a, 2, m);
   const DLine Zr{a.zl + 2 * ns + m, nm};
   const RLine Xz{a.xr + m, nm}, X1{a.xr + ns + m, nm}, X2{a.xr + 2 * ns + m, nm};
   const RLine X4{a.xr + 3 * ns + m, nm}, X5{a.xr + 4 * ns + m, nm};
@@ -444,7 +459,7 @@ __device__ __forceinline__ void helmholtz_phi_v(const SplitArgs &a, const Tabs<B
         ring.get(r, 0, row(Zr.p, r));
         ring.get(r, 1, row(Xz.p, r));
 #pragma unroll
-        for (int e = 1; e <= BW; ++e) ring.get(r, 1 + e, ub.p + (e - 1) * (int)ns + (r - 1) * (int)nm);
+        for (int e = 1; e <= BW; ++e) ring.get(r, 1 + e, ub.p + (e - 1) * (int)ub.es + (r - 1) * (int)ub.s);
         if (r <= n - 2 * BW) {
           ring.get(r, BW + 2, row(h0, r + BW));
           ring.get(r, BW + 3, row(h1, r + BW));
@@ -517,7 +532,7 @@ __device__ __forceinline__ void helmholtz_phi_v(const SplitArgs &a, const Tabs<B
         ring.get(r, 0, row(Zr.p, r));
         ring.get(r, 1, row(Xz.p, r));
 #pragma unroll
-        for (int e = 1; e <= BW; ++e) ring.get(r, 1 + e, vu.p + (e - 1) * (int)ns + (r - 1) * (int)nm);
+        for (int e = 1; e <= BW; ++e) ring.get(r, 1 + e, vu.p + (e - 1) * (int)vu.es + (r - 1) * (int)vu.s);
       });
   a.dv[2 * nm + m] = z2(dh1, dhn);
 }
@@ -554,12 +569,15 @@ constexpr size_t helm_smem() {
 
 // With a fourth role (a second scalar) three resident blocks keep the 168 registers of one
 // scalar's kernel; four would cap it at 128 and spill.
+// One scalar: up to two 32-mode groups per block (Tuning::groups); the bound keeps 168 registers.
 template <int BW, typename PT, int NS>
-__global__ void __launch_bounds__(kLanes * (kHelmRoles + NS - 1), NS == 1 ? 4 : 3) k_helmholtz(SplitArgs a) {
+__global__ void __launch_bounds__(NS == 1 ? 2 * kLanes * kHelmRoles : kLanes * (kHelmRoles + 1), NS == 1 ? 2 : 3)
+k_helmholtz(SplitArgs a) {
   extern __shared__ double2 helm_ring[];
   if (a.dsc->err) return;  // a failed dt update leaves the state untouched
-  const int role = threadIdx.x / kLanes;
-  const int64_t m = (int64_t)blockIdx.x * kLanes + (threadIdx.x % kLanes);
+  constexpr int R = kHelmRoles + NS - 1;
+  const int role = (threadIdx.x / kLanes) % R, grp = threadIdx.x / (kLanes * R);
+  const int64_t m = ((int64_t)blockIdx.x * a.groups + grp) * kLanes + (threadIdx.x % kLanes);
   if (m == 0 || m >= a.nmodes) return;
   const Tabs<BW> tb = tabs_at<BW>(a.tabs, a.ny);
   const Ring<kHelmUnits<BW>> ring{helm_ring + threadIdx.x, (int)blockDim.x};
@@ -575,7 +593,7 @@ __global__ void __launch_bounds__(kLanes * (kHelmRoles + NS - 1), NS == 1 ? 4 : 
 
 // ------------------------------------------------------------------------------------------
 // k_assemble: one thread per (y, mode); grid (modes / 256, ny).
-__global__ void __launch_bounds__(256) k_assemble(SplitArgs a) {
+__global__ void __launch_bounds__(512) k_assemble(SplitArgs a) {
   if (a.dsc->err) return;
   const int64_t nm = a.nmodes, ns = a.ns;
   const int r = blockIdx.y + 1;
@@ -798,6 +816,8 @@ cudaError_t split_bw(Handle &h, int part, int substep, const double *dt_ptr, cud
   a.dt_ptr = dtp;
   a.vf = h.vf;
   a.vf_l = vop_lband_doubles(h);
+  a.groups = h.nsc == 1 ? h.tune.groups : 1;
+  a.ulayout = h.tune.ulayout;
 
   MeanArgs ma;
   ma.ny = h.ny;
@@ -823,7 +843,8 @@ cudaError_t split_bw(Handle &h, int part, int substep, const double *dt_ptr, cud
   ma.dt_ptr = dtp;
 
   cudaError_t e;
-  const unsigned blocks = (unsigned)((h.nmodes + kLanes - 1) / kLanes);
+  const int G = a.groups;
+  const unsigned blocks = (unsigned)((h.nmodes + (int64_t)kLanes * G - 1) / ((int64_t)kLanes * G));
   if (part == 0) {
     // the mean lines touch only mode 0, which the split kernels skip: run them beside those
     if ((e = cudaEventRecord(h.ev_fork, st)) != cudaSuccess) return e;
@@ -836,8 +857,8 @@ cudaError_t split_bw(Handle &h, int part, int substep, const double *dt_ptr, cud
       if (h.mixed) k_hvhg<BW, float2, 2><<<blocks, kLanes * (kRoles + 1), 0, st>>>(a);
       else k_hvhg<BW, double2, 2><<<blocks, kLanes * (kRoles + 1), 0, st>>>(a);
     } else {
-      if (h.mixed) k_hvhg<BW, float2, 1><<<blocks, kLanes * kRoles, 0, st>>>(a);
-      else k_hvhg<BW, double2, 1><<<blocks, kLanes * kRoles, 0, st>>>(a);
+      if (h.mixed) k_hvhg<BW, float2, 1><<<blocks, kLanes * kRoles * G, 0, st>>>(a);
+      else k_hvhg<BW, double2, 1><<<blocks, kLanes * kRoles * G, 0, st>>>(a);
     }
     return cudaGetLastError();
   }
@@ -847,13 +868,14 @@ cudaError_t split_bw(Handle &h, int part, int substep, const double *dt_ptr, cud
       if (h.mixed) k_helmholtz<BW, float2, 2><<<blocks, nt, helm_smem<BW, 2>(), st>>>(a);
       else k_helmholtz<BW, double2, 2><<<blocks, nt, helm_smem<BW, 2>(), st>>>(a);
     } else {
-      if (h.mixed) k_helmholtz<BW, float2, 1><<<blocks, kLanes * kHelmRoles, helm_smem<BW>(), st>>>(a);
-      else k_helmholtz<BW, double2, 1><<<blocks, kLanes * kHelmRoles, helm_smem<BW>(), st>>>(a);
+      if (h.mixed) k_helmholtz<BW, float2, 1><<<blocks, kLanes * kHelmRoles * G, G * helm_smem<BW>(), st>>>(a);
+      else k_helmholtz<BW, double2, 1><<<blocks, kLanes * kHelmRoles * G, G * helm_smem<BW>(), st>>>(a);
     }
     return cudaGetLastError();
   }
-  const dim3 agrid((unsigned)((h.nmodes + 255) / 256), (unsigned)h.ny);
-  k_assemble<<<agrid, 256, 0, st>>>(a);
+  const int at = h.tune.asm_threads;
+  const dim3 agrid((unsigned)((h.nmodes + at - 1) / at), (unsigned)h.ny);
+  k_assemble<<<agrid, at, 0, st>>>(a);
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
   return cudaStreamWaitEvent(st, h.ev_join, 0);
 }
@@ -902,38 +924,38 @@ cudaError_t launch_vop_factor(Handle &h, cudaStream_t st) {
   cudaError_t e = cudaSuccess;
   switch (h.bw) {
     case 2:
-      e = ring_smem(k_helmholtz<2, float2, 1>, helm_smem<2>());
-      if (e == cudaSuccess) e = ring_smem(k_helmholtz<2, double2, 1>, helm_smem<2>());
+      e = ring_smem(k_helmholtz<2, float2, 1>, 2 * helm_smem<2>());
+      if (e == cudaSuccess) e = ring_smem(k_helmholtz<2, double2, 1>, 2 * helm_smem<2>());
       if (e == cudaSuccess) e = ring_smem(k_helmholtz<2, float2, 2>, helm_smem<2, 2>());
       if (e == cudaSuccess) e = ring_smem(k_helmholtz<2, double2, 2>, helm_smem<2, 2>());
       break;
     case 3:
-      e = ring_smem(k_helmholtz<3, float2, 1>, helm_smem<3>());
-      if (e == cudaSuccess) e = ring_smem(k_helmholtz<3, double2, 1>, helm_smem<3>());
+      e = ring_smem(k_helmholtz<3, float2, 1>, 2 * helm_smem<3>());
+      if (e == cudaSuccess) e = ring_smem(k_helmholtz<3, double2, 1>, 2 * helm_smem<3>());
       if (e == cudaSuccess) e = ring_smem(k_helmholtz<3, float2, 2>, helm_smem<3, 2>());
       if (e == cudaSuccess) e = ring_smem(k_helmholtz<3, double2, 2>, helm_smem<3, 2>());
       break;
     case 4:
-      e = ring_smem(k_helmholtz<4, float2, 1>, helm_smem<4>());
-      if (e == cudaSuccess) e = ring_smem(k_helmholtz<4, double2, 1>, helm_smem<4>());
+      e = ring_smem(k_helmholtz<4, float2, 1>, 2 * helm_smem<4>());
+      if (e == cudaSuccess) e = ring_smem(k_helmholtz<4, double2, 1>, 2 * helm_smem<4>());
       if (e == cudaSuccess) e = ring_smem(k_helmholtz<4, float2, 2>, helm_smem<4, 2>());
       if (e == cudaSuccess) e = ring_smem(k_helmholtz<4, double2, 2>, helm_smem<4, 2>());
       break;
     case 5:
-      e = ring_smem(k_helmholtz<5, float2, 1>, helm_smem<5>());
-      if (e == cudaSuccess) e = ring_smem(k_helmholtz<5, double2, 1>, helm_smem<5>());
+      e = ring_smem(k_helmholtz<5, float2, 1>, 2 * helm_smem<5>());
+      if (e == cudaSuccess) e = ring_smem(k_helmholtz<5, double2, 1>, 2 * helm_smem<5>());
       if (e == cudaSuccess) e = ring_smem(k_helmholtz<5, float2, 2>, helm_smem<5, 2>());
       if (e == cudaSuccess) e = ring_smem(k_helmholtz<5, double2, 2>, helm_smem<5, 2>());
       break;
     case 6:
-      e = ring_smem(k_helmholtz<6, float2, 1>, helm_smem<6>());
-      if (e == cudaSuccess) e = ring_smem(k_helmholtz<6, double2, 1>, helm_smem<6>());
+      e = ring_smem(k_helmholtz<6, float2, 1>, 2 * helm_smem<6>());
+      if (e == cudaSuccess) e = ring_smem(k_helmholtz<6, double2, 1>, 2 * helm_smem<6>());
       if (e == cudaSuccess) e = ring_smem(k_helmholtz<6, float2, 2>, helm_smem<6, 2>());
       if (e == cudaSuccess) e = ring_smem(k_helmholtz<6, double2, 2>, helm_smem<6, 2>());
       break;
     case 7:
-      e = ring_smem(k_helmholtz<7, float2, 1>, helm_smem<7>());
-      if (e == cudaSuccess) e = ring_smem(k_helmholtz<7, double2, 1>, helm_smem<7>());
+      e = ring_smem(k_helmholtz<7, float2, 1>, 2 * helm_smem<7>());
+      if (e == cudaSuccess) e = ring_smem(k_helmholtz<7, double2, 1>, 2 * helm_smem<7>());
       if (e == cudaSuccess) e = ring_smem(k_helmholtz<7, float2, 2>, helm_smem<7, 2>());
       if (e == cudaSuccess) e = ring_smem(k_helmholtz<7, double2, 2>, helm_smem<7, 2>());
       break;

@@ -21,7 +21,7 @@ from dataclasses import dataclass, field, fields
 import numpy as np
 
 from . import _lib
-from ._lib import KmmConfig, KmmError, KmmInfo, KmmScalars, check
+from ._lib import KmmConfig, KmmError, KmmInfo, KmmScalars, KmmTuning, check
 
 NFIELD = 10
 
@@ -56,6 +56,7 @@ class Config:
     n_scalar: int = 1
     pr2: float = 0.2
     bulk_t2: float = 1.0
+    autotune: int = 0
 
     def to_c(self) -> KmmConfig:
         c = KmmConfig()
@@ -255,6 +256,28 @@ class Channel:
         self.config.control_amp = float(amp)
         if amp != 0.0:
             self.config.control_yd = yd
+
+    # -- launch shapes ------------------------------------------------------------------
+    def autotune(self) -> dict:
+        """kmm_autotune: time the candidate launch shapes on this grid, keep the fastest."""
+        t = KmmTuning()
+        check(self._lib.kmm_autotune(self._h, C.byref(t)))
+        return t.as_dict()
+
+    @property
+    def tuning(self) -> dict:
+        t = KmmTuning()
+        check(self._lib.kmm_get_tuning(self._h, C.byref(t)))
+        return t.as_dict()
+
+    def set_tuning(self, **shapes):
+        """kmm_set_tuning: pin launch shapes (z_lines_per_block, x_rows_per_block, x_threads,
+        modes_per_block, u_layout, assemble_threads); unnamed ones keep their current values."""
+        t = KmmTuning()
+        check(self._lib.kmm_get_tuning(self._h, C.byref(t)))
+        for k, v in shapes.items():
+            setattr(t, k, int(v))
+        check(self._lib.kmm_set_tuning(self._h, C.byref(t)))
 
     # -- discrete adjoint of the control objective -------------------------------------
     def adjoint_forward(self, nsteps: int, w_tau: float = 1.0, w_q: float = 0.0) -> float:

@@ -65,7 +65,8 @@ typedef struct kmm_config {
   int32_t n_scalar;           /* passive scalars: 1 (the reference; 0 reads as 1) or 2 */
   double pr2;                 /* Prandtl number of the second scalar */
   double bulk_t2;             /* target bulk value of the second scalar */
-  int32_t reserved[2];
+  int32_t autotune;           /* 1: kmm_create runs kmm_autotune before it returns */
+  int32_t reserved;
 } kmm_config;
 
 /* Per-step diagnostics printed by main.f90:147-151. */
@@ -88,6 +89,24 @@ typedef struct kmm_info {
   int32_t fft_radix_x[8];     /* radix passes of the x transform (0-terminated) */
   int32_t fft_radix_z[8];
 } kmm_info;
+
+/* Launch shapes chosen by kmm_autotune (the hand-tuned defaults before it runs), and the
+ * measured device time (ms) of every candidate it tried. */
+typedef struct kmm_tuning {
+  int32_t z_lines_per_block;  /* z transforms (y_to_x, x_to_y): kx lines a block transforms */
+  int32_t x_rows_per_block;   /* x pass (dft_x_realspace): z rows a block takes */
+  int32_t x_threads;          /*   and its threads */
+  int32_t modes_per_block;    /* (kx, kz) systems a block of the hvhg and Helmholtz solvers takes */
+  int32_t u_layout;           /* U factor storage: 0 = [offset][y][mode], 1 = [y][offset][mode] */
+  int32_t assemble_threads;   /* threads per block of the C1/C2 assembly */
+  int32_t tuned;              /* 1 once kmm_autotune has run */
+  int32_t reserved;
+  double ms_z[3];             /* zinv + zfwd per z variant */
+  double ms_x[3];             /* x pass per x variant */
+  double ms_modes[2];         /* hvhg + Helmholtz at 32 and 64 modes per block */
+  double ms_layout[2];        /* hvhg + Helmholtz per U layout */
+  double ms_assemble[3];      /* assembly at 128, 256, 512 threads */
+} kmm_tuning;
 
 typedef struct kmm_handle kmm_handle;
 
@@ -193,6 +212,19 @@ const char *kmm_stat_spec_name(int i);
 
 /* The cudaStream_t (as void*) every launch of the handle goes to, for event timing. */
 int kmm_get_stream(const kmm_handle *h, void **stream);
+
+/* Autotuner (no counterpart in the reference): times the candidate launch shapes of the z
+ * transforms, the x pass, the per-mode solvers (systems per block, U factor layout) and the
+ * assembly on the handle's own grid and buffers, keeps the fastest of each, and reports them
+ * (out may be NULL).  The state is left unchanged; the next kmm_step captures its graph with
+ * the chosen shapes.  kmm_get_tuning reports the shapes in use. */
+int kmm_autotune(kmm_handle *h, kmm_tuning *out);
+int kmm_get_tuning(const kmm_handle *h, kmm_tuning *out);
+/* Pins the launch shapes of t (its shape fields; the timings are ignored), for instance a tuning
+ * recorded from an earlier kmm_autotune on the same grid.  Every shape must be one of the grid's
+ * candidates (KMM_ERR_ARG otherwise).  Results do not depend on the shapes: every candidate runs
+ * the same arithmetic per line and per mode. */
+int kmm_set_tuning(kmm_handle *h, const kmm_tuning *t);
 
 /* Kernel ids reported by kmm_profile_step. */
 #define KMM_NKERNEL 8

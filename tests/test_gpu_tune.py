@@ -1,0 +1,73 @@
+"""The autotuner (kmm_autotune / kmm_set_tuning) on the GPU: every candidate launch shape gives the
+default's results bit for bit (the shapes change how lines and modes are spread over blocks, not
+their arithmetic), tuning leaves the state unchanged, and its choices are reported."""
+import numpy as np
+import pytest
+
+from channel_passive_b200 import Channel, KmmError
+from channel_passive_b200 import _lib
+from oracle import kmm as okmm
+from tests.helpers import STATE_SLOTS, make_pair, seeded_state
+
+pytestmark = pytest.mark.gpu
+
+
+def _run(cfg, U, tuning=None, nsteps=2):
+    with Channel(cfg) as ch:
+        if tuning:
+            ch.set_tuning(**tuning)
+        ch.set_initial_data_uvw(U, 0.01)
+        ch.step(nsteps)
+        return ch.download_state(10)[0]
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+def test_every_candidate_shape_is_bit_identical(precision):
+    cfg, p = make_pair(nx=64, ny=65, nz=64, control_amp=-1.0, precision=precision)
+    U = seeded_state(cfg, okmm.make_operators(p).y)
+    ref = _run(cfg, U)
+    with Channel(cfg) as ch:
+        rep = ch.autotune()
+    assert rep["tuned"] == 1
+    # the candidates: variant shapes reported by the tuner's timings are tried one knob at a time
+    z_lines = {16: (8, 32), 8: (4, 16)}[8 if precision == 0 else 16]
+    x_shapes = [(1, 128), (4, 256)] if precision == 1 else [(1, 128), (2, 128)]
+    cases = [dict(z_lines_per_block=z) for z in z_lines]
+    cases += [dict(x_rows_per_block=r, x_threads=t) for r, t in x_shapes]
+    cases += [dict(modes_per_block=64), dict(u_layout=1), dict(assemble_threads=128), dict(assemble_threads=512)]
+    for case in cases:
+        got = _run(cfg, U, case)
+        for f in STATE_SLOTS:
+            assert np.array_equal(got[f], ref[f]), (case, f)
+
+
+def test_autotune_keeps_the_state_and_reports_its_choice():
+    cfg, p = make_pair(nx=64, ny=65, nz=64, control_amp=-1.0, precision=1)
+    U = seeded_state(cfg, okmm.make_operators(p).y)
+    ref = _run(cfg, U, nsteps=3)
+    with Channel(cfg) as ch:
+        ch.set_initial_data_uvw(U, 0.01)
+        ch.step(1)
+        before, rk_before = ch.download_state(10)
+        rep = ch.autotune()
+        after, rk_after = ch.download_state(10)
+        for f in STATE_SLOTS:
+            assert np.array_equal(after[f], before[f])
+        assert np.array_equal(rk_after, rk_before)
+        ch.step(2)
+        got, _ = ch.download_state(10)
+        t = ch.tuning
+    for f in STATE_SLOTS:
+        assert np.array_equal(got[f], ref[f]), f
+    assert t["tuned"] == 1 and t["modes_per_block"] in (32, 64) and t["assemble_threads"] in (128, 256, 512)
+    assert all(x > 0 for x in rep["ms_z"] + rep["ms_x"] + rep["ms_modes"] + rep["ms_assemble"])
+    with pytest.raises(KmmError) as e:
+        with Channel(cfg) as ch:
+            ch.set_tuning(z_lines_per_block=7)
+    assert e.value.code == _lib.KMM_ERR_ARG
+
+
+def test_create_with_autotune_flag():
+    cfg, p = make_pair(nx=64, ny=65, nz=64, precision=1, autotune=1)
+    with Channel(cfg) as ch:
+        assert ch.tuning["tuned"] == 1
