@@ -87,6 +87,8 @@ struct Tuning {
   int ulayout = 0;        // U factor storage: 0 = [offset][y][mode], 1 = [y][offset][mode]
   int asm_threads = 256;  // threads per block of the assembly kernel
   bool tuned = false;
+  // device ms of every candidate of the last autotune (kmm_tuning's ms_* fields)
+  double ms_z[3] = {}, ms_x[3] = {}, ms_modes[2] = {}, ms_layout[2] = {}, ms_assemble[3] = {};
 };
 
 struct Handle {

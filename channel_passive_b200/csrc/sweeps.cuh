@@ -102,28 +102,29 @@ struct RLine {
 template <int BW>
 struct UBand {
   double *p;   // [BW][ny][s]
-  double *px;  // [BW][BW][s]
+  double *px;  // [BW][BW][xs]
   int64_t s;   // stride between rows (number of modes)
   int64_t es;  // stride between offsets (ny * number of modes)
+  int64_t xs;  // stride between the extra entries of the first rows (number of modes)
   __device__ __forceinline__ double get(int r, int e) const {
     if (e <= BW) return p[(e - 1) * (int)es + (r - 1) * (int)s];
-    return r <= BW ? px[((r - 1) * BW + e - BW - 1) * (int)s] : 0.0;
+    return r <= BW ? px[((r - 1) * BW + e - BW - 1) * (int)xs] : 0.0;
   }
   __device__ __forceinline__ void set(int r, int e, double v) const {
     if (e <= BW) p[(e - 1) * (int)es + (r - 1) * (int)s] = v;
-    else if (r <= BW) px[((r - 1) * BW + e - BW - 1) * (int)s] = v;
+    else if (r <= BW) px[((r - 1) * BW + e - BW - 1) * (int)xs] = v;
   }
   __device__ __forceinline__ const double *row_ptr(int r) const { return p + (r - 1) * (int)s; }
 };
 template <int BW>
 __device__ __forceinline__ UBand<BW> make_uband(double *base, int64_t s, int64_t es) {
-  return UBand<BW>{base, base + BW * es, s, es};
+  return UBand<BW>{base, base + BW * es, s, es, s};
 }
-// The same with the first rows' extra entries at base + px_off, for layouts whose row and offset
-// strides are not (modes, ny * modes).
+// The same for layouts whose row and offset strides are not (modes, ny * modes): the first rows'
+// extra entries sit at base + px_off, xs apart ([BW][BW][mode] for xs = number of modes).
 template <int BW>
-__device__ __forceinline__ UBand<BW> make_uband(double *base, int64_t s, int64_t es, int64_t px_off) {
-  return UBand<BW>{base, base + px_off, s, es};
+__device__ __forceinline__ UBand<BW> make_uband(double *base, int64_t s, int64_t es, int64_t px_off, int64_t xs) {
+  return UBand<BW>{base, base + px_off, s, es, xs};
 }
 
 // Per-mode L factor of a profile LU kept for later forward sweeps, the UBand idea for L:

@@ -156,21 +156,17 @@ int autotune(Handle &h, kmm_tuning *out) {
   TUNE_CUDA(cudaStreamSynchronize(st));
   TUNE_CUDA(cudaStreamSynchronize(h.side));
   h.tune.tuned = true;
+  std::memcpy(h.tune.ms_z, rep.ms_z, sizeof(rep.ms_z));
+  std::memcpy(h.tune.ms_x, rep.ms_x, sizeof(rep.ms_x));
+  std::memcpy(h.tune.ms_modes, rep.ms_modes, sizeof(rep.ms_modes));
+  std::memcpy(h.tune.ms_layout, rep.ms_layout, sizeof(rep.ms_layout));
+  std::memcpy(h.tune.ms_assemble, rep.ms_assemble, sizeof(rep.ms_assemble));
   // the step graph holds the old launch shapes: capture it again at the next step
   if (h.gexec) cudaGraphExecDestroy(h.gexec);
   if (h.graph) cudaGraphDestroy(h.graph);
   h.gexec = nullptr;
   h.graph = nullptr;
-  if (out) {
-    kmm_tuning cur;
-    kmm_get_tuning(reinterpret_cast<const kmm_handle *>(&h), &cur);
-    std::memcpy(out, &cur, offsetof(kmm_tuning, ms_z));
-    std::memcpy(out->ms_z, rep.ms_z, sizeof(rep.ms_z));
-    std::memcpy(out->ms_x, rep.ms_x, sizeof(rep.ms_x));
-    std::memcpy(out->ms_modes, rep.ms_modes, sizeof(rep.ms_modes));
-    std::memcpy(out->ms_layout, rep.ms_layout, sizeof(rep.ms_layout));
-    std::memcpy(out->ms_assemble, rep.ms_assemble, sizeof(rep.ms_assemble));
-  }
+  if (out) kmm_get_tuning(reinterpret_cast<const kmm_handle *>(&h), out);
   return KMM_OK;
 }
 
@@ -189,6 +185,11 @@ int kmm_get_tuning(const kmm_handle *hh, kmm_tuning *out) {
   out->u_layout = h.tune.ulayout;
   out->assemble_threads = h.tune.asm_threads;
   out->tuned = h.tune.tuned ? 1 : 0;
+  std::memcpy(out->ms_z, h.tune.ms_z, sizeof(out->ms_z));
+  std::memcpy(out->ms_x, h.tune.ms_x, sizeof(out->ms_x));
+  std::memcpy(out->ms_modes, h.tune.ms_modes, sizeof(out->ms_modes));
+  std::memcpy(out->ms_layout, h.tune.ms_layout, sizeof(out->ms_layout));
+  std::memcpy(out->ms_assemble, h.tune.ms_assemble, sizeof(out->ms_assemble));
   return KMM_OK;
 }
 

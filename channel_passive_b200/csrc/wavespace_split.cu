@@ -85,8 +85,8 @@ struct SplitArgs {
 template <int BW>
 __device__ __forceinline__ UBand<BW> role_uband(const SplitArgs &a, int role, int64_t m) {
   double *base = a.ub + role * a.ub_role + m;
-  return a.ulayout == 0 ? make_uband<BW>(base, a.nmodes, a.ns, BW * a.ns)
-                        : make_uband<BW>(base, BW * a.nmodes, a.nmodes, BW * a.ns);
+  return a.ulayout == 0 ? make_uband<BW>(base, a.nmodes, a.ns)
+                        : make_uband<BW>(base, BW * a.nmodes, a.nmodes, BW * a.ns, a.nmodes);
 }
 
 template <typename PT> __device__ __forceinline__ double2 ldp(const PT *p);

@@ -217,7 +217,8 @@ int kmm_get_stream(const kmm_handle *h, void **stream);
  * transforms, the x pass, the per-mode solvers (systems per block, U factor layout) and the
  * assembly on the handle's own grid and buffers, keeps the fastest of each, and reports them
  * (out may be NULL).  The state is left unchanged; the next kmm_step captures its graph with
- * the chosen shapes.  kmm_get_tuning reports the shapes in use. */
+ * the chosen shapes.  kmm_get_tuning reports the shapes in use and the timings of the last
+ * kmm_autotune (zero before one ran; a handle created with cfg.autotune = 1 has them). */
 int kmm_autotune(kmm_handle *h, kmm_tuning *out);
 int kmm_get_tuning(const kmm_handle *h, kmm_tuning *out);
 /* Pins the launch shapes of t (its shape fields; the timings are ignored), for instance a tuning

@@ -70,4 +70,7 @@ def test_autotune_keeps_the_state_and_reports_its_choice():
 def test_create_with_autotune_flag():
     cfg, p = make_pair(nx=64, ny=65, nz=64, precision=1, autotune=1)
     with Channel(cfg) as ch:
-        assert ch.tuning["tuned"] == 1
+        t = ch.tuning
+    # the timings of the tuning run at creation stay with the handle
+    assert t["tuned"] == 1 and all(x > 0 for x in t["ms_z"] + t["ms_x"] + t["ms_modes"] + t["ms_assemble"])
+    assert t["ms_layout"][t["u_layout"]] == min(t["ms_layout"])
