@@ -557,6 +557,12 @@ int kmm_create(const kmm_config *cfg, kmm_handle **out) {
       return fail(KMM_ERR_CUDA);
     }
   }
+  // untuned launch shapes: 64-mode solver blocks with their operator tables in shared memory
+  // where two such blocks fit on an SM, else 32-mode blocks reading the tables through L1
+  if (solver_tables_default(*h)) {
+    h->tune.groups = 2;
+    h->tune.stab = 1;
+  }
   if (cfg->autotune && (rc = autotune(*h, nullptr))) return fail(rc);
   *out = reinterpret_cast<kmm_handle *>(h);
   return KMM_OK;

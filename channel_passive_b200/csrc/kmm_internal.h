@@ -86,9 +86,10 @@ struct Tuning {
   int groups = 1;         // 32-mode groups per block of the hvhg and Helmholtz kernels (1 or 2)
   int ulayout = 0;        // U factor storage: 0 = [offset][y][mode], 1 = [y][offset][mode]
   int asm_threads = 256;  // threads per block of the assembly kernel
+  int stab = 0;           // 1: the hvhg and Helmholtz kernels read the operator tables from shared memory
   bool tuned = false;
   // device ms of every candidate of the last autotune (kmm_tuning's ms_* fields)
-  double ms_z[3] = {}, ms_x[3] = {}, ms_modes[2] = {}, ms_layout[2] = {}, ms_assemble[3] = {};
+  double ms_z[3] = {}, ms_x[3] = {}, ms_modes[2] = {}, ms_layout[2] = {}, ms_assemble[3] = {}, ms_tables[2] = {};
 };
 
 struct Handle {
@@ -244,6 +245,12 @@ int64_t vop_factor_doubles(const Handle &h);
 cudaError_t launch_vop_factor(Handle &h, cudaStream_t st);
 // Doubles of U factor storage per solver role.
 int64_t split_ub_role(const Handle &h);
+// Operator tables in shared memory for the hvhg and Helmholtz kernels: their bytes per block,
+// whether a block of `groups` 32-mode groups can hold them beside its staging ring, and whether
+// a handle starts with them (two resident 64-mode blocks per SM).
+size_t solver_tables_bytes(const Handle &h);
+bool solver_tables_fit(const Handle &h, int groups);
+bool solver_tables_default(const Handle &h);
 
 // One time_march substep enqueued kernel by kernel on st (api.cu), the device scalars read back,
 // and the step graph captured if it is not yet.

@@ -180,6 +180,19 @@ __device__ __forceinline__ Tabs<BW> tabs_at(const double *base, int ny) {
   return t;
 }
 
+// The same from T1 on (T1, T2, L0, U0 contiguous as above); T0 is left unset.
+template <int BW>
+__device__ __forceinline__ Tabs<BW> tabs_from_t1(const double *t1, int ny) {
+  const int64_t tw = (int64_t)ny * (4 * BW + 1);
+  Tabs<BW> t;
+  t.t0 = nullptr;
+  t.t1 = t1;
+  t.t2 = t1 + tw;
+  t.l0 = t1 + 2 * tw;
+  t.u0 = t.l0 + (int64_t)ny * (2 * BW + 1);
+  return t;
+}
+
 // (M x)_q from the backward window w[j] = x_{r+j}: sum_j M(q, r+j-q) w[j].
 template <int BW, typename WT>
 __device__ __forceinline__ double2 mvc(const double *t, int q, int r, const WT &w) {

@@ -6,7 +6,9 @@
 //   z transforms   kx lines per block (transforms2.cu ZVar; zinv + zfwd timed together),
 //   x pass         z rows per block and threads (XVar),
 //   per-mode solve 32 or 64 (kx, kz) systems per block of k_hvhg and k_helmholtz (one scalar),
-//                  and the U factor storage layout of the Helmholtz roles,
+//                  each with the operator tables read through L1 or copied to shared memory
+//                  (where a block can hold them), then the U factor storage layout of the
+//                  Helmholtz roles,
 //   assembly       threads per block.
 // Each candidate runs once to warm up, then kReps times between CUDA events on the handle's
 // stream; the minimum of the means wins.  The solver runs mutate the state, so the state, the
@@ -129,13 +131,33 @@ int autotune(Handle &h, kmm_tuning *out) {
     return e;
   };
   const int ng = h.nsc == 1 ? 2 : 1;
-  for (int g = 0; g < ng; ++g) {
-    h.tune.groups = g + 1;
-    h.tune.ulayout = 0;
-    if ((rc = measure(restore, solve, &rep.ms_modes[g]))) return rc;
-  }
-  h.tune.groups = best(rep.ms_modes, ng) + 1;
-  rep.ms_layout[0] = rep.ms_modes[h.tune.groups - 1];
+  double ms_gs[2][2];  // [groups - 1][tables in shared memory]
+  int bg = 1, bs = 0;
+  for (int g = 0; g < ng; ++g)
+    for (int sh = 0; sh < 2; ++sh) {
+      ms_gs[g][sh] = 0.0;
+      if (sh && !solver_tables_fit(h, g + 1)) continue;
+      h.tune.groups = g + 1;
+      h.tune.stab = sh;
+      h.tune.ulayout = 0;
+      if ((rc = measure(restore, solve, &ms_gs[g][sh]))) return rc;
+      if (ms_gs[g][sh] < ms_gs[bg - 1][bs] || (g == 0 && sh == 0)) {
+        bg = g + 1;
+        bs = sh;
+      }
+    }
+  // report the fastest measured time of each knob value (0: not measured)
+  auto keep_min = [](double &acc, double v) {
+    if (v > 0.0 && (acc == 0.0 || v < acc)) acc = v;
+  };
+  for (int g = 0; g < ng; ++g)
+    for (int sh = 0; sh < 2; ++sh) {
+      keep_min(rep.ms_modes[g], ms_gs[g][sh]);
+      keep_min(rep.ms_tables[sh], ms_gs[g][sh]);
+    }
+  h.tune.groups = bg;
+  h.tune.stab = bs;
+  rep.ms_layout[0] = ms_gs[bg - 1][bs];
   h.tune.ulayout = 1;
   if ((rc = measure(restore, solve, &rep.ms_layout[1]))) return rc;
   h.tune.ulayout = best(rep.ms_layout, 2);
@@ -161,6 +183,7 @@ int autotune(Handle &h, kmm_tuning *out) {
   std::memcpy(h.tune.ms_modes, rep.ms_modes, sizeof(rep.ms_modes));
   std::memcpy(h.tune.ms_layout, rep.ms_layout, sizeof(rep.ms_layout));
   std::memcpy(h.tune.ms_assemble, rep.ms_assemble, sizeof(rep.ms_assemble));
+  std::memcpy(h.tune.ms_tables, rep.ms_tables, sizeof(rep.ms_tables));
   // the step graph holds the old launch shapes: capture it again at the next step
   if (h.gexec) cudaGraphExecDestroy(h.gexec);
   if (h.graph) cudaGraphDestroy(h.graph);
@@ -185,11 +208,13 @@ int kmm_get_tuning(const kmm_handle *hh, kmm_tuning *out) {
   out->u_layout = h.tune.ulayout;
   out->assemble_threads = h.tune.asm_threads;
   out->tuned = h.tune.tuned ? 1 : 0;
+  out->tables_shared = h.tune.stab;
   std::memcpy(out->ms_z, h.tune.ms_z, sizeof(out->ms_z));
   std::memcpy(out->ms_x, h.tune.ms_x, sizeof(out->ms_x));
   std::memcpy(out->ms_modes, h.tune.ms_modes, sizeof(out->ms_modes));
   std::memcpy(out->ms_layout, h.tune.ms_layout, sizeof(out->ms_layout));
   std::memcpy(out->ms_assemble, h.tune.ms_assemble, sizeof(out->ms_assemble));
+  std::memcpy(out->ms_tables, h.tune.ms_tables, sizeof(out->ms_tables));
   return KMM_OK;
 }
 
@@ -207,7 +232,9 @@ int kmm_set_tuning(kmm_handle *hh, const kmm_tuning *t) {
   }
   const int g = t->modes_per_block == 32 ? 1 : t->modes_per_block == 64 ? 2 : 0;
   const bool asm_ok = t->assemble_threads == 128 || t->assemble_threads == 256 || t->assemble_threads == 512;
-  if (zv < 0 || xv < 0 || g == 0 || (g == 2 && h.nsc != 1) || (t->u_layout != 0 && t->u_layout != 1) || !asm_ok) {
+  const bool tab_ok = t->tables_shared == 0 || (t->tables_shared == 1 && g != 0 && solver_tables_fit(h, g));
+  if (zv < 0 || xv < 0 || g == 0 || (g == 2 && h.nsc != 1) || (t->u_layout != 0 && t->u_layout != 1) || !asm_ok ||
+      !tab_ok) {
     set_error("kmm_set_tuning: a requested shape is not among this grid's candidates (see kmm_autotune)");
     return KMM_ERR_ARG;
   }
@@ -216,6 +243,7 @@ int kmm_set_tuning(kmm_handle *hh, const kmm_tuning *t) {
   next.groups = g;
   next.ulayout = t->u_layout;
   next.asm_threads = t->assemble_threads;
+  next.stab = t->tables_shared;
   DeviceGuard dg(h.cfg.device);
   cudaStreamSynchronize(h.stream);
   h.tune = next;

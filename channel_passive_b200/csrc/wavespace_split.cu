@@ -77,7 +77,21 @@ struct SplitArgs {
   int64_t vf_l;
   int groups;        // 32-mode groups per block of k_hvhg and k_helmholtz (Tuning::groups)
   int ulayout;       // U factor layout of the per-role regions (Tuning::ulayout)
+  int stab;          // 1: k_hvhg and k_helmholtz copy the operator tables they read to shared memory
 };
+
+// Operator tables in shared memory (SplitArgs::stab).  Every lane of a warp reads the same table
+// entry at the same row (the modes of a warp sweep in lockstep), yet beside the streamed lines
+// L1 kept only about a third of those reads.  The block copies the 3 tables a kernel reads,
+// 3 * ny * (4BW+1) doubles starting at table `first` of T0, T1, T2, L0 + U0, before any sweep.
+template <int BW>
+__device__ __forceinline__ const double *tabs_to_shared(const SplitArgs &a, int first, double *smem) {
+  const int tw = a.ny * (4 * BW + 1);
+  const double *src = a.tabs + first * tw;
+  for (int i = threadIdx.x; i < 3 * tw; i += blockDim.x) smem[i] = src[i];
+  __syncthreads();
+  return smem;
+}
 
 // A solver role's U factors for mode m: [offset][y][mode] (layout 0) or [y][offset][mode]
 // (layout 1, the BW offsets of one row next to each other); the first rows' extra entries follow
@@ -263,12 +277,16 @@ __device__ __forceinline__ void hvhg_role(const SplitArgs &a, const Tabs<BW> &tb
 template <int BW, typename PT, int NS>
 __global__ void __launch_bounds__(NS == 1 ? 2 * kLanes * kRoles : kLanes * (kRoles + 1), NS == 1 ? 2 : 3)
 k_hvhg(SplitArgs a) {
-  if (a.dsc->err) return;
+  extern __shared__ double hvhg_tabs[];
+  if (a.dsc->err) return;  // uniform over the block, like a.stab
   constexpr int R = kRoles + NS - 1;
   const int role = (threadIdx.x / kLanes) % R, grp = threadIdx.x / (kLanes * R);
   const int64_t m = ((int64_t)blockIdx.x * a.groups + grp) * kLanes + (threadIdx.x % kLanes);
+  // T1, T2 and the D0 factor (L0, U0) are what the hvhg roles read: from T1 on
+  const double *t1 = a.tabs + a.ny * (4 * BW + 1);
+  if (a.stab) t1 = tabs_to_shared<BW>(a, 1, hvhg_tabs);
   if (m == 0 || m >= a.nmodes) return;
-  const Tabs<BW> tb = tabs_at<BW>(a.tabs, a.ny);
+  const Tabs<BW> tb = tabs_from_t1<BW>(t1, a.ny);
   const bool s1 = a.substep == 1;
   switch (role) {
     case 0: s1 ? hvhg_role<BW, PT, 0, 2>(a, tb, m) : hvhg_role<BW, PT, 0, 1>(a, tb, m); break;
@@ -574,12 +592,16 @@ template <int BW, typename PT, int NS>
 __global__ void __launch_bounds__(NS == 1 ? 2 * kLanes * kHelmRoles : kLanes * (kHelmRoles + 1), NS == 1 ? 2 : 3)
 k_helmholtz(SplitArgs a) {
   extern __shared__ double2 helm_ring[];
-  if (a.dsc->err) return;  // a failed dt update leaves the state untouched
+  if (a.dsc->err) return;  // a failed dt update leaves the state untouched (uniform over the block)
   constexpr int R = kHelmRoles + NS - 1;
   const int role = (threadIdx.x / kLanes) % R, grp = threadIdx.x / (kLanes * R);
   const int64_t m = ((int64_t)blockIdx.x * a.groups + grp) * kLanes + (threadIdx.x % kLanes);
+  // T0, T1, T2 (after the staging ring when in shared memory)
+  const double *t0 = a.tabs;
+  if (a.stab)
+    t0 = tabs_to_shared<BW>(a, 0, reinterpret_cast<double *>(helm_ring + kStageSlots * kHelmUnits<BW> * blockDim.x));
   if (m == 0 || m >= a.nmodes) return;
-  const Tabs<BW> tb = tabs_at<BW>(a.tabs, a.ny);
+  const Tabs<BW> tb = tabs_at<BW>(t0, a.ny);  // (its L0 and U0 are not read here)
   const Ring<kHelmUnits<BW>> ring{helm_ring + threadIdx.x, (int)blockDim.x};
   switch (role) {
     case 0: helmholtz_role<BW, 0, PT>(a, tb, m, ring); break;
@@ -818,6 +840,7 @@ cudaError_t split_bw(Handle &h, int part, int substep, const double *dt_ptr, cud
   a.vf_l = vop_lband_doubles(h);
   a.groups = h.nsc == 1 ? h.tune.groups : 1;
   a.ulayout = h.tune.ulayout;
+  a.stab = h.tune.stab;
 
   MeanArgs ma;
   ma.ny = h.ny;
@@ -845,6 +868,7 @@ cudaError_t split_bw(Handle &h, int part, int substep, const double *dt_ptr, cud
   cudaError_t e;
   const int G = a.groups;
   const unsigned blocks = (unsigned)((h.nmodes + (int64_t)kLanes * G - 1) / ((int64_t)kLanes * G));
+  const size_t tsm = a.stab ? solver_tables_bytes(h) : 0;
   if (part == 0) {
     // the mean lines touch only mode 0, which the split kernels skip: run them beside those
     if ((e = cudaEventRecord(h.ev_fork, st)) != cudaSuccess) return e;
@@ -854,22 +878,23 @@ cudaError_t split_bw(Handle &h, int part, int substep, const double *dt_ptr, cud
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
     if ((e = cudaEventRecord(h.ev_join, h.side)) != cudaSuccess) return e;
     if (h.nsc == 2) {
-      if (h.mixed) k_hvhg<BW, float2, 2><<<blocks, kLanes * (kRoles + 1), 0, st>>>(a);
-      else k_hvhg<BW, double2, 2><<<blocks, kLanes * (kRoles + 1), 0, st>>>(a);
+      if (h.mixed) k_hvhg<BW, float2, 2><<<blocks, kLanes * (kRoles + 1), tsm, st>>>(a);
+      else k_hvhg<BW, double2, 2><<<blocks, kLanes * (kRoles + 1), tsm, st>>>(a);
     } else {
-      if (h.mixed) k_hvhg<BW, float2, 1><<<blocks, kLanes * kRoles * G, 0, st>>>(a);
-      else k_hvhg<BW, double2, 1><<<blocks, kLanes * kRoles * G, 0, st>>>(a);
+      if (h.mixed) k_hvhg<BW, float2, 1><<<blocks, kLanes * kRoles * G, tsm, st>>>(a);
+      else k_hvhg<BW, double2, 1><<<blocks, kLanes * kRoles * G, tsm, st>>>(a);
     }
     return cudaGetLastError();
   }
   if (part == 1) {
     if (h.nsc == 2) {
       constexpr int nt = kLanes * (kHelmRoles + 1);
-      if (h.mixed) k_helmholtz<BW, float2, 2><<<blocks, nt, helm_smem<BW, 2>(), st>>>(a);
-      else k_helmholtz<BW, double2, 2><<<blocks, nt, helm_smem<BW, 2>(), st>>>(a);
+      if (h.mixed) k_helmholtz<BW, float2, 2><<<blocks, nt, helm_smem<BW, 2>() + tsm, st>>>(a);
+      else k_helmholtz<BW, double2, 2><<<blocks, nt, helm_smem<BW, 2>() + tsm, st>>>(a);
     } else {
-      if (h.mixed) k_helmholtz<BW, float2, 1><<<blocks, kLanes * kHelmRoles * G, G * helm_smem<BW>(), st>>>(a);
-      else k_helmholtz<BW, double2, 1><<<blocks, kLanes * kHelmRoles * G, G * helm_smem<BW>(), st>>>(a);
+      const size_t sm = G * helm_smem<BW>() + tsm;
+      if (h.mixed) k_helmholtz<BW, float2, 1><<<blocks, kLanes * kHelmRoles * G, sm, st>>>(a);
+      else k_helmholtz<BW, double2, 1><<<blocks, kLanes * kHelmRoles * G, sm, st>>>(a);
     }
     return cudaGetLastError();
   }
@@ -904,6 +929,65 @@ int64_t vop_lband_doubles(const Handle &h) {
 
 int64_t vop_factor_doubles(const Handle &h) { return vop_lband_doubles(h) + split_ub_role(h); }
 
+namespace {
+
+template <int BW>
+cudaError_t set_smem_limit_bw(int bytes) {
+  auto lim = [bytes](auto kern) { return cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes); };
+  cudaError_t e = lim(k_helmholtz<BW, float2, 1>);
+  if (e == cudaSuccess) e = lim(k_helmholtz<BW, double2, 1>);
+  if (e == cudaSuccess) e = lim(k_helmholtz<BW, float2, 2>);
+  if (e == cudaSuccess) e = lim(k_helmholtz<BW, double2, 2>);
+  if (e == cudaSuccess) e = lim(k_hvhg<BW, float2, 1>);
+  if (e == cudaSuccess) e = lim(k_hvhg<BW, double2, 1>);
+  if (e == cudaSuccess) e = lim(k_hvhg<BW, float2, 2>);
+  if (e == cudaSuccess) e = lim(k_hvhg<BW, double2, 2>);
+  return e;
+}
+
+cudaError_t set_solver_smem_limits(const Handle &h) {
+  int dev = 0, optin = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e == cudaSuccess) e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+  if (e != cudaSuccess) return e;
+  switch (h.bw) {
+    case 2: return set_smem_limit_bw<2>(optin);
+    case 3: return set_smem_limit_bw<3>(optin);
+    case 4: return set_smem_limit_bw<4>(optin);
+    case 5: return set_smem_limit_bw<5>(optin);
+    case 6: return set_smem_limit_bw<6>(optin);
+    case 7: return set_smem_limit_bw<7>(optin);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+size_t helm_ring_bytes(const Handle &h, int groups) {
+  const size_t per = sizeof(double2) * (size_t)kStageSlots * (5 + h.bw) * kLanes;  // kHelmUnits<BW>
+  return per * (h.nsc == 2 ? kHelmRoles + 1 : (size_t)kHelmRoles * groups);
+}
+
+}  // namespace
+
+size_t solver_tables_bytes(const Handle &h) { return sizeof(double) * 3 * (size_t)h.ny * (4 * h.bw + 1); }
+
+bool solver_tables_fit(const Handle &h, int groups) {
+  int dev = 0, optin = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess ||
+      cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) != cudaSuccess)
+    return false;
+  return helm_ring_bytes(h, groups) + solver_tables_bytes(h) <= (size_t)optin;
+}
+
+bool solver_tables_default(const Handle &h) {
+  int dev = 0, per_sm = 0;
+  if (h.nsc != 1 || cudaGetDevice(&dev) != cudaSuccess ||
+      cudaDeviceGetAttribute(&per_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev) != cudaSuccess)
+    return false;
+  // two resident blocks of 64 modes (the one wave of 12 warps per SM the kernel has without the
+  // tables), with the 1 KB the runtime reserves per block
+  return 2 * (helm_ring_bytes(h, 2) + solver_tables_bytes(h) + 1024) <= (size_t)per_sm;
+}
+
 cudaError_t launch_vop_factor(Handle &h, cudaStream_t st) {
   SplitArgs a{};
   a.ny = h.ny;
@@ -917,50 +1001,10 @@ cudaError_t launch_vop_factor(Handle &h, cudaStream_t st) {
   a.vf = h.vf;
   a.vf_l = vop_lband_doubles(h);
   const unsigned blocks = (unsigned)((h.nmodes + 127) / 128);
-  // the Helmholtz kernel's staging ring may exceed the default 48 KB of dynamic shared memory
-  auto ring_smem = [](auto kern, size_t bytes) {
-    return cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
-  };
-  cudaError_t e = cudaSuccess;
-  switch (h.bw) {
-    case 2:
-      e = ring_smem(k_helmholtz<2, float2, 1>, 2 * helm_smem<2>());
-      if (e == cudaSuccess) e = ring_smem(k_helmholtz<2, double2, 1>, 2 * helm_smem<2>());
-      if (e == cudaSuccess) e = ring_smem(k_helmholtz<2, float2, 2>, helm_smem<2, 2>());
-      if (e == cudaSuccess) e = ring_smem(k_helmholtz<2, double2, 2>, helm_smem<2, 2>());
-      break;
-    case 3:
-      e = ring_smem(k_helmholtz<3, float2, 1>, 2 * helm_smem<3>());
-      if (e == cudaSuccess) e = ring_smem(k_helmholtz<3, double2, 1>, 2 * helm_smem<3>());
-      if (e == cudaSuccess) e = ring_smem(k_helmholtz<3, float2, 2>, helm_smem<3, 2>());
-      if (e == cudaSuccess) e = ring_smem(k_helmholtz<3, double2, 2>, helm_smem<3, 2>());
-      break;
-    case 4:
-      e = ring_smem(k_helmholtz<4, float2, 1>, 2 * helm_smem<4>());
-      if (e == cudaSuccess) e = ring_smem(k_helmholtz<4, double2, 1>, 2 * helm_smem<4>());
-      if (e == cudaSuccess) e = ring_smem(k_helmholtz<4, float2, 2>, helm_smem<4, 2>());
-      if (e == cudaSuccess) e = ring_smem(k_helmholtz<4, double2, 2>, helm_smem<4, 2>());
-      break;
-    case 5:
-      e = ring_smem(k_helmholtz<5, float2, 1>, 2 * helm_smem<5>());
-      if (e == cudaSuccess) e = ring_smem(k_helmholtz<5, double2, 1>, 2 * helm_smem<5>());
-      if (e == cudaSuccess) e = ring_smem(k_helmholtz<5, float2, 2>, helm_smem<5, 2>());
-      if (e == cudaSuccess) e = ring_smem(k_helmholtz<5, double2, 2>, helm_smem<5, 2>());
-      break;
-    case 6:
-      e = ring_smem(k_helmholtz<6, float2, 1>, 2 * helm_smem<6>());
-      if (e == cudaSuccess) e = ring_smem(k_helmholtz<6, double2, 1>, 2 * helm_smem<6>());
-      if (e == cudaSuccess) e = ring_smem(k_helmholtz<6, float2, 2>, helm_smem<6, 2>());
-      if (e == cudaSuccess) e = ring_smem(k_helmholtz<6, double2, 2>, helm_smem<6, 2>());
-      break;
-    case 7:
-      e = ring_smem(k_helmholtz<7, float2, 1>, 2 * helm_smem<7>());
-      if (e == cudaSuccess) e = ring_smem(k_helmholtz<7, double2, 1>, 2 * helm_smem<7>());
-      if (e == cudaSuccess) e = ring_smem(k_helmholtz<7, float2, 2>, helm_smem<7, 2>());
-      if (e == cudaSuccess) e = ring_smem(k_helmholtz<7, double2, 2>, helm_smem<7, 2>());
-      break;
-    default: break;
-  }
+  // the solver kernels' staging ring and operator tables may exceed the default 48 KB of dynamic
+  // shared memory: allow every instantiation of this BW the device's opt-in maximum (the
+  // attribute only bounds a launch; each launch asks for what it uses)
+  cudaError_t e = set_solver_smem_limits(h);
   if (e != cudaSuccess) return e;
   switch (h.bw) {
     case 2: k_vop_factor<2><<<blocks, 128, 0, st>>>(a); break;

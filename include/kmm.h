@@ -100,12 +100,15 @@ typedef struct kmm_tuning {
   int32_t u_layout;           /* U factor storage: 0 = [offset][y][mode], 1 = [y][offset][mode] */
   int32_t assemble_threads;   /* threads per block of the C1/C2 assembly */
   int32_t tuned;              /* 1 once kmm_autotune has run */
-  int32_t reserved;
+  int32_t tables_shared;      /* 1: the hvhg and Helmholtz solvers copy the B-spline operator
+                                 tables they read into shared memory first */
   double ms_z[3];             /* zinv + zfwd per z variant */
   double ms_x[3];             /* x pass per x variant */
-  double ms_modes[2];         /* hvhg + Helmholtz at 32 and 64 modes per block */
+  double ms_modes[2];         /* hvhg + Helmholtz at 32 and 64 modes per block (best tables choice) */
   double ms_layout[2];        /* hvhg + Helmholtz per U layout */
   double ms_assemble[3];      /* assembly at 128, 256, 512 threads */
+  double ms_tables[2];        /* hvhg + Helmholtz with the tables read through L1 / from shared
+                                 memory (best modes per block; 0 where they do not fit) */
 } kmm_tuning;
 
 typedef struct kmm_handle kmm_handle;

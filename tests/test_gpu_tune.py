@@ -35,6 +35,8 @@ def test_every_candidate_shape_is_bit_identical(precision):
     cases = [dict(z_lines_per_block=z) for z in z_lines]
     cases += [dict(x_rows_per_block=r, x_threads=t) for r, t in x_shapes]
     cases += [dict(modes_per_block=64), dict(u_layout=1), dict(assemble_threads=128), dict(assemble_threads=512)]
+    # the operator tables through L1 or from shared memory, at both block sizes
+    cases += [dict(modes_per_block=mb, tables_shared=ts) for mb in (32, 64) for ts in (0, 1)]
     for case in cases:
         got = _run(cfg, U, case)
         for f in STATE_SLOTS:
@@ -60,7 +62,8 @@ def test_autotune_keeps_the_state_and_reports_its_choice():
     for f in STATE_SLOTS:
         assert np.array_equal(got[f], ref[f]), f
     assert t["tuned"] == 1 and t["modes_per_block"] in (32, 64) and t["assemble_threads"] in (128, 256, 512)
-    assert all(x > 0 for x in rep["ms_z"] + rep["ms_x"] + rep["ms_modes"] + rep["ms_assemble"])
+    assert all(x > 0 for x in rep["ms_z"] + rep["ms_x"] + rep["ms_modes"] + rep["ms_assemble"] + rep["ms_tables"])
+    assert t["tables_shared"] in (0, 1)
     with pytest.raises(KmmError) as e:
         with Channel(cfg) as ch:
             ch.set_tuning(z_lines_per_block=7)
