@@ -8,3 +8,4 @@ interface.
 """
 from .solver import Channel, Config, KmmError, NFIELD, ensemble_step, labs_fill_full, read_input_file  # noqa: F401
 from . import ic  # noqa: F401
+from .hdf5_io import IoFile  # noqa: F401

@@ -19,6 +19,9 @@ KMM_ERR_DT = 3
 KMM_ERR_NONFINITE = 4
 KMM_ERR_ARG = 5
 KMM_ERR_TIMEOUT = 6  # reserved
+KMM_ERR_IO = 7
+KMM_STORE_U, KMM_STORE_V, KMM_STORE_W, KMM_STORE_G, KMM_STORE_PHI, KMM_STORE_THETA = 1, 2, 4, 8, 16, 32
+KMM_STORE_ALL = 63
 
 KMM_PREC_FP64 = 0
 KMM_PREC_MIXED = 1
@@ -87,6 +90,10 @@ class KmmTuning(C.Structure):
         return d
 
 
+class KmmRestartInfo(C.Structure):
+    _fields_ = [("timestep", C.c_int32), ("reserved", C.c_int32), ("time", C.c_double), ("dt", C.c_double)]
+
+
 # every symbol include/kmm.h declares, with its ctypes signature
 _P = C.c_void_p
 _D = C.POINTER(C.c_double)
@@ -143,6 +150,27 @@ SIGNATURES = {
     "kmm_get_tuning": (C.c_int, [_P, C.POINTER(KmmTuning)]),
     "kmm_set_tuning": (C.c_int, [_P, C.POINTER(KmmTuning)]),
     "kmm_helmholtz_solve_noalloc": (C.c_int, [C.c_int, C.c_int, C.c_int, _P, _P, _P, _P, _P, _P]),
+    "kmm_io_create": (C.c_int, [C.c_char_p, C.c_int32, C.POINTER(_P)]),
+    "kmm_io_open": (C.c_int, [C.c_char_p, C.c_int32, C.POINTER(_P)]),
+    "kmm_io_close": (C.c_int, [_P]),
+    "kmm_io_string_set": (C.c_int, [_P, C.c_char_p, C.c_char_p]),
+    "kmm_io_string_get": (C.c_int, [_P, C.c_char_p, C.c_char_p, C.c_int64]),
+    "kmm_io_exists": (C.c_int, [_P, C.c_char_p]),
+    "kmm_io_line_write_double": (C.c_int, [_P, C.c_char_p, C.c_int64, _D, C.c_char_p]),
+    "kmm_io_line_write_integer": (C.c_int, [_P, C.c_char_p, C.c_int64, C.POINTER(C.c_int32), C.c_char_p]),
+    "kmm_io_line_read_double": (C.c_int, [_P, C.c_char_p, C.c_int64, C.c_int64, C.c_int64, _D]),
+    "kmm_io_line_read_integer": (C.c_int, [_P, C.c_char_p, C.c_int64, C.c_int64, C.c_int64, C.POINTER(C.c_int32)]),
+    "kmm_io_plane_write_double": (C.c_int, [_P, C.c_char_p, C.c_int64, C.c_int64, _D, C.c_char_p]),
+    "kmm_io_plane_read_double": (C.c_int, [_P, C.c_char_p, C.c_int64, C.c_int64, _D]),
+    "kmm_io_field_writev_double": (C.c_int, [_P, C.c_char_p, C.c_int64, C.c_int64, C.c_int64, C.c_int32, _D]),
+    "kmm_io_field_readv_double": (C.c_int, [_P, C.c_char_p, C.c_int64, C.c_int64, C.c_int64, C.c_int32,
+                                            C.c_int64, C.c_int64, C.c_int64, C.c_int64, _D]),
+    "kmm_io_dataset_write_raw": (C.c_int, [_P, C.c_char_p, C.c_int32, C.POINTER(C.c_int64), C.c_int32, C.c_int32,
+                                           _P]),
+    "kmm_io_attr_write_integer": (C.c_int, [_P, C.c_char_p, C.c_char_p, C.c_int64, C.POINTER(C.c_int32)]),
+    "kmm_io_delete": (C.c_int, [_P, C.c_char_p]),
+    "kmm_data_store": (C.c_int, [_P, C.c_char_p, C.c_int32, C.c_double, C.c_int32]),
+    "kmm_restart": (C.c_int, [_P, C.c_char_p, C.c_int32, C.POINTER(KmmRestartInfo)]),
 }
 
 _lib = None

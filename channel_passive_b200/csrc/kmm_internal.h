@@ -168,6 +168,8 @@ cudaError_t launch_labs_mat_mul(Handle &h, int which, const double2 *x, double2 
                                 cudaStream_t st);
 
 void set_error(const std::string &msg);
+// Frees a checkpoint file handle without writing it (an error part-way through a data store).
+void io_discard(kmm_io *io);
 
 // Makes a handle's device current for the lifetime of the guard and gives the caller's current
 // device back on destruction.  Every handle entry point holds one, so handles on several GPUs,

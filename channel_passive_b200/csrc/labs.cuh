@@ -16,25 +16,28 @@
 
 namespace kmm {
 
-__device__ __forceinline__ double2 z2(double a, double b) { return make_double2(a, b); }
-__device__ __forceinline__ double2 zadd(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
-__device__ __forceinline__ double2 zsub(double2 a, double2 b) { return make_double2(a.x - b.x, a.y - b.y); }
-__device__ __forceinline__ double2 zmul(double2 a, double2 b) {
+__host__ __device__ __forceinline__ double2 z2(double a, double b) { return make_double2(a, b); }
+__host__ __device__ __forceinline__ double2 zadd(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
+__host__ __device__ __forceinline__ double2 zsub(double2 a, double2 b) { return make_double2(a.x - b.x, a.y - b.y); }
+__host__ __device__ __forceinline__ double2 zmul(double2 a, double2 b) {
   return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
 }
-__device__ __forceinline__ double2 zscale(double s, double2 a) { return make_double2(s * a.x, s * a.y); }
-__device__ __forceinline__ double2 zdiv(double2 a, double2 b) {
+__host__ __device__ __forceinline__ double2 zscale(double s, double2 a) { return make_double2(s * a.x, s * a.y); }
+__host__ __device__ __forceinline__ double2 zdiv(double2 a, double2 b) {
   const double d = b.x * b.x + b.y * b.y;
   return make_double2((a.x * b.x + a.y * b.y) / d, (a.y * b.x - a.x * b.y) / d);
 }
+
+// (The helpers above, Line<double2>, BandM and the three routines below also compile for the
+// host, where the restart reconstructions of initial_step.f90 use them with stride 1.)
 
 // Strided complex line; storage double2 or float2, arithmetic always in double.
 template <typename T> struct Line;
 template <> struct Line<double2> {
   double2 *p;
   int64_t s;
-  __device__ __forceinline__ double2 ld(int i) const { return p[(i - 1) * (int)s]; }
-  __device__ __forceinline__ void st(int i, double2 v) const { p[(i - 1) * (int)s] = v; }
+  __host__ __device__ __forceinline__ double2 ld(int i) const { return p[(i - 1) * (int)s]; }
+  __host__ __device__ __forceinline__ void st(int i, double2 v) const { p[(i - 1) * (int)s] = v; }
 };
 template <> struct Line<float2> {
   float2 *p;
@@ -58,15 +61,17 @@ template <int BW> struct BandS {
 template <int BW> struct BandM {
   double *p;
   int64_t s;
-  __device__ __forceinline__ double g(int r, int j) const { return p[((int64_t)(j - 1) * (2 * BW + 1) + (r - 1)) * s]; }
-  __device__ __forceinline__ void set(int r, int j, double v) const {
+  __host__ __device__ __forceinline__ double g(int r, int j) const {
+    return p[((int64_t)(j - 1) * (2 * BW + 1) + (r - 1)) * s];
+  }
+  __host__ __device__ __forceinline__ void set(int r, int j, double v) const {
     p[((int64_t)(j - 1) * (2 * BW + 1) + (r - 1)) * s] = v;
   }
 };
 
 // fixed_bandec, module_labs.f90:3487-3636.
 template <int BW>
-__device__ __noinline__ void labs_lu(BandM<BW> A, int n) {
+__host__ __device__ __noinline__ void labs_lu(BandM<BW> A, int n) {
   constexpr int bw = BW, m = BW + 1;
   for (int i = 1; i <= bw; ++i) {  // upper region
     const double dummy = 1.0 / A.g(m, i);
@@ -179,7 +184,7 @@ __device__ __noinline__ void labs_lu(BandM<BW> A, int n) {
 
 // fixed_banbks, module_labs.f90:4252-4318 (complex right-hand side, in place).
 template <int BW, typename BandT, typename LineT>
-__device__ __noinline__ void labs_bs(BandT A, LineT b, int n) {
+__host__ __device__ __noinline__ void labs_bs(BandT A, LineT b, int n) {
   constexpr int bw = BW, m = BW + 1;
   for (int i = 1; i <= bw; ++i) {
     double2 acc = b.ld(i);
@@ -223,8 +228,8 @@ __device__ __noinline__ void labs_bs(BandT A, LineT b, int n) {
 }
 
 // LABS_mat_mul_bw, module_labs.f90:4687-4722: b = A x (x and b distinct).
-template <int BW, typename XT, typename BT>
-__device__ __noinline__ void labs_mat_mul(BandS<BW> A, XT x, BT b, int n) {
+template <int BW, typename BandT, typename XT, typename BT>
+__host__ __device__ __noinline__ void labs_mat_mul(BandT A, XT x, BT b, int n) {
   constexpr int bw = BW;
   for (int j = 1; j <= bw; ++j) {
     double2 acc = z2(0.0, 0.0);

@@ -295,6 +295,19 @@ class Channel:
         check(self._lib.kmm_adjoint_backward(self._h, C.byref(dA), _dptr(dg)))
         return dA.value, dg
 
+    def data_store(self, path: str, timestep: int = 0, time: float = 0.0, fields: int = _lib.KMM_STORE_ALL):
+        """kmm_data_store (data_store.f90:11-173): the state and the problem definition as a restart
+        file in the reference's HDF5 layout; timestep and time are the driver's counters."""
+        check(self._lib.kmm_data_store(self._h, str(path).encode(), int(timestep), float(time), int(fields)))
+
+    def restart(self, path: str, option: int = 1) -> dict:
+        """kmm_restart (initial_step.f90:15-56, 184-513): the state from a restart file with
+        restart_option 1 (u, v, w, theta), 2 (g, phi, theta + mean profiles) or 3 (v, g, theta +
+        mean profiles); returns the file's timestep, time and dt (the handle's dt becomes it)."""
+        info = _lib.KmmRestartInfo()
+        check(self._lib.kmm_restart(self._h, str(path).encode(), int(option), C.byref(info)))
+        return {"timestep": info.timestep, "time": info.time, "dt": info.dt}
+
     def adjoint_release(self):
         check(self._lib.kmm_adjoint_release(self._h))
 

@@ -36,6 +36,8 @@ extern "C" {
 #define KMM_ERR_NONFINITE 4   /* NaN / Inf in the velocity maximum or in uploaded state */
 #define KMM_ERR_ARG 5         /* null pointer, bad substep, size mismatch */
 #define KMM_ERR_TIMEOUT 6     /* reserved: no entry point waits on the device with a limit yet */
+#define KMM_ERR_IO 7          /* checkpoint file: unreadable, missing dataset, unexpected shape or
+                                 type (the checks of module_hdf5_io.f90:212-345, same messages) */
 
 #define KMM_PREC_FP64 0       /* every kernel in FP64 */
 #define KMM_PREC_MIXED 1      /* FP32 transforms/products, FP64 state, v-influence and mean modes */
@@ -362,6 +364,81 @@ int kmm_dev_solve_u_w(kmm_handle *h, double *g, double *f, const double *kx, con
 int kmm_adjoint_forward(kmm_handle *h, int nsteps, double w_tau, double w_q, double *J);
 int kmm_adjoint_backward(kmm_handle *h, double *dJ_dA, double *dJ_dgains);
 int kmm_adjoint_release(kmm_handle *h);
+
+/* ---- Checkpoint files (channel_hdf5_io, module_hdf5_io.f90:6-456) --------------------------
+ * HDF5 files with the reference's datasets and layout, read and written by the library itself
+ * (no HDF5 library): root-group datasets, lines (1-D float64 / int32), planes (Fortran (a, b)),
+ * fields (Fortran (ny, nx/2, nz) of (re, im) pairs: ESIO layout 0, and on reading the legacy
+ * ESIO layouts 1 and 2 that an int32[8] esio_field_metadata attribute announces).  One process
+ * holds the whole file: the reference's MPI decomposition becomes the (start, count) arguments of
+ * the reads.  A file is written when it is closed; a file opened with readwrite = 1 is read whole
+ * and written again on close. */
+typedef struct kmm_io kmm_io;
+/* io_file_create (module_hdf5_io.f90:63-78): overwrite = 0 refuses an existing path.  Like the
+ * reference it sets the root attribute Native_IO. */
+int kmm_io_create(const char *path, int32_t overwrite, kmm_io **out);
+/* io_file_open (:80-95) */
+int kmm_io_open(const char *path, int32_t readwrite, kmm_io **out);
+/* io_file_close (:107-114): writes the file if it was created or changed; frees io either way. */
+int kmm_io_close(kmm_io *io);
+/* io_string_set on "/" (:169-210): replaces the root attribute `name`. */
+int kmm_io_string_set(kmm_io *io, const char *name, const char *value);
+int kmm_io_string_get(kmm_io *io, const char *name, char *buf, int64_t len);
+/* 1 if the root group holds dataset `name`, 0 if not (negative on a bad argument). */
+int kmm_io_exists(kmm_io *io, const char *name);
+/* io_line_write_double / _integer (:347-376): a 1-D dataset of n values, optional comment. */
+int kmm_io_line_write_double(kmm_io *io, const char *name, int64_t n, const double *v, const char *comment);
+int kmm_io_line_write_integer(kmm_io *io, const char *name, int64_t n, const int32_t *v, const char *comment);
+/* io_line_read_double / _integer (:357-386): values [start, start + count) of a line of n. */
+int kmm_io_line_read_double(kmm_io *io, const char *name, int64_t n, int64_t start, int64_t count, double *v);
+int kmm_io_line_read_integer(kmm_io *io, const char *name, int64_t n, int64_t start, int64_t count, int32_t *v);
+/* io_plane_write_double (:388-403): v is Fortran (na, nb). */
+int kmm_io_plane_write_double(kmm_io *io, const char *name, int64_t na, int64_t nb, const double *v,
+                              const char *comment);
+int kmm_io_plane_read_double(kmm_io *io, const char *name, int64_t na, int64_t nb, double *v);
+/* io_field_writev_double / io_field_readv_double (:405-419): v is Fortran (ncomp, ny, nxh, nz);
+ * a read takes kx [x0, x0 + xn) and kz [z0, z0 + zn) (all of y) into (ncomp, ny, xn, zn). */
+int kmm_io_field_writev_double(kmm_io *io, const char *name, int64_t ny, int64_t nxh, int64_t nz, int32_t ncomp,
+                               const double *v);
+int kmm_io_field_readv_double(kmm_io *io, const char *name, int64_t ny, int64_t nxh, int64_t nz, int32_t ncomp,
+                              int64_t x0, int64_t xn, int64_t z0, int64_t zn, double *v);
+/* A dataset of any C-order shape (rank 0 = scalar) of float64 (kind 0; ncomp > 1 makes each element
+ * an array of ncomp float64) or int32 (kind 1), and an int32 attribute on a dataset: for files
+ * the readers above must refuse, and for tools.  kmm_io_delete removes a dataset. */
+int kmm_io_dataset_write_raw(kmm_io *io, const char *name, int32_t rank, const int64_t *cdims, int32_t kind,
+                             int32_t ncomp, const void *data);
+int kmm_io_attr_write_integer(kmm_io *io, const char *dataset, const char *name, int64_t n, const int32_t *v);
+int kmm_io_delete(kmm_io *io, const char *name);
+
+/* data_store / data_store_f (data_store.f90:11-173, 176-420): writes the handle's state as a
+ * restart file: the root attributes, the scalar lines (timestep, time, nu, Pr, U_gal, U_avg,
+ * W_avg, T_avg, Re, LMFx/y/z, Lx/y/z, Stretch, dt, nx, ny, nz, LABS_K, LABS_BW), the mean
+ * profiles U_mean (with U_gal added back), W_mean, T_mean, the operator lines and planes
+ * (LABS_COL, LABS_CENTER_LINE, LABS_INTEGRATE, LABS_KNOT, LABS_D0/D1/D2_FULL, LABS_D0/D1/D2_BAND)
+ * and the fields selected by `fields` (the input file's write_u ... write_t switches):
+ * u, v, w and theta from the state, g and phi from RK_STORE 1 and 2.  timestep and time are
+ * the caller's (the driver counts them); dt is the handle's. */
+#define KMM_STORE_U 1
+#define KMM_STORE_V 2
+#define KMM_STORE_W 4
+#define KMM_STORE_G 8
+#define KMM_STORE_PHI 16
+#define KMM_STORE_THETA 32
+#define KMM_STORE_ALL 63
+int kmm_data_store(kmm_handle *h, const char *path, int32_t timestep, double time, int32_t fields);
+/* initial_step with a restart file (initial_step.f90:15-56, 184-513): restart_option 1 reads
+ * u, v, w, theta (data_read_uvw) and runs set_initial_data_uvw; 2 reads g, phi, theta and the
+ * mean profiles (data_read_gphi) and rebuilds u, v, w (set_initial_data_gphi); 3 reads v, g,
+ * theta and the mean profiles (data_read_vg) and rebuilds u, w and phi (set_initial_data_vg).
+ * U_gal is taken off the mean streamwise velocity as the reference does.  The handle's dt
+ * becomes the file's; timestep, time and dt are returned. */
+typedef struct kmm_restart_info {
+  int32_t timestep;
+  int32_t reserved;
+  double time;
+  double dt;
+} kmm_restart_info;
+int kmm_restart(kmm_handle *h, const char *path, int32_t restart_option, kmm_restart_info *out);
 
 /* Allocation-free batched Helmholtz solve.  No counterpart in the reference: it exists for
  * callers that may not allocate device memory (code running while a stream is captured into a

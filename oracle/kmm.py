@@ -686,6 +686,61 @@ def set_initial_data_uvw(U, ops: Operators, p: Params):
     return RK
 
 
+def set_initial_data_gphi(RK, ops: Operators, p: Params):
+    """initial_step.f90:430-513 (restart option 2): u, v, w and theta from the stores g, phi,
+    theta (RK[0..2]; their (0, 0) mode holds the mean U, W, theta).  Returns U (10 fields)."""
+    kxi, kzi = wavenumbers(p.nx, p.nz)
+    U = np.zeros((10, p.nz, p.nxh, p.ny), dtype=np.complex128)
+    lmfxr, lmfzr = 1.0 / p.lmfx, 1.0 / p.lmfz
+    ny, bw = p.ny, ops.bw
+    for j, kzv in enumerate(kzi):
+        for k, kxv in enumerate(kxi):
+            if kxv == 0 and kzv == 0:
+                U[0, j, k], U[2, j, k], U[6, j, k] = RK[0, j, k], RK[1, j, k], RK[2, j, k]
+                continue
+            k2 = (kzv * lmfzr) ** 2 + (kxv * lmfxr) ** 2
+            kxx, kzz = 1j * kxv * lmfxr / k2, 1j * kzv * lmfzr / k2
+            D = -k2 * ops.D0 + ops.D2
+            for col in (0, ny - 1):  # Dirichlet rows: only the diagonal of D2 - k^2 D0
+                keep = D[bw, col]
+                D[:, col] = 0.0
+                D[bw, col] = keep
+            c = RK[1, j, k].copy()
+            c[0] = c[-1] = 0.0
+            c = labs.bs(labs.lu(D), c)
+            U[1, j, k] = labs.mat_mul(ops.D0, c)
+            dv = labs.mat_mul(ops.D1, c)
+            g = RK[0, j, k]
+            U[0, j, k] = kxx * dv - kzz * g
+            U[2, j, k] = kxx * g + kzz * dv
+            U[6, j, k] = RK[2, j, k]
+    return U
+
+
+def set_initial_data_vg(U, RK, ops: Operators, p: Params):
+    """initial_step.f90:301-353 (restart option 3): u, w (and phi into RK[1]) from v = U[1] and
+    g = RK[0]; theta from RK[2]; the (0, 0) mode takes U, W, theta from the stores.  Returns
+    (U, RK), both new arrays."""
+    kxi, kzi = wavenumbers(p.nx, p.nz)
+    U, RK = U.copy(), RK.copy()
+    lmfxr, lmfzr = 1.0 / p.lmfx, 1.0 / p.lmfz
+    for j, kzv in enumerate(kzi):
+        for k, kxv in enumerate(kxi):
+            if kxv == 0 and kzv == 0:
+                U[0, j, k], U[1, j, k], U[2, j, k], U[6, j, k] = RK[0, j, k], 0.0, RK[1, j, k], RK[2, j, k]
+                continue
+            c = labs.bs(ops.D0_lu, U[1, j, k])
+            dv = labs.mat_mul(ops.D1, c)
+            k2 = (kxv * lmfxr) ** 2 + (kzv * lmfzr) ** 2
+            RK[1, j, k] = labs.mat_mul(ops.D2, c) - k2 * U[1, j, k]
+            kxx, kzz = 1j * kxv * lmfxr / k2, 1j * kzv * lmfzr / k2
+            g = RK[0, j, k]
+            U[0, j, k] = kxx * dv - kzz * g
+            U[2, j, k] = kxx * g + kzz * dv
+            U[6, j, k] = RK[2, j, k]
+    return U, RK
+
+
 # ----------------------------------------------------------------------------
 # pressure (row 19): get_pressure / cal_pressure / solve_ppe, get_pressure.f90:1-137
 # ----------------------------------------------------------------------------
