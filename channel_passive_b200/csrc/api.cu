@@ -213,7 +213,9 @@ int enqueue_substep(Handle &h, int s, cudaStream_t st, cudaEvent_t *ev = nullptr
     return rc;
   if ((rc = rec(KMM_K_HVHG, [&] { return launch_ws_hvhg(h, s, nullptr, st); }))) return rc;
   if ((rc = rec(KMM_K_HELMHOLTZ, [&] { return launch_ws_helmholtz(h, s, nullptr, st); }))) return rc;
-  if ((rc = rec(KMM_K_ASSEMBLE, [&] { return launch_ws_assemble(h, s, nullptr, st); }))) return rc;
+  if ((rc = rec(KMM_K_ASSEMBLE, [&] { return launch_ws_assemble_only(h, s, nullptr, st); }))) return rc;
+  // the mean lines (side stream) join here, outside the assembly's event pair
+  KMM_CUDA(launch_ws_join(h, st));
   return KMM_OK;
 }
 
@@ -557,12 +559,7 @@ int kmm_create(const kmm_config *cfg, kmm_handle **out) {
       return fail(KMM_ERR_CUDA);
     }
   }
-  // untuned launch shapes: 64-mode solver blocks with their operator tables in shared memory
-  // where two such blocks fit on an SM, else 32-mode blocks reading the tables through L1
-  if (solver_tables_default(*h)) {
-    h->tune.groups = 2;
-    h->tune.stab = 1;
-  }
+  default_solver_shapes(*h);  // the untuned solver launch shapes
   if (cfg->autotune && (rc = autotune(*h, nullptr))) return fail(rc);
   *out = reinterpret_cast<kmm_handle *>(h);
   return KMM_OK;

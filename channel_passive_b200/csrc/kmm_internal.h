@@ -83,13 +83,17 @@ struct Adjoint;
 struct Tuning {
   int z = 0;              // z-transform variant (lines per block, transforms2.cu ZVar)
   int x = 0;              // x-pass variant (rows per block and threads, XVar)
-  int groups = 1;         // 32-mode groups per block of the hvhg and Helmholtz kernels (1 or 2)
+  int groups = 1;         // 32-mode groups per block of the hvhg kernel (1 or 2)
+  int hgroups = 1;        // 32-mode groups per block of the Helmholtz kernel (1, 2 or 4)
+  int hstab = 0;          // 1: the Helmholtz kernel reads the operator tables from shared memory
+  int stage = 1;          // steps of staging look-ahead of the Helmholtz sweeps (1 or 2)
   int ulayout = 0;        // U factor storage: 0 = [offset][y][mode], 1 = [y][offset][mode]
   int asm_threads = 256;  // threads per block of the assembly kernel
-  int stab = 0;           // 1: the hvhg and Helmholtz kernels read the operator tables from shared memory
+  int stab = 0;           // 1: the hvhg kernel reads the operator tables from shared memory
   bool tuned = false;
   // device ms of every candidate of the last autotune (kmm_tuning's ms_* fields)
   double ms_z[3] = {}, ms_x[3] = {}, ms_modes[2] = {}, ms_layout[2] = {}, ms_assemble[3] = {}, ms_tables[2] = {};
+  double ms_helm[3][2][2] = {};  // [32/64/128 modes][tables via L1 / shared][look-ahead 1 / 2]
 };
 
 struct Handle {
@@ -222,6 +226,10 @@ cudaError_t launch_wavespace_split(Handle &h, int substep, const double *dt_over
 cudaError_t launch_ws_hvhg(Handle &h, int substep, const double *dt_override, cudaStream_t st);
 cudaError_t launch_ws_helmholtz(Handle &h, int substep, const double *dt_override, cudaStream_t st);
 cudaError_t launch_ws_assemble(Handle &h, int substep, const double *dt_override, cudaStream_t st);
+// The assembly kernel alone, and the join of the mean lines (the side stream) onto st; the
+// kernel-by-kernel profile records the assembly without the join.
+cudaError_t launch_ws_assemble_only(Handle &h, int substep, const double *dt_ptr, cudaStream_t st);
+cudaError_t launch_ws_join(Handle &h, cudaStream_t st);
 // The pressure of the state (pressure.cu): p planes [y][mode] into out, with the wall values
 // bc [2][nmodes] (launch_ydiff); mom as in launch_xphys2.  Uses MID, P, the solver lines zc
 // and U region 0 as scratch; cudaErrorNotSupported for x lengths without a four-step shape.
@@ -247,12 +255,13 @@ int64_t vop_factor_doubles(const Handle &h);
 cudaError_t launch_vop_factor(Handle &h, cudaStream_t st);
 // Doubles of U factor storage per solver role.
 int64_t split_ub_role(const Handle &h);
-// Operator tables in shared memory for the hvhg and Helmholtz kernels: their bytes per block,
-// whether a block of `groups` 32-mode groups can hold them beside its staging ring, and whether
-// a handle starts with them (two resident 64-mode blocks per SM).
+// Operator tables in shared memory for the hvhg and Helmholtz kernels (their bytes per block,
+// whether hvhg's block holds them) and the Helmholtz shapes a block can hold (groups, tables,
+// look-ahead); default_solver_shapes sets a new handle's solver shapes.
 size_t solver_tables_bytes(const Handle &h);
-bool solver_tables_fit(const Handle &h, int groups);
-bool solver_tables_default(const Handle &h);
+bool hvhg_tables_fit(const Handle &h);
+bool helm_shape_fits(const Handle &h, int hgroups, int hstab, int stage);
+void default_solver_shapes(Handle &h);
 
 // One time_march substep enqueued kernel by kernel on st (api.cu), the device scalars read back,
 // and the step graph captured if it is not yet.

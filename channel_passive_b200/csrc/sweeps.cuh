@@ -53,20 +53,21 @@ __device__ __forceinline__ void cp_async_wait() {
   asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
 }
 
-// Steps of look-ahead of an asynchronously staged sweep, and its ring slots.
+// Steps of look-ahead of an asynchronously staged sweep (by default; the Helmholtz kernel takes
+// its own as a template parameter), and its ring slots.
 constexpr int kStageAhead = 1;
 constexpr int kStageSlots = kStageAhead + 1;
 
-// A thread-private ring in shared memory of kStageSlots slots x K 16-byte units, interleaved
-// across the block's nt threads (unit (slot, k) of thread t at smem[(slot * K + k) * nt + t]):
-// the rows one sweep step reads, copied in by cp.async kStageAhead steps before that step.
-// Slots are indexed by the sweep step (the row being eliminated), so a step's inputs may come
-// from other rows (the emission rows q = r + BW of a backward sweep).
-template <int K>
+// A thread-private ring in shared memory of S slots x K 16-byte units, interleaved across the
+// block's nt threads (unit (slot, k) of thread t at smem[(slot * K + k) * nt + t]): the rows one
+// sweep step reads, copied in by cp.async S - 1 steps before that step.  Slots are indexed by the
+// sweep step (the row being eliminated), so a step's inputs may come from other rows (the
+// emission rows q = r + BW of a backward sweep).
+template <int K, int S = kStageSlots>
 struct Ring {
   double2 *base;  // this thread's column: smem + threadIdx.x
   int nt;
-  __device__ __forceinline__ double2 *at(int step, int k) const { return base + ((step % kStageSlots) * K + k) * nt; }
+  __device__ __forceinline__ double2 *at(int step, int k) const { return base + ((step % S) * K + k) * nt; }
   __device__ __forceinline__ void get(int step, int k, const double2 *g) const { cp_async16(at(step, k), g); }
   __device__ __forceinline__ void get(int step, int k, const float2 *g) const { cp_async8(at(step, k), g); }
   __device__ __forceinline__ void get(int step, int k, const double *g) const { cp_async8(at(step, k), g); }

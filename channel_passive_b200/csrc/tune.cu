@@ -5,10 +5,11 @@
 // candidates are
 //   z transforms   kx lines per block (transforms2.cu ZVar; zinv + zfwd timed together),
 //   x pass         z rows per block and threads (XVar),
-//   per-mode solve 32 or 64 (kx, kz) systems per block of k_hvhg and k_helmholtz (one scalar),
-//                  each with the operator tables read through L1 or copied to shared memory
-//                  (where a block can hold them), then the U factor storage layout of the
-//                  Helmholtz roles,
+//   hvhg           32 or 64 (kx, kz) systems per block (one scalar), each with the operator
+//                  tables read through L1 or copied to shared memory,
+//   Helmholtz      32, 64 or 128 systems per block x tables through L1 / in shared memory x one
+//                  or two rows of staging look-ahead, where a block's shared memory holds the
+//                  shape; then the U factor storage layout,
 //   assembly       threads per block.
 // Each candidate runs once to warm up, then kReps times between CUDA events on the handle's
 // stream; the minimum of the means wins.  The solver runs mutate the state, so the state, the
@@ -123,49 +124,92 @@ int autotune(Handle &h, kmm_tuning *out) {
     TUNE_CUDA(launch_xphys(h, h.MID, 2, st));
     TUNE_CUDA(launch_zfwd(h, h.MID, h.P, nprod, h.rescale, !h.mixed, st));
   }
-  // hvhg forks the mean lines to the side stream; join them so no run overlaps the next restore
+  // hvhg forks the mean lines to the side stream: every restore first waits for them.  The join
+  // event's last record may sit in the captured step graph, which a wait outside the graph
+  // refuses: record it on the side stream first.
+  TUNE_CUDA(cudaEventRecord(h.ev_join, h.side));
+  auto restore_joined = [&]() -> int {
+    TUNE_CUDA(cudaStreamWaitEvent(st, h.ev_join, 0));
+    return restore();
+  };
+  auto keep_min = [](double &acc, double v) {
+    if (v > 0.0 && (acc == 0.0 || v < acc)) acc = v;
+  };
+  // k_hvhg: modes per block x tables through L1 / in shared memory
+  const int ng = h.nsc == 1 ? 2 : 1;
+  {
+    double best_ms = 0.0;
+    int bg = 1, bs = 0;
+    for (int g = 1; g <= ng; ++g)
+      for (int sh = 0; sh < 2; ++sh) {
+        if (sh && !hvhg_tables_fit(h)) continue;
+        h.tune.groups = g;
+        h.tune.stab = sh;
+        double ms = 0.0;
+        auto body = [&]() { return launch_ws_hvhg(h, 2, nullptr, st); };
+        if ((rc = measure(restore_joined, body, &ms))) return rc;
+        keep_min(rep.ms_modes[g - 1], ms);
+        keep_min(rep.ms_tables[sh], ms);
+        if (best_ms == 0.0 || ms < best_ms) {
+          best_ms = ms;
+          bg = g;
+          bs = sh;
+        }
+      }
+    h.tune.groups = bg;
+    h.tune.stab = bs;
+  }
+  // k_helmholtz after the chosen hvhg: modes per block x tables x staging look-ahead, then the
+  // U factor layout
+  auto after_hvhg = [&]() -> int {
+    int r = restore_joined();
+    if (r) return r;
+    TUNE_CUDA(launch_ws_hvhg(h, 2, nullptr, st));
+    return KMM_OK;
+  };
+  auto helm = [&]() { return launch_ws_helmholtz(h, 2, nullptr, st); };
+  {
+    h.tune.ulayout = 0;
+    double best_ms = 0.0;
+    int bg = 1, bs = 0, ba = 1;
+    const int hg_n[3] = {1, 2, 4};
+    for (int gi = 0; gi < 3; ++gi)
+      for (int sh = 0; sh < 2; ++sh)
+        for (int sa = 1; sa <= 2; ++sa) {
+          const int g = hg_n[gi];
+          if (!helm_shape_fits(h, g, sh, sa)) continue;
+          h.tune.hgroups = g;
+          h.tune.hstab = sh;
+          h.tune.stage = sa;
+          double ms = 0.0;
+          if ((rc = measure(after_hvhg, helm, &ms))) return rc;
+          rep.ms_helm[(gi * 2 + sh) * 2 + sa - 1] = ms;
+          if (best_ms == 0.0 || ms < best_ms) {
+            best_ms = ms;
+            bg = g;
+            bs = sh;
+            ba = sa;
+          }
+        }
+    h.tune.hgroups = bg;
+    h.tune.hstab = bs;
+    h.tune.stage = ba;
+    rep.ms_layout[0] = best_ms;
+  }
+  h.tune.ulayout = 1;
+  if ((rc = measure(after_hvhg, helm, &rep.ms_layout[1]))) return rc;
+  h.tune.ulayout = rep.ms_layout[1] < rep.ms_layout[0] ? 1 : 0;
   auto solve = [&]() {
     cudaError_t e = launch_ws_hvhg(h, 2, nullptr, st);
     if (e == cudaSuccess) e = launch_ws_helmholtz(h, 2, nullptr, st);
     if (e == cudaSuccess) e = cudaStreamWaitEvent(st, h.ev_join, 0);
     return e;
   };
-  const int ng = h.nsc == 1 ? 2 : 1;
-  double ms_gs[2][2];  // [groups - 1][tables in shared memory]
-  int bg = 1, bs = 0;
-  for (int g = 0; g < ng; ++g)
-    for (int sh = 0; sh < 2; ++sh) {
-      ms_gs[g][sh] = 0.0;
-      if (sh && !solver_tables_fit(h, g + 1)) continue;
-      h.tune.groups = g + 1;
-      h.tune.stab = sh;
-      h.tune.ulayout = 0;
-      if ((rc = measure(restore, solve, &ms_gs[g][sh]))) return rc;
-      if (ms_gs[g][sh] < ms_gs[bg - 1][bs] || (g == 0 && sh == 0)) {
-        bg = g + 1;
-        bs = sh;
-      }
-    }
-  // report the fastest measured time of each knob value (0: not measured)
-  auto keep_min = [](double &acc, double v) {
-    if (v > 0.0 && (acc == 0.0 || v < acc)) acc = v;
-  };
-  for (int g = 0; g < ng; ++g)
-    for (int sh = 0; sh < 2; ++sh) {
-      keep_min(rep.ms_modes[g], ms_gs[g][sh]);
-      keep_min(rep.ms_tables[sh], ms_gs[g][sh]);
-    }
-  h.tune.groups = bg;
-  h.tune.stab = bs;
-  rep.ms_layout[0] = ms_gs[bg - 1][bs];
-  h.tune.ulayout = 1;
-  if ((rc = measure(restore, solve, &rep.ms_layout[1]))) return rc;
-  h.tune.ulayout = best(rep.ms_layout, 2);
   const int athreads[3] = {128, 256, 512};
   for (int i = 0; i < 3; ++i) {
     h.tune.asm_threads = athreads[i];
     auto prep = [&]() -> int {
-      int r = restore();
+      int r = restore_joined();
       if (r) return r;
       TUNE_CUDA(solve());
       return KMM_OK;
@@ -174,7 +218,7 @@ int autotune(Handle &h, kmm_tuning *out) {
     if ((rc = measure(prep, body, &rep.ms_assemble[i]))) return rc;
   }
   h.tune.asm_threads = athreads[best(rep.ms_assemble, 3)];
-  if ((rc = restore())) return rc;
+  if ((rc = restore_joined())) return rc;
   TUNE_CUDA(cudaStreamSynchronize(st));
   TUNE_CUDA(cudaStreamSynchronize(h.side));
   h.tune.tuned = true;
@@ -184,6 +228,7 @@ int autotune(Handle &h, kmm_tuning *out) {
   std::memcpy(h.tune.ms_layout, rep.ms_layout, sizeof(rep.ms_layout));
   std::memcpy(h.tune.ms_assemble, rep.ms_assemble, sizeof(rep.ms_assemble));
   std::memcpy(h.tune.ms_tables, rep.ms_tables, sizeof(rep.ms_tables));
+  std::memcpy(h.tune.ms_helm, rep.ms_helm, sizeof(rep.ms_helm));
   // the step graph holds the old launch shapes: capture it again at the next step
   if (h.gexec) cudaGraphExecDestroy(h.gexec);
   if (h.graph) cudaGraphDestroy(h.graph);
@@ -205,6 +250,9 @@ int kmm_get_tuning(const kmm_handle *hh, kmm_tuning *out) {
   std::memset(out, 0, sizeof(*out));
   tile_shapes(h, h.tune.z, h.tune.x, &out->z_lines_per_block, &out->x_rows_per_block, &out->x_threads);
   out->modes_per_block = 32 * (h.nsc == 1 ? h.tune.groups : 1);
+  out->helm_modes_per_block = 32 * (h.nsc == 1 ? h.tune.hgroups : 1);
+  out->helm_tables_shared = h.tune.hstab;
+  out->helm_stage_ahead = h.nsc == 1 ? h.tune.stage : 1;
   out->u_layout = h.tune.ulayout;
   out->assemble_threads = h.tune.asm_threads;
   out->tuned = h.tune.tuned ? 1 : 0;
@@ -215,6 +263,7 @@ int kmm_get_tuning(const kmm_handle *hh, kmm_tuning *out) {
   std::memcpy(out->ms_layout, h.tune.ms_layout, sizeof(out->ms_layout));
   std::memcpy(out->ms_assemble, h.tune.ms_assemble, sizeof(out->ms_assemble));
   std::memcpy(out->ms_tables, h.tune.ms_tables, sizeof(out->ms_tables));
+  std::memcpy(out->ms_helm, h.tune.ms_helm, sizeof(out->ms_helm));
   return KMM_OK;
 }
 
@@ -232,9 +281,14 @@ int kmm_set_tuning(kmm_handle *hh, const kmm_tuning *t) {
   }
   const int g = t->modes_per_block == 32 ? 1 : t->modes_per_block == 64 ? 2 : 0;
   const bool asm_ok = t->assemble_threads == 128 || t->assemble_threads == 256 || t->assemble_threads == 512;
-  const bool tab_ok = t->tables_shared == 0 || (t->tables_shared == 1 && g != 0 && solver_tables_fit(h, g));
+  const bool tab_ok = t->tables_shared == 0 || (t->tables_shared == 1 && hvhg_tables_fit(h));
+  const int hg = t->helm_modes_per_block == 32 ? 1 : t->helm_modes_per_block == 64 ? 2
+                 : t->helm_modes_per_block == 128 ? 4 : 0;
+  const bool helm_ok = hg != 0 && (t->helm_tables_shared == 0 || t->helm_tables_shared == 1) &&
+                       (t->helm_stage_ahead == 1 || t->helm_stage_ahead == 2) &&
+                       helm_shape_fits(h, hg, t->helm_tables_shared, t->helm_stage_ahead);
   if (zv < 0 || xv < 0 || g == 0 || (g == 2 && h.nsc != 1) || (t->u_layout != 0 && t->u_layout != 1) || !asm_ok ||
-      !tab_ok) {
+      !tab_ok || !helm_ok) {
     set_error("kmm_set_tuning: a requested shape is not among this grid's candidates (see kmm_autotune)");
     return KMM_ERR_ARG;
   }
@@ -244,6 +298,9 @@ int kmm_set_tuning(kmm_handle *hh, const kmm_tuning *t) {
   next.ulayout = t->u_layout;
   next.asm_threads = t->assemble_threads;
   next.stab = t->tables_shared;
+  next.hgroups = hg;
+  next.hstab = t->helm_tables_shared;
+  next.stage = t->helm_stage_ahead;
   DeviceGuard dg(h.cfg.device);
   cudaStreamSynchronize(h.stream);
   h.tune = next;

@@ -75,9 +75,11 @@ struct SplitArgs {
   const double *dt_ptr;
   double *vf;        // the v operator's profile LU per mode: LBand, then UBand at vf + vf_l
   int64_t vf_l;
-  int groups;        // 32-mode groups per block of k_hvhg and k_helmholtz (Tuning::groups)
+  int groups;        // 32-mode groups per block of k_hvhg (Tuning::groups)
+  int hgroups;       // 32-mode groups per block of k_helmholtz (Tuning::hgroups)
   int ulayout;       // U factor layout of the per-role regions (Tuning::ulayout)
-  int stab;          // 1: k_hvhg and k_helmholtz copy the operator tables they read to shared memory
+  int stab;          // 1: k_hvhg copies the operator tables it reads to shared memory
+  int hstab;         // 1: k_helmholtz does (Tuning::hstab)
 };
 
 // Operator tables in shared memory (SplitArgs::stab).  Every lane of a warp reads the same table
@@ -301,21 +303,21 @@ k_hvhg(SplitArgs a) {
 
 // ------------------------------------------------------------------------------------------
 // k_helmholtz.  Every sweep stages the rows it reads through a thread-private shared-memory ring
-// (Ring, cp.async kStageAhead steps ahead): the kernel's 12 warps per SM would need more L1 than
-// there is to keep prefetched lines until use.  Units per step: kHelmUnits<BW>.
+// (Ring, cp.async SA steps ahead): the kernel's 12 warps per SM would need more L1 than there is
+// to keep prefetched lines until use.  Units per step: kHelmUnits<BW>.
 template <int BW>
 constexpr int kHelmUnits = 5 + BW;
 
 // A staged nonlinear-term unit, widened to double2.
-template <typename PT, int K>
-__device__ __forceinline__ double2 ring_hv(const Ring<K> &ring, int step, int k) {
+template <typename PT, int K, int S>
+__device__ __forceinline__ double2 ring_hv(const Ring<K, S> &ring, int step, int k) {
   if constexpr (sizeof(PT) == sizeof(float2)) return ring.f(step, k);
   else return ring.c(step, k);
 }
 
-template <int BW, int ROLE, typename PT>
+template <int BW, int ROLE, typename PT, int SA>
 __device__ __forceinline__ void helmholtz_role(const SplitArgs &a, const Tabs<BW> &tb, int64_t m,
-                                               const Ring<kHelmUnits<BW>> &ring) {
+                                               const Ring<kHelmUnits<BW>, SA + 1> &ring) {
   const int n = a.ny, s = a.substep;
   const int64_t nm = a.nmodes, ns = a.ns;
   const double dt = *a.dt_ptr, nu = a.nu;
@@ -359,7 +361,7 @@ __device__ __forceinline__ void helmholtz_role(const SplitArgs &a, const Tabs<BW
   };
   auto rh = [&](int step, int k) { return ring_hv<PT>(ring, step, k); };
   // forward units: 0 store, 1 hA, 2 hB, 3 D2 store (substep 1)
-  lu_fwd<BW, 1, 0, kStageAhead, true>(n, [&](int r, double *rw, bool c) { helm_row<BW>(tb, r, n, dummy, beta, rw, c); },
+  lu_fwd<BW, 1, 0, SA, true>(n, [&](int r, double *rw, bool c) { helm_row<BW>(tb, r, n, dummy, beta, rw, c); },
       [&](int r, double2 *bc, double *) {
         const double2 h = SCAL ? rh(r, 1) : zadd(rh(r, 1), rh(r, 2));
         bc[0] = rhs(ring.c(r, 0), h, s == 1 ? ring.c(r, 3) : z2(0.0, 0.0), visc, r);
@@ -373,7 +375,7 @@ __device__ __forceinline__ void helmholtz_role(const SplitArgs &a, const Tabs<BW
       });
   // backward units: 0 Z(r), 1..BW U(r, e), BW+1 hA(q), BW+2 hB(q) with q = r + BW
   const DLine out{ROLE == 0 ? a.S + 3 * ns + m : ROLE == 3 ? a.S + 4 * ns + m : a.S + m, nm};
-  bwd_emit<BW, 1, 0, kStageAhead, true>(n, [&](int r, int e) { return e <= BW ? ring.d(r, e) : ub.get(r, e); },
+  bwd_emit<BW, 1, 0, SA, true>(n, [&](int r, int e) { return e <= BW ? ring.d(r, e) : ub.get(r, e); },
       [&](int r, double2 *zc, double *) { zc[0] = ring.c(r, 0); },
       [&](int q, int r, const double2 (&wc)[1][2 * BW + 1], const double (&)[1][2 * BW + 1]) {
         const double2 f = mvc<BW>(tb.t0, q, r, wc[0]), d2f = mvc<BW>(tb.t2, q, r, wc[0]);
@@ -402,9 +404,9 @@ __device__ __forceinline__ void helmholtz_role(const SplitArgs &a, const Tabs<BW
 //     (solve_v_f.f90:140-153, the LU of solve_g.f90:42-71);
 //   (D2 - k^2 D0) v_p = phi_p with the wall velocities at rows 1 and n, and v_h = phi_h with zero
 //     walls (solve_v_f.f90:202-272).
-template <int BW, typename PT>
+template <int BW, typename PT, int SA>
 __device__ __forceinline__ void helmholtz_phi_v(const SplitArgs &a, const Tabs<BW> &tb, int64_t m,
-                                                const Ring<kHelmUnits<BW>> &ring) {
+                                                const Ring<kHelmUnits<BW>, SA + 1> &ring) {
   const int n = a.ny, s = a.substep;
   const int64_t nm = a.nmodes, ns = a.ns;
   const double dt = *a.dt_ptr, nu = a.nu;
@@ -440,7 +442,7 @@ __device__ __forceinline__ void helmholtz_phi_v(const SplitArgs &a, const Tabs<B
     return zadd(zadd(zscale(zeta, h), zscale(1.0 - alpha * k2, f)), zscale(alpha, d2f));
   };
   // phi forward units: 0 store, 1..3 HV0, V2, V3, 4 D2 store (substep 1)
-  lu_fwd<BW, 1, 1, kStageAhead, true>(n, [&](int r, double *rw, bool c) { helm_row<BW>(tb, r, n, dummy, beta, rw, c); },
+  lu_fwd<BW, 1, 1, SA, true>(n, [&](int r, double *rw, bool c) { helm_row<BW>(tb, r, n, dummy, beta, rw, c); },
       [&](int r, double2 *bc, double *br) {
         const double2 h = zadd(rh(r, 1), zadd(rh(r, 2), rh(r, 3)));
         bc[0] = rhs(ring.c(r, 0), h, s == 1 ? ring.c(r, 4) : z2(0.0, 0.0), r);
@@ -460,7 +462,7 @@ __device__ __forceinline__ void helmholtz_phi_v(const SplitArgs &a, const Tabs<B
       });
   // phi backward units: 0 Z(r), 1 Xz(r), 2..BW+1 U(r, e), BW+2..BW+4 HV0, V2, V3 at q = r + BW
   const DLine out{a.zl + 4 * ns + m, nm};
-  bwd_emit<BW, 1, 1, kStageAhead, true>(n, [&](int r, int e) { return e <= BW ? ring.d(r, 1 + e) : ub.get(r, e); },
+  bwd_emit<BW, 1, 1, SA, true>(n, [&](int r, int e) { return e <= BW ? ring.d(r, 1 + e) : ub.get(r, e); },
       [&](int r, double2 *zc, double *zr) {
         zc[0] = ring.c(r, 0);
         zr[0] = ring.d(r, 1);
@@ -510,7 +512,7 @@ __device__ __forceinline__ void helmholtz_phi_v(const SplitArgs &a, const Tabs<B
   const LBand<BW> vl = make_lband<BW>(a.vf + m, nm, ns, n);
   const UBand<BW> vu = make_uband<BW>(a.vf + a.vf_l + m, nm, ns);
   // v forward units: 0 phi_p(r), 1 phi_h(r), 2..BW+2 L(r, r-d) for d = 0..BW
-  fwd_lband<BW, 1, 1, kStageAhead, true>([&](int r, int d) { return d <= BW ? ring.d(r, 2 + d) : vl.get(r, d); }, n,
+  fwd_lband<BW, 1, 1, SA, true>([&](int r, int d) { return d <= BW ? ring.d(r, 2 + d) : vl.get(r, d); }, n,
       [&](int r, double2 *bc, double *br) {
         const bool wall = (r == 1 || r == n);
         bc[0] = (r == 1) ? vlo : (r == n) ? vhi : ring.c(r, 0);
@@ -529,7 +531,7 @@ __device__ __forceinline__ void helmholtz_phi_v(const SplitArgs &a, const Tabs<B
   // v backward units: 0 Z(r), 1 Xz(r), 2..BW+1 U(r, e)
   const DLine Sv{a.S + ns + m, nm}, Sw{a.S + 2 * ns + m, nm};
   double dh1 = 0.0, dhn = 0.0;
-  bwd_emit<BW, 1, 1, kStageAhead, true>(n, [&](int r, int e) { return e <= BW ? ring.d(r, 1 + e) : vu.get(r, e); },
+  bwd_emit<BW, 1, 1, SA, true>(n, [&](int r, int e) { return e <= BW ? ring.d(r, 1 + e) : vu.get(r, e); },
       [&](int r, double2 *zc, double *zr) {
         zc[0] = ring.c(r, 0);
         zr[0] = ring.d(r, 1);
@@ -580,35 +582,39 @@ __global__ void __launch_bounds__(128) k_vop_factor(SplitArgs a) {
 // Three roles per mode: theta, g, and phi with v (helmholtz_phi_v); a fourth for a second scalar.
 constexpr int kHelmRoles = 3;
 
-template <int BW, int NS = 1>
+// Staging ring bytes of one 32-mode group (NS scalars, SA steps of look-ahead).
+template <int BW, int NS = 1, int SA = 1>
 constexpr size_t helm_smem() {
-  return sizeof(double2) * (size_t)kStageSlots * kHelmUnits<BW> * kLanes * (kHelmRoles + NS - 1);
+  return sizeof(double2) * (size_t)(SA + 1) * kHelmUnits<BW> * kLanes * (kHelmRoles + NS - 1);
 }
 
 // With a fourth role (a second scalar) three resident blocks keep the 168 registers of one
 // scalar's kernel; four would cap it at 128 and spill.
-// One scalar: up to two 32-mode groups per block (Tuning::groups); the bound keeps 168 registers.
-template <int BW, typename PT, int NS>
-__global__ void __launch_bounds__(NS == 1 ? 2 * kLanes * kHelmRoles : kLanes * (kHelmRoles + 1), NS == 1 ? 2 : 3)
+// One scalar: 1, 2 or 4 32-mode groups per block (Tuning::hgroups) and 1 or 2 steps of staging
+// look-ahead (Tuning::stage); the bound (384 threads) keeps 168 registers.  Four groups with the
+// tables in shared memory and two steps of look-ahead hold 218 KB at ny = 129, one block (12
+// warps) per SM.
+template <int BW, typename PT, int NS, int SA>
+__global__ void __launch_bounds__(NS == 1 ? 4 * kLanes * kHelmRoles : kLanes * (kHelmRoles + 1), NS == 1 ? 1 : 3)
 k_helmholtz(SplitArgs a) {
   extern __shared__ double2 helm_ring[];
   if (a.dsc->err) return;  // a failed dt update leaves the state untouched (uniform over the block)
   constexpr int R = kHelmRoles + NS - 1;
   const int role = (threadIdx.x / kLanes) % R, grp = threadIdx.x / (kLanes * R);
-  const int64_t m = ((int64_t)blockIdx.x * a.groups + grp) * kLanes + (threadIdx.x % kLanes);
+  const int64_t m = ((int64_t)blockIdx.x * a.hgroups + grp) * kLanes + (threadIdx.x % kLanes);
   // T0, T1, T2 (after the staging ring when in shared memory)
   const double *t0 = a.tabs;
-  if (a.stab)
-    t0 = tabs_to_shared<BW>(a, 0, reinterpret_cast<double *>(helm_ring + kStageSlots * kHelmUnits<BW> * blockDim.x));
+  if (a.hstab)
+    t0 = tabs_to_shared<BW>(a, 0, reinterpret_cast<double *>(helm_ring + (SA + 1) * kHelmUnits<BW> * blockDim.x));
   if (m == 0 || m >= a.nmodes) return;
   const Tabs<BW> tb = tabs_at<BW>(t0, a.ny);  // (its L0 and U0 are not read here)
-  const Ring<kHelmUnits<BW>> ring{helm_ring + threadIdx.x, (int)blockDim.x};
+  const Ring<kHelmUnits<BW>, SA + 1> ring{helm_ring + threadIdx.x, (int)blockDim.x};
   switch (role) {
-    case 0: helmholtz_role<BW, 0, PT>(a, tb, m, ring); break;
-    case 1: helmholtz_role<BW, 1, PT>(a, tb, m, ring); break;
-    case 2: helmholtz_phi_v<BW, PT>(a, tb, m, ring); break;
+    case 0: helmholtz_role<BW, 0, PT, SA>(a, tb, m, ring); break;
+    case 1: helmholtz_role<BW, 1, PT, SA>(a, tb, m, ring); break;
+    case 2: helmholtz_phi_v<BW, PT, SA>(a, tb, m, ring); break;
     default:
-      if constexpr (NS == 2) helmholtz_role<BW, 3, PT>(a, tb, m, ring);
+      if constexpr (NS == 2) helmholtz_role<BW, 3, PT, SA>(a, tb, m, ring);
       break;
   }
 }
@@ -839,8 +845,10 @@ cudaError_t split_bw(Handle &h, int part, int substep, const double *dt_ptr, cud
   a.vf = h.vf;
   a.vf_l = vop_lband_doubles(h);
   a.groups = h.nsc == 1 ? h.tune.groups : 1;
+  a.hgroups = h.nsc == 1 ? h.tune.hgroups : 1;
   a.ulayout = h.tune.ulayout;
   a.stab = h.tune.stab;
+  a.hstab = h.tune.hstab;
 
   MeanArgs ma;
   ma.ny = h.ny;
@@ -868,7 +876,7 @@ cudaError_t split_bw(Handle &h, int part, int substep, const double *dt_ptr, cud
   cudaError_t e;
   const int G = a.groups;
   const unsigned blocks = (unsigned)((h.nmodes + (int64_t)kLanes * G - 1) / ((int64_t)kLanes * G));
-  const size_t tsm = a.stab ? solver_tables_bytes(h) : 0;
+  const size_t tsm = a.stab ? solver_tables_bytes(h) : 0, htsm = a.hstab ? solver_tables_bytes(h) : 0;
   if (part == 0) {
     // the mean lines touch only mode 0, which the split kernels skip: run them beside those
     if ((e = cudaEventRecord(h.ev_fork, st)) != cudaSuccess) return e;
@@ -889,20 +897,28 @@ cudaError_t split_bw(Handle &h, int part, int substep, const double *dt_ptr, cud
   if (part == 1) {
     if (h.nsc == 2) {
       constexpr int nt = kLanes * (kHelmRoles + 1);
-      if (h.mixed) k_helmholtz<BW, float2, 2><<<blocks, nt, helm_smem<BW, 2>() + tsm, st>>>(a);
-      else k_helmholtz<BW, double2, 2><<<blocks, nt, helm_smem<BW, 2>() + tsm, st>>>(a);
+      if (h.mixed) k_helmholtz<BW, float2, 2, 1><<<blocks, nt, helm_smem<BW, 2>() + htsm, st>>>(a);
+      else k_helmholtz<BW, double2, 2, 1><<<blocks, nt, helm_smem<BW, 2>() + htsm, st>>>(a);
     } else {
-      const size_t sm = G * helm_smem<BW>() + tsm;
-      if (h.mixed) k_helmholtz<BW, float2, 1><<<blocks, kLanes * kHelmRoles * G, sm, st>>>(a);
-      else k_helmholtz<BW, double2, 1><<<blocks, kLanes * kHelmRoles * G, sm, st>>>(a);
+      const int HG = a.hgroups;
+      const unsigned hb = (unsigned)((h.nmodes + (int64_t)kLanes * HG - 1) / ((int64_t)kLanes * HG));
+      const int nt = kLanes * kHelmRoles * HG;
+      if (h.tune.stage == 2) {
+        const size_t sm = HG * helm_smem<BW, 1, 2>() + htsm;
+        if (h.mixed) k_helmholtz<BW, float2, 1, 2><<<hb, nt, sm, st>>>(a);
+        else k_helmholtz<BW, double2, 1, 2><<<hb, nt, sm, st>>>(a);
+      } else {
+        const size_t sm = HG * helm_smem<BW>() + htsm;
+        if (h.mixed) k_helmholtz<BW, float2, 1, 1><<<hb, nt, sm, st>>>(a);
+        else k_helmholtz<BW, double2, 1, 1><<<hb, nt, sm, st>>>(a);
+      }
     }
     return cudaGetLastError();
   }
   const int at = h.tune.asm_threads;
   const dim3 agrid((unsigned)((h.nmodes + at - 1) / at), (unsigned)h.ny);
   k_assemble<<<agrid, at, 0, st>>>(a);
-  if ((e = cudaGetLastError()) != cudaSuccess) return e;
-  return cudaStreamWaitEvent(st, h.ev_join, 0);
+  return cudaGetLastError();
 }
 
 cudaError_t split_part(Handle &h, int part, int substep, const double *dt_ptr, cudaStream_t st) {
@@ -934,10 +950,12 @@ namespace {
 template <int BW>
 cudaError_t set_smem_limit_bw(int bytes) {
   auto lim = [bytes](auto kern) { return cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes); };
-  cudaError_t e = lim(k_helmholtz<BW, float2, 1>);
-  if (e == cudaSuccess) e = lim(k_helmholtz<BW, double2, 1>);
-  if (e == cudaSuccess) e = lim(k_helmholtz<BW, float2, 2>);
-  if (e == cudaSuccess) e = lim(k_helmholtz<BW, double2, 2>);
+  cudaError_t e = lim(k_helmholtz<BW, float2, 1, 1>);
+  if (e == cudaSuccess) e = lim(k_helmholtz<BW, double2, 1, 1>);
+  if (e == cudaSuccess) e = lim(k_helmholtz<BW, float2, 1, 2>);
+  if (e == cudaSuccess) e = lim(k_helmholtz<BW, double2, 1, 2>);
+  if (e == cudaSuccess) e = lim(k_helmholtz<BW, float2, 2, 1>);
+  if (e == cudaSuccess) e = lim(k_helmholtz<BW, double2, 2, 1>);
   if (e == cudaSuccess) e = lim(k_hvhg<BW, float2, 1>);
   if (e == cudaSuccess) e = lim(k_hvhg<BW, double2, 1>);
   if (e == cudaSuccess) e = lim(k_hvhg<BW, float2, 2>);
@@ -961,31 +979,53 @@ cudaError_t set_solver_smem_limits(const Handle &h) {
   }
 }
 
-size_t helm_ring_bytes(const Handle &h, int groups) {
-  const size_t per = sizeof(double2) * (size_t)kStageSlots * (5 + h.bw) * kLanes;  // kHelmUnits<BW>
-  return per * (h.nsc == 2 ? kHelmRoles + 1 : (size_t)kHelmRoles * groups);
+size_t helm_ring_bytes(const Handle &h, int hgroups, int stage) {
+  const size_t per = sizeof(double2) * (size_t)(stage + 1) * (5 + h.bw) * kLanes;  // kHelmUnits<BW>
+  return per * (h.nsc == 2 ? kHelmRoles + 1 : (size_t)kHelmRoles * hgroups);
+}
+
+int device_attr(cudaDeviceAttr attr) {
+  int dev = 0, v = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&v, attr, dev) != cudaSuccess) return 0;
+  return v;
 }
 
 }  // namespace
 
 size_t solver_tables_bytes(const Handle &h) { return sizeof(double) * 3 * (size_t)h.ny * (4 * h.bw + 1); }
 
-bool solver_tables_fit(const Handle &h, int groups) {
-  int dev = 0, optin = 0;
-  if (cudaGetDevice(&dev) != cudaSuccess ||
-      cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) != cudaSuccess)
-    return false;
-  return helm_ring_bytes(h, groups) + solver_tables_bytes(h) <= (size_t)optin;
+bool hvhg_tables_fit(const Handle &h) {
+  return solver_tables_bytes(h) <= (size_t)device_attr(cudaDevAttrMaxSharedMemoryPerBlockOptin);
 }
 
-bool solver_tables_default(const Handle &h) {
-  int dev = 0, per_sm = 0;
-  if (h.nsc != 1 || cudaGetDevice(&dev) != cudaSuccess ||
-      cudaDeviceGetAttribute(&per_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev) != cudaSuccess)
-    return false;
-  // two resident blocks of 64 modes (the one wave of 12 warps per SM the kernel has without the
-  // tables), with the 1 KB the runtime reserves per block
-  return 2 * (helm_ring_bytes(h, 2) + solver_tables_bytes(h) + 1024) <= (size_t)per_sm;
+bool helm_shape_fits(const Handle &h, int hgroups, int hstab, int stage) {
+  if (h.nsc == 2 && (hgroups != 1 || stage != 1)) return false;
+  const size_t bytes = helm_ring_bytes(h, hgroups, stage) + (hstab ? solver_tables_bytes(h) : 0);
+  return bytes <= (size_t)device_attr(cudaDevAttrMaxSharedMemoryPerBlockOptin);
+}
+
+void default_solver_shapes(Handle &h) {
+  // k_hvhg: 32-mode blocks reading the tables through L1 (what the tuner measured as fastest
+  // or even with the alternatives at 192x129x192).  k_helmholtz: the largest blocks that still
+  // put a block on nearly every SM, with the tables in shared memory and two steps of staging
+  // look-ahead where a block holds them; else 64-mode blocks with the tables where two fit on
+  // an SM; else 32-mode blocks reading the tables through L1.
+  h.tune.groups = 1;
+  h.tune.stab = 0;
+  h.tune.hgroups = 1;
+  h.tune.hstab = 0;
+  h.tune.stage = 1;
+  if (h.nsc != 1) return;
+  const int sms = device_attr(cudaDevAttrMultiProcessorCount);
+  const size_t per_sm = (size_t)device_attr(cudaDevAttrMaxSharedMemoryPerMultiprocessor);
+  if (h.nmodes >= (int64_t)kLanes * 4 * sms * 9 / 10 && helm_shape_fits(h, 4, 1, 2)) {
+    h.tune.hgroups = 4;
+    h.tune.hstab = 1;
+    h.tune.stage = 2;
+  } else if (2 * (helm_ring_bytes(h, 2, 1) + solver_tables_bytes(h) + 1024) <= per_sm) {
+    h.tune.hgroups = 2;
+    h.tune.hstab = 1;
+  }
 }
 
 cudaError_t launch_vop_factor(Handle &h, cudaStream_t st) {
@@ -1026,8 +1066,15 @@ cudaError_t launch_ws_helmholtz(Handle &h, int substep, const double *dt_ptr, cu
   return split_part(h, 1, substep, dt_ptr, st);
 }
 
-cudaError_t launch_ws_assemble(Handle &h, int substep, const double *dt_ptr, cudaStream_t st) {
+cudaError_t launch_ws_assemble_only(Handle &h, int substep, const double *dt_ptr, cudaStream_t st) {
   return split_part(h, 2, substep, dt_ptr, st);
+}
+
+cudaError_t launch_ws_join(Handle &h, cudaStream_t st) { return cudaStreamWaitEvent(st, h.ev_join, 0); }
+
+cudaError_t launch_ws_assemble(Handle &h, int substep, const double *dt_ptr, cudaStream_t st) {
+  cudaError_t e = launch_ws_assemble_only(h, substep, dt_ptr, st);
+  return e == cudaSuccess ? launch_ws_join(h, st) : e;
 }
 
 cudaError_t launch_wavespace_split(Handle &h, int substep, const double *dt_ptr, cudaStream_t st) {

@@ -98,19 +98,24 @@ typedef struct kmm_tuning {
   int32_t z_lines_per_block;  /* z transforms (y_to_x, x_to_y): kx lines a block transforms */
   int32_t x_rows_per_block;   /* x pass (dft_x_realspace): z rows a block takes */
   int32_t x_threads;          /*   and its threads */
-  int32_t modes_per_block;    /* (kx, kz) systems a block of the hvhg and Helmholtz solvers takes */
+  int32_t modes_per_block;    /* (kx, kz) systems a block of the hvhg solver takes (32, 64) */
   int32_t u_layout;           /* U factor storage: 0 = [offset][y][mode], 1 = [y][offset][mode] */
   int32_t assemble_threads;   /* threads per block of the C1/C2 assembly */
   int32_t tuned;              /* 1 once kmm_autotune has run */
-  int32_t tables_shared;      /* 1: the hvhg and Helmholtz solvers copy the B-spline operator
-                                 tables they read into shared memory first */
+  int32_t tables_shared;      /* 1: the hvhg solver copies the B-spline operator tables it reads
+                                 into shared memory first */
+  int32_t helm_modes_per_block;  /* systems a block of the Helmholtz solver takes (32, 64, 128) */
+  int32_t helm_tables_shared;    /* 1: the Helmholtz solver reads the tables from shared memory */
+  int32_t helm_stage_ahead;      /* rows its sweeps stage ahead through shared memory (1, 2) */
+  int32_t reserved;
   double ms_z[3];             /* zinv + zfwd per z variant */
   double ms_x[3];             /* x pass per x variant */
-  double ms_modes[2];         /* hvhg + Helmholtz at 32 and 64 modes per block (best tables choice) */
-  double ms_layout[2];        /* hvhg + Helmholtz per U layout */
+  double ms_modes[2];         /* hvhg at 32 and 64 modes per block (best tables choice) */
+  double ms_layout[2];        /* Helmholtz per U layout */
   double ms_assemble[3];      /* assembly at 128, 256, 512 threads */
-  double ms_tables[2];        /* hvhg + Helmholtz with the tables read through L1 / from shared
-                                 memory (best modes per block; 0 where they do not fit) */
+  double ms_tables[2];        /* hvhg with the tables read through L1 / from shared memory */
+  double ms_helm[12];         /* Helmholtz at [32, 64, 128 modes][tables via L1, shared]
+                                 [look-ahead 1, 2] (row-major; 0 where a shape does not fit) */
 } kmm_tuning;
 
 typedef struct kmm_handle kmm_handle;
@@ -241,7 +246,8 @@ int kmm_set_tuning(kmm_handle *h, const kmm_tuning *t);
 #define KMM_K_ZFWD 4        /* x_to_y: z forward transform of the 8 products (+ rescale) */
 #define KMM_K_HVHG 5        /* wavespace part 1: control probe, mean-mode fork, hvhg D0 solves */
 #define KMM_K_HELMHOLTZ 6   /* wavespace part 2: theta, g, phi and v Helmholtz solves */
-#define KMM_K_ASSEMBLE 7    /* wavespace part 3: C1/C2 assembly, u and w, mean-mode join */
+#define KMM_K_ASSEMBLE 7    /* wavespace part 3: C1/C2 assembly, u and w (the join of the mean-mode
+                               lines, which run beside the solver kernels, is outside every id) */
 
 /* Runs nsteps RK3 steps launching kernel by kernel with a CUDA event pair around every
  * launch on the handle's stream; ms[k] = mean device time per launch of kernel k,

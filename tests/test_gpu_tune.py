@@ -35,8 +35,11 @@ def test_every_candidate_shape_is_bit_identical(precision):
     cases = [dict(z_lines_per_block=z) for z in z_lines]
     cases += [dict(x_rows_per_block=r, x_threads=t) for r, t in x_shapes]
     cases += [dict(modes_per_block=64), dict(u_layout=1), dict(assemble_threads=128), dict(assemble_threads=512)]
-    # the operator tables through L1 or from shared memory, at both block sizes
+    # hvhg: the operator tables through L1 or from shared memory, at both block sizes
     cases += [dict(modes_per_block=mb, tables_shared=ts) for mb in (32, 64) for ts in (0, 1)]
+    # Helmholtz: block size x tables x staging look-ahead
+    cases += [dict(helm_modes_per_block=mb, helm_tables_shared=ts, helm_stage_ahead=sa)
+              for mb in (32, 64, 128) for ts in (0, 1) for sa in (1, 2)]
     for case in cases:
         got = _run(cfg, U, case)
         for f in STATE_SLOTS:
@@ -63,7 +66,11 @@ def test_autotune_keeps_the_state_and_reports_its_choice():
         assert np.array_equal(got[f], ref[f]), f
     assert t["tuned"] == 1 and t["modes_per_block"] in (32, 64) and t["assemble_threads"] in (128, 256, 512)
     assert all(x > 0 for x in rep["ms_z"] + rep["ms_x"] + rep["ms_modes"] + rep["ms_assemble"] + rep["ms_tables"])
-    assert t["tables_shared"] in (0, 1)
+    assert t["tables_shared"] in (0, 1) and t["helm_stage_ahead"] in (1, 2)
+    # every Helmholtz shape that fits this grid was timed, and the chosen one is the fastest
+    helm = [x for x in rep["ms_helm"] if x > 0]
+    assert len(helm) >= 8 and min(helm) == rep["ms_layout"][0]
+    assert t["helm_modes_per_block"] in (32, 64, 128)
     with pytest.raises(KmmError) as e:
         with Channel(cfg) as ch:
             ch.set_tuning(z_lines_per_block=7)
