@@ -247,6 +247,7 @@ int check_device_error(Handle &h, int err) {
   KMM_CUDA(cudaMemcpy(&h.dsc->err, &zero, sizeof(int), cudaMemcpyHostToDevice));
   if (err == KMM_ERR_DT) set_error("ABORT due to timestep dt (dt <= 1e-14 or dt > 1e5)");
   else if (err == KMM_ERR_NONFINITE) set_error("non-finite velocity in the physical-space step");
+  else if (err == KMM_ERR_TIMEOUT) set_error("a bounded device wait gave up: a TMA tile copy of the z transforms did not complete");
   else set_error("device error " + std::to_string(err));
   return err;
 }
@@ -560,6 +561,9 @@ int kmm_create(const kmm_config *cfg, kmm_handle **out) {
     }
   }
   default_solver_shapes(*h);  // the untuned solver launch shapes
+  // the z transforms stage their input tiles through TMA where the grid allows the tile map
+  // (0.062 -> 0.054 ms y_to_x, 312 -> 315 steps/s at 192x129x192 mixed, same-box A/B)
+  h->tune.ztma = z_tma_possible(*h, h->tune.z) ? 1 : 0;
   if (cfg->autotune && (rc = autotune(*h, nullptr))) return fail(rc);
   *out = reinterpret_cast<kmm_handle *>(h);
   return KMM_OK;

@@ -82,6 +82,7 @@ struct Adjoint;
 // Launch shapes the autotuner (kmm_autotune, tune.cu) chooses; the defaults are the hand-tuned ones.
 struct Tuning {
   int z = 0;              // z-transform variant (lines per block, transforms2.cu ZVar)
+  int ztma = 0;           // 1: the z transforms stage each block's input tile through TMA
   int x = 0;              // x-pass variant (rows per block and threads, XVar)
   int groups = 1;         // 32-mode groups per block of the hvhg kernel (1 or 2)
   int hgroups = 1;        // 32-mode groups per block of the Helmholtz kernel (1, 2 or 4)
@@ -94,6 +95,7 @@ struct Tuning {
   // device ms of every candidate of the last autotune (kmm_tuning's ms_* fields)
   double ms_z[3] = {}, ms_x[3] = {}, ms_modes[2] = {}, ms_layout[2] = {}, ms_assemble[3] = {}, ms_tables[2] = {};
   double ms_helm[3][2][2] = {};  // [32/64/128 modes][tables via L1 / shared][look-ahead 1 / 2]
+  double ms_z_tma[3] = {};       // the z variants with TMA-staged input tiles
 };
 
 struct Handle {
@@ -259,6 +261,9 @@ int64_t split_ub_role(const Handle &h);
 // whether hvhg's block holds them) and the Helmholtz shapes a block can hold (groups, tables,
 // look-ahead); default_solver_shapes sets a new handle's solver shapes.
 size_t solver_tables_bytes(const Handle &h);
+// Whether the z transforms of variant zvar can stage their input tiles through TMA on this grid
+// (four-step length, tile within the shared-memory limit, tile map accepted by the encoder).
+bool z_tma_possible(const Handle &h, int zvar);
 bool hvhg_tables_fit(const Handle &h);
 bool helm_shape_fits(const Handle &h, int hgroups, int hstab, int stage);
 void default_solver_shapes(Handle &h);

@@ -6,6 +6,7 @@
 // are line-major in shared memory with the odd leading dimension (N1+1)*N2 | 1 and are
 // transformed in place (fft4_ip), natural order in and out, so the 3/2 padding and truncation
 // read and write plain positions k and N - k.
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include "fft2.cuh"
@@ -34,33 +35,131 @@ constexpr int z_threads() {
 // kz index for p < nz/2 and p > nz, -1 for the zero band nz/2..nz.
 __device__ __forceinline__ int zpad_src(int p, int nh) { return p < nh ? p : (p > 2 * nh ? p - nh : -1); }
 
+// ---- TMA staging of the z-transform input tiles (cp.async.bulk.tensor, no multicast) -------
+// A block's input tile (its KB kx columns of all rows of one (field, y) plane) is copied into
+// shared memory as 3-D tensor boxes of (2 KB scalars, tile_rows(n) rows, 1 plane); the copies
+// complete on an mbarrier whose wait has an iteration limit.
+constexpr int kTmaWaitIters = 1 << 20;
+
+// Rows of one TMA box over n rows: n split into ceil(n / 256) equal boxes (0 if they are not equal).
+__host__ __device__ constexpr int tile_rows(int n) {
+  const int nb = (n + 255) / 256;
+  return n % nb == 0 ? n / nb : 0;
+}
+
+__device__ __forceinline__ unsigned smem_u32(const void *p) { return (unsigned)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ void mbar_init(uint64_t *bar, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, unsigned phase) {
+  unsigned ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(phase)
+      : "memory");
+  return ok != 0;
+}
+// bounded wait for phase 0 of `bar`; false if it gave up
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar) {
+  for (int it = 0; it < kTmaWaitIters; ++it)
+    if (mbar_try_wait(bar, 0)) return true;
+  return false;
+}
+__device__ __forceinline__ void tma_load_3d(void *dst, const CUtensorMap *map, int x, int y, int z, uint64_t *bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];"
+      ::"r"(smem_u32(dst)), "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(z), "r"(smem_u32(bar))
+      : "memory");
+}
+
+// Copies a block's tile (KB columns x n rows of element E) into `base`, in tile_rows(n)-row boxes,
+// and waits for it.  Thread 0 arms the barrier and issues the copies; every thread waits (the
+// completed phase makes the bytes visible to it).  Returns false, for the whole block, if the
+// wait gave up: the error flag is set and the block should leave.
+template <typename E, int KB>
+__device__ __forceinline__ bool tma_tile(unsigned char *base, const CUtensorMap *map, int n, int x, int plane,
+                                         uint64_t *bar, int *err) {
+  if (threadIdx.x == 0) mbar_init(bar, 1);
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    const int rows = tile_rows(n);
+    mbar_expect_tx(bar, (unsigned)(KB * n * sizeof(E)));
+    for (int r0 = 0; r0 < n; r0 += rows) tma_load_3d(base + (size_t)r0 * KB * sizeof(E), map, x, r0, plane, bar);
+  }
+  const bool ok = mbar_wait_bounded(bar);
+  if (__syncthreads_or(!ok)) {
+    // the copy did not complete: flag it and give it one more bounded wait before the block leaves
+    if (threadIdx.x == 0) atomicCAS(err, 0, KMM_ERR_TIMEOUT);
+    mbar_wait_bounded(bar);
+    return false;
+  }
+  return true;
+}
+
+// Dynamic shared memory of a z kernel with TMA: the larger of the tile and the FFT lines (the lines
+// overlay the tile once every thread has taken its inputs), plus 128 bytes so that the tile can
+// start on a 128-byte shared address.
+template <typename R, int N1, int N2, int KB, typename E>
+constexpr size_t z_smem_tma(int n) {
+  const size_t tile = (size_t)KB * n * sizeof(E);
+  const size_t lines = (size_t)KB * ip_lda<N1, N2>() * sizeof(typename Cpx<R>::T);
+  return (tile > lines ? tile : lines) + 128;
+}
+
 // y_to_x: grid (ceil(nxh/KB), ny, nfield).  Thread (l, n1) of step 1 reads its N2 points
 // x[n1 + N1*n2] of kx line l straight from the Y-pencil (16 consecutive kx per row: one coalesced
-// run), transforms them in registers and leaves them in shared memory; thread (l, k2) of step 2
-// finishes the line and writes X[k2 + N2*k1] straight into the X-pencil slab.
-template <typename R, int N1, int N2, int KB>
+// run) or, with TMA, from the block's tile in shared memory, transforms them in registers and
+// leaves them in shared memory; thread (l, k2) of step 2 finishes the line and writes
+// X[k2 + N2*k1] straight into the X-pencil slab.
+template <typename R, int N1, int N2, int KB, bool TMA = false>
 __global__ void __launch_bounds__(z_threads<N1, N2, KB>()) k_zinv2(const double2 *__restrict__ src,
                                                                   typename Cpx<R>::T *__restrict__ dst,
                                                                   FftPlan pl, int nz, int nxh, int64_t ns,
-                                                                  int64_t nm) {
+                                                                  int64_t nm, const __grid_constant__ CUtensorMap tmap,
+                                                                  int ny, int *err) {
   using C = typename Cpx<R>::T;
   constexpr int N = N1 * N2, LD = ip_lda<N1, N2>();
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  C *a = reinterpret_cast<C *>(smem_raw);
+  // with TMA the tile (and the lines over it) starts on the next 128-byte shared address
+  unsigned char *base = TMA ? smem_raw + ((128u - (smem_u32(smem_raw) & 127u)) & 127u) : smem_raw;
+  C *a = reinterpret_cast<C *>(base);
   const int nh = nz / 2;
   const int kx0 = blockIdx.x * KB, y = blockIdx.y, f = blockIdx.z;
   const int l = threadIdx.x % KB, item = threadIdx.x / KB;
   const bool live = kx0 + l < nxh;
   const C *tw = tw_of<R>(pl);
+  C v[N2];
+  if constexpr (TMA) {
+    __shared__ __align__(8) uint64_t bar;
+    if (!tma_tile<double2, KB>(base, &tmap, nz, 2 * kx0, f * ny + y, &bar, err)) return;
+    const double2 *tile = reinterpret_cast<const double2 *>(base);
+    if (item < N1) {
+      const int n1 = item;
+#pragma unroll
+      for (int n2 = 0; n2 < N2; ++n2) {
+        const int kzi = zpad_src(n1 + N1 * n2, nh);
+        v[n2] = (live && kzi >= 0) ? ld_as<C>(tile + kzi * KB + l) : cmake<C>(0.0, 0.0);
+      }
+    }
+    __syncthreads();  // the FFT lines overlay the tile
+  } else {
+    if (item < N1) {
+      const int n1 = item;
+      const double2 *sp = src + f * ns + (int64_t)y * nz * nxh + kx0 + l;
+#pragma unroll
+      for (int n2 = 0; n2 < N2; ++n2) {
+        const int kzi = zpad_src(n1 + N1 * n2, nh);
+        v[n2] = (live && kzi >= 0) ? ld_as<C>(sp + (int64_t)kzi * nxh) : cmake<C>(0.0, 0.0);
+      }
+    }
+  }
   if (item < N1) {
     const int n1 = item;
-    const double2 *sp = src + f * ns + (int64_t)y * nz * nxh + kx0 + l;
-    C v[N2];
-#pragma unroll
-    for (int n2 = 0; n2 < N2; ++n2) {
-      const int kzi = zpad_src(n1 + N1 * n2, nh);
-      v[n2] = (live && kzi >= 0) ? ld_as<C>(sp + (int64_t)kzi * nxh) : cmake<C>(0.0, 0.0);
-    }
     reg_dft<C, N2>(v, +1);
     C *yl = a + l * LD;
     yl[n1] = v[0];
@@ -88,25 +187,45 @@ __global__ void __launch_bounds__(z_threads<N1, N2, KB>()) k_zinv2(const double2
 // x_to_y: grid (ceil(nxh/KB), ny, nfield).  The mirror of k_zinv2: step 1 reads the X-pencil
 // slab, step 2 writes the kept frequencies (truncation of ppdfftw_dft_z_forward,
 // module_ppdfftw.f90:811-817) with the kz Nyquist row zeroed and the rescale folded in.
-template <typename R, int N1, int N2, int KB, typename D>
+// With TMA, step 1 takes its points from the block's tile of the slab (KB kx columns of the N
+// rows of one (field, y) plane), which the FFT lines then overlay.
+template <typename R, int N1, int N2, int KB, typename D, bool TMA = false>
 __global__ void __launch_bounds__(z_threads<N1, N2, KB>()) k_zfwd2(const typename Cpx<R>::T *__restrict__ src,
                                                                   D *__restrict__ dst, FftPlan pl, int nz, int nxh,
-                                                                  int64_t ns, int64_t nm, double scale) {
+                                                                  int64_t ns, int64_t nm, double scale,
+                                                                  const __grid_constant__ CUtensorMap tmap, int ny,
+                                                                  int *err) {
   using C = typename Cpx<R>::T;
   constexpr int N = N1 * N2, LD = ip_lda<N1, N2>();
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  C *a = reinterpret_cast<C *>(smem_raw);
+  unsigned char *base = TMA ? smem_raw + ((128u - (smem_u32(smem_raw) & 127u)) & 127u) : smem_raw;
+  C *a = reinterpret_cast<C *>(base);
   const int nh = nz / 2;
   const int kx0 = blockIdx.x * KB, y = blockIdx.y, f = blockIdx.z;
   const int l = threadIdx.x % KB, item = threadIdx.x / KB;
   const bool live = kx0 + l < nxh;
   const C *tw = tw_of<R>(pl);
+  C v[N2];
+  if constexpr (TMA) {
+    __shared__ __align__(8) uint64_t bar;
+    if (!tma_tile<C, KB>(base, &tmap, N, 2 * kx0, f * ny + y, &bar, err)) return;
+    const C *tile = reinterpret_cast<const C *>(base);
+    if (item < N1) {
+      const int n1 = item;
+#pragma unroll
+      for (int n2 = 0; n2 < N2; ++n2) v[n2] = live ? tile[(n1 + N1 * n2) * KB + l] : cmake<C>(0.0, 0.0);
+    }
+    __syncthreads();  // the FFT lines overlay the tile
+  } else {
+    if (item < N1) {
+      const int n1 = item;
+      const C *sp = src + f * nm + (int64_t)y * N * nxh + kx0 + l;
+#pragma unroll
+      for (int n2 = 0; n2 < N2; ++n2) v[n2] = live ? sp[(int64_t)(n1 + N1 * n2) * nxh] : cmake<C>(0.0, 0.0);
+    }
+  }
   if (item < N1) {
     const int n1 = item;
-    const C *sp = src + f * nm + (int64_t)y * N * nxh + kx0 + l;
-    C v[N2];
-#pragma unroll
-    for (int n2 = 0; n2 < N2; ++n2) v[n2] = live ? sp[(int64_t)(n1 + N1 * n2) * nxh] : cmake<C>(0.0, 0.0);
     reg_dft<C, N2>(v, -1);
     C *yl = a + l * LD;
     yl[n1] = v[0];
@@ -514,6 +633,11 @@ cudaError_t prepare_transforms2() {
           set_smem(k_zfwd2<double, N1, N2, ZD::KB, double2>, optin);
           set_smem(k_zfwd2<float, N1, N2, ZF::KB, float2>, optin);
           set_smem(k_zfwd2<float, N1, N2, ZF::KB, double2>, optin);
+          set_smem(k_zinv2<double, N1, N2, ZD::KB, true>, optin);
+          set_smem(k_zinv2<float, N1, N2, ZF::KB, true>, optin);
+          set_smem(k_zfwd2<double, N1, N2, ZD::KB, double2, true>, optin);
+          set_smem(k_zfwd2<float, N1, N2, ZF::KB, float2, true>, optin);
+          set_smem(k_zfwd2<float, N1, N2, ZF::KB, double2, true>, optin);
           set_smem(k_xphys2<double, N1, N2, XD::ZB, XD::ZT, false, 1, VV>, optin);
           set_smem(k_xphys2<float, N1, N2, XF::ZB, XF::ZT, false, 1, VV>, optin);
           set_smem(k_xphys2<double, N1, N2, XD::ZB, XD::ZT, false, 2, VV>, optin);
@@ -522,6 +646,70 @@ cudaError_t prepare_transforms2() {
     });
   }
   return cudaSuccess;
+}
+
+// The driver's tensor-map encoder (cuTensorMapEncodeTiled), fetched once through the runtime.
+using EncodeTiledFn = CUresult (*)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
+                                   const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
+                                   CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+EncodeTiledFn encode_tiled() {
+  static const EncodeTiledFn fn = [] {
+    void *p = nullptr;
+    cudaDriverEntryPointQueryResult q{};
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess)
+      return (EncodeTiledFn) nullptr;
+    return reinterpret_cast<EncodeTiledFn>(p);
+  }();
+  return fn;
+}
+
+int opt_in_smem() {
+  int dev = 0, optin = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess ||
+      cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) != cudaSuccess)
+    return 0;
+  return optin;
+}
+
+// The tile map of a z kernel's input: `base` holds nfield planes per y of n rows x nxh complex
+// elements of es-byte scalars (a (2 nxh, n, nfield ny) tensor of scalars); a box is KB complex
+// columns by tile_rows(n) rows of one plane.  The rules of a tiled map, checked here: base and
+// strides (2 nxh es, 2 nxh es n) multiples of 16 bytes, box extents <= 256, inner box 2 KB es
+// bytes a multiple of 16, every copy's x coordinate 2 kx0 scalars (kx0 a multiple of KB) a
+// multiple of 16 bytes, and every box's shared destination (r0 KB 2 es bytes past a 128-byte
+// aligned tile) on a 128-byte boundary.  False where the grid or the encoder does not allow it;
+// the caller then loads per thread.
+bool z_tile_map(const void *base, int nxh, int n, int nfield, int ny, int KB, size_t es, CUtensorMap *m) {
+  const EncodeTiledFn fn = encode_tiled();
+  const int rows = tile_rows(n);
+  if (!fn || 2 * KB > 256 || rows == 0 || (2 * KB * es) % 16 != 0 || (2 * (size_t)nxh * es) % 16 != 0 ||
+      ((size_t)rows * KB * 2 * es) % 128 != 0 || (reinterpret_cast<uintptr_t>(base) & 15u) != 0)
+    return false;
+  const cuuint64_t dims[3] = {2ull * (cuuint64_t)nxh, (cuuint64_t)n, (cuuint64_t)nfield * (cuuint64_t)ny};
+  const cuuint64_t strides[2] = {2ull * es * (cuuint64_t)nxh, 2ull * es * (cuuint64_t)nxh * (cuuint64_t)n};
+  const cuuint32_t box[3] = {(cuuint32_t)(2 * KB), (cuuint32_t)rows, 1u}, ones[3] = {1u, 1u, 1u};
+  return fn(m, es == 4 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3,
+            const_cast<void *>(base), dims, strides, box, ones, CU_TENSOR_MAP_INTERLEAVE_NONE,
+            CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+// y_to_x through TMA: only from the state S (the map covers its 3 + nsc fields)
+template <typename R, int N1, int N2, int KB>
+bool zinv_tma_map(const Handle &h, const double2 *src, int nfield, CUtensorMap *m) {
+  return h.tune.ztma && src == h.S && nfield <= 3 + h.nsc &&
+         z_smem_tma<R, N1, N2, KB, double2>(h.nz) <= (size_t)opt_in_smem() &&
+         z_tile_map(h.S, h.nxh, h.nz, 3 + h.nsc, h.ny, KB, sizeof(double), m);
+}
+
+// x_to_y through TMA: only from the slab MID (the map covers its 5 + 3 nsc fields)
+template <typename R, int N1, int N2, int KB>
+bool zfwd_tma_map(const Handle &h, const void *mid, int nfield, CUtensorMap *m) {
+  const int nprod = 5 + 3 * h.nsc;
+  return h.tune.ztma && mid == h.MID && nfield <= nprod &&
+         z_smem_tma<R, N1, N2, KB, typename Cpx<R>::T>(N1 * N2) <= (size_t)opt_in_smem() &&
+         z_tile_map(h.MID, h.nxh, N1 * N2, nprod, h.ny, KB, sizeof(R), m);
 }
 
 // Returns cudaErrorNotSupported when the length has no four-step shape (caller falls back).
@@ -533,8 +721,14 @@ cudaError_t launch_zinv2(Handle &h, const double2 *src, void *mid, int nfield, c
         using C = typename Cpx<R>::T;
         constexpr int KB = ZVar<R, tuned_variant<N1 * N2, V>()>::KB;
         dim3 grid((unsigned)((h.nxh + KB - 1) / KB), (unsigned)h.ny, (unsigned)nfield);
-        k_zinv2<R, N1, N2, KB><<<grid, z_threads<N1, N2, KB>(), z_smem<R, N1, N2, KB>(), st>>>(
-            src, reinterpret_cast<C *>(mid), h.pz, h.nz, h.nxh, h.ns, h.nm);
+        CUtensorMap tmap{};
+        if (zinv_tma_map<R, N1, N2, KB>(h, src, nfield, &tmap))
+          k_zinv2<R, N1, N2, KB, true><<<grid, z_threads<N1, N2, KB>(), z_smem_tma<R, N1, N2, KB, double2>(h.nz),
+                                         st>>>(src, reinterpret_cast<C *>(mid), h.pz, h.nz, h.nxh, h.ns, h.nm, tmap,
+                                               h.ny, &h.dsc->err);
+        else
+          k_zinv2<R, N1, N2, KB, false><<<grid, z_threads<N1, N2, KB>(), z_smem<R, N1, N2, KB>(), st>>>(
+              src, reinterpret_cast<C *>(mid), h.pz, h.nz, h.nxh, h.ns, h.nm, tmap, h.ny, &h.dsc->err);
         err = cudaGetLastError();
       });
     });
@@ -553,8 +747,15 @@ cudaError_t launch_zfwd2(Handle &h, const void *mid, void *dst, int nfield, doub
         using C = typename Cpx<R>::T;
         constexpr int KB = ZVar<R, tuned_variant<N1 * N2, V>()>::KB;
         dim3 grid((unsigned)((h.nxh + KB - 1) / KB), (unsigned)h.ny, (unsigned)nfield);
-        k_zfwd2<R, N1, N2, KB, D><<<grid, z_threads<N1, N2, KB>(), z_smem<R, N1, N2, KB>(), st>>>(
-            reinterpret_cast<const C *>(mid), reinterpret_cast<D *>(dst), h.pz, h.nz, h.nxh, h.ns, h.nm, scale);
+        CUtensorMap tmap{};
+        if (zfwd_tma_map<R, N1, N2, KB>(h, mid, nfield, &tmap))
+          k_zfwd2<R, N1, N2, KB, D, true><<<grid, z_threads<N1, N2, KB>(), z_smem_tma<R, N1, N2, KB, C>(N1 * N2),
+                                            st>>>(reinterpret_cast<const C *>(mid), reinterpret_cast<D *>(dst), h.pz,
+                                                  h.nz, h.nxh, h.ns, h.nm, scale, tmap, h.ny, &h.dsc->err);
+        else
+          k_zfwd2<R, N1, N2, KB, D, false><<<grid, z_threads<N1, N2, KB>(), z_smem<R, N1, N2, KB>(), st>>>(
+              reinterpret_cast<const C *>(mid), reinterpret_cast<D *>(dst), h.pz, h.nz, h.nxh, h.ns, h.nm, scale,
+              tmap, h.ny, &h.dsc->err);
         err = cudaGetLastError();
       });
     });
@@ -566,6 +767,23 @@ cudaError_t launch_zfwd2(Handle &h, const void *mid, void *dst, int nfield, doub
     go.template operator()<double, double2>();
   }
   return err;
+}
+
+bool z_tma_possible(const Handle &h, int zvar) {
+  bool ok = false;
+  auto go = [&]<typename R>() {
+    with_shape(h.nz32, [&]<int N1, int N2>() {
+      with_variant(zvar, [&]<int V>() {
+        constexpr int KB = ZVar<R, tuned_variant<N1 * N2, V>()>::KB;
+        CUtensorMap m{};
+        ok = z_smem_tma<R, N1, N2, KB, double2>(h.nz) <= (size_t)opt_in_smem() &&
+             z_tile_map(h.S, h.nxh, h.nz, 3 + h.nsc, h.ny, KB, sizeof(double), &m);
+      });
+    });
+  };
+  if (h.mixed) go.template operator()<float>();
+  else go.template operator()<double>();
+  return ok;
 }
 
 cudaError_t launch_xadj2(Handle &h, const double2 *base_mid, double2 *lmid, double scale, cudaStream_t st) {

@@ -3,7 +3,8 @@
 // No counterpart in the reference (FFTW's planner, FFTW_MEASURE at module_ppdfftw.f90:422-477, is
 // its nearest relative: it times candidate plans at set-up and keeps the fastest).  The
 // candidates are
-//   z transforms   kx lines per block (transforms2.cu ZVar; zinv + zfwd timed together),
+//   z transforms   kx lines per block (transforms2.cu ZVar; zinv + zfwd timed together), each
+//                  with per-thread input loads or TMA-staged input tiles,
 //   x pass         z rows per block and threads (XVar),
 //   hvhg           32 or 64 (kx, kz) systems per block (one scalar), each with the operator
 //                  tables read through L1 or copied to shared memory,
@@ -96,17 +97,30 @@ int autotune(Handle &h, kmm_tuning *out) {
   std::memset(&rep, 0, sizeof(rep));
   int rc;
   const int nprod = 5 + 3 * h.nsc;
-  // z transforms
-  for (int v = 0; v < 3; ++v) {
-    h.tune.z = v;
-    auto body = [&]() {
-      cudaError_t e = launch_zinv(h, h.S, h.MID, nfld, st);
-      if (e == cudaSuccess) e = launch_zfwd(h, h.MID, h.P, nprod, h.rescale, !h.mixed, st);
-      return e;
-    };
-    if ((rc = measure(none, body, &rep.ms_z[v]))) return rc;
-  }
-  h.tune.z = best(rep.ms_z, 3);
+  // z transforms: lines per block, each with per-thread input loads or TMA-staged input tiles
+  // (where the grid allows the tile map)
+  double best_z = 0.0;
+  int bz = 0, bt = 0;
+  for (int t = 0; t < 2; ++t)
+    for (int v = 0; v < 3; ++v) {
+      if (t && !z_tma_possible(h, v)) continue;
+      h.tune.z = v;
+      h.tune.ztma = t;
+      auto body = [&]() {
+        cudaError_t e = launch_zinv(h, h.S, h.MID, nfld, st);
+        if (e == cudaSuccess) e = launch_zfwd(h, h.MID, h.P, nprod, h.rescale, !h.mixed, st);
+        return e;
+      };
+      double *slot = t ? &rep.ms_z_tma[v] : &rep.ms_z[v];
+      if ((rc = measure(none, body, slot))) return rc;
+      if (best_z == 0.0 || *slot < best_z) {
+        best_z = *slot;
+        bz = v;
+        bt = t;
+      }
+    }
+  h.tune.z = bz;
+  h.tune.ztma = bt;
   // x pass, each run on fresh z-inverse slabs
   for (int v = 0; v < 3; ++v) {
     h.tune.x = v;
@@ -229,6 +243,7 @@ int autotune(Handle &h, kmm_tuning *out) {
   std::memcpy(h.tune.ms_assemble, rep.ms_assemble, sizeof(rep.ms_assemble));
   std::memcpy(h.tune.ms_tables, rep.ms_tables, sizeof(rep.ms_tables));
   std::memcpy(h.tune.ms_helm, rep.ms_helm, sizeof(rep.ms_helm));
+  std::memcpy(h.tune.ms_z_tma, rep.ms_z_tma, sizeof(rep.ms_z_tma));
   // the step graph holds the old launch shapes: capture it again at the next step
   if (h.gexec) cudaGraphExecDestroy(h.gexec);
   if (h.graph) cudaGraphDestroy(h.graph);
@@ -253,6 +268,7 @@ int kmm_get_tuning(const kmm_handle *hh, kmm_tuning *out) {
   out->helm_modes_per_block = 32 * (h.nsc == 1 ? h.tune.hgroups : 1);
   out->helm_tables_shared = h.tune.hstab;
   out->helm_stage_ahead = h.nsc == 1 ? h.tune.stage : 1;
+  out->z_tma = h.tune.ztma;
   out->u_layout = h.tune.ulayout;
   out->assemble_threads = h.tune.asm_threads;
   out->tuned = h.tune.tuned ? 1 : 0;
@@ -264,6 +280,7 @@ int kmm_get_tuning(const kmm_handle *hh, kmm_tuning *out) {
   std::memcpy(out->ms_assemble, h.tune.ms_assemble, sizeof(out->ms_assemble));
   std::memcpy(out->ms_tables, h.tune.ms_tables, sizeof(out->ms_tables));
   std::memcpy(out->ms_helm, h.tune.ms_helm, sizeof(out->ms_helm));
+  std::memcpy(out->ms_z_tma, h.tune.ms_z_tma, sizeof(out->ms_z_tma));
   return KMM_OK;
 }
 
@@ -287,8 +304,9 @@ int kmm_set_tuning(kmm_handle *hh, const kmm_tuning *t) {
   const bool helm_ok = hg != 0 && (t->helm_tables_shared == 0 || t->helm_tables_shared == 1) &&
                        (t->helm_stage_ahead == 1 || t->helm_stage_ahead == 2) &&
                        helm_shape_fits(h, hg, t->helm_tables_shared, t->helm_stage_ahead);
+  const bool tma_ok = t->z_tma == 0 || (t->z_tma == 1 && zv >= 0 && z_tma_possible(h, zv));
   if (zv < 0 || xv < 0 || g == 0 || (g == 2 && h.nsc != 1) || (t->u_layout != 0 && t->u_layout != 1) || !asm_ok ||
-      !tab_ok || !helm_ok) {
+      !tab_ok || !helm_ok || !tma_ok) {
     set_error("kmm_set_tuning: a requested shape is not among this grid's candidates (see kmm_autotune)");
     return KMM_ERR_ARG;
   }
@@ -301,6 +319,7 @@ int kmm_set_tuning(kmm_handle *hh, const kmm_tuning *t) {
   next.hgroups = hg;
   next.hstab = t->helm_tables_shared;
   next.stage = t->helm_stage_ahead;
+  next.ztma = t->z_tma;
   DeviceGuard dg(h.cfg.device);
   cudaStreamSynchronize(h.stream);
   h.tune = next;

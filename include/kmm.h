@@ -35,7 +35,7 @@ extern "C" {
 #define KMM_ERR_DT 3          /* dt <= 1e-14 or dt > 1e5 (dft_x_realspace.f90:494-497) */
 #define KMM_ERR_NONFINITE 4   /* NaN / Inf in the velocity maximum or in uploaded state */
 #define KMM_ERR_ARG 5         /* null pointer, bad substep, size mismatch */
-#define KMM_ERR_TIMEOUT 6     /* reserved: no entry point waits on the device with a limit yet */
+#define KMM_ERR_TIMEOUT 6     /* a bounded device wait gave up (a TMA tile copy of the z transforms) */
 #define KMM_ERR_IO 7          /* checkpoint file: unreadable, missing dataset, unexpected shape or
                                  type (the checks of module_hdf5_io.f90:212-345, same messages) */
 
@@ -107,7 +107,8 @@ typedef struct kmm_tuning {
   int32_t helm_modes_per_block;  /* systems a block of the Helmholtz solver takes (32, 64, 128) */
   int32_t helm_tables_shared;    /* 1: the Helmholtz solver reads the tables from shared memory */
   int32_t helm_stage_ahead;      /* rows its sweeps stage ahead through shared memory (1, 2) */
-  int32_t reserved;
+  int32_t z_tma;              /* 1: the z transforms stage each block's input tile through TMA
+                                 (cp.async.bulk.tensor into shared memory) */
   double ms_z[3];             /* zinv + zfwd per z variant */
   double ms_x[3];             /* x pass per x variant */
   double ms_modes[2];         /* hvhg at 32 and 64 modes per block (best tables choice) */
@@ -116,6 +117,8 @@ typedef struct kmm_tuning {
   double ms_tables[2];        /* hvhg with the tables read through L1 / from shared memory */
   double ms_helm[12];         /* Helmholtz at [32, 64, 128 modes][tables via L1, shared]
                                  [look-ahead 1, 2] (row-major; 0 where a shape does not fit) */
+  double ms_z_tma[3];         /* zinv + zfwd per z variant with TMA-staged input tiles (0 where
+                                 the grid does not allow them) */
 } kmm_tuning;
 
 typedef struct kmm_handle kmm_handle;

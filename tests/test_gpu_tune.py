@@ -33,6 +33,8 @@ def test_every_candidate_shape_is_bit_identical(precision):
     z_lines = {16: (8, 32), 8: (4, 16)}[8 if precision == 0 else 16]
     x_shapes = [(1, 128), (4, 256)] if precision == 1 else [(1, 128), (2, 128)]
     cases = [dict(z_lines_per_block=z) for z in z_lines]
+    # the z transforms with TMA-staged input tiles, at the default and both other z shapes
+    cases += [dict(z_tma=1)] + [dict(z_lines_per_block=z, z_tma=1) for z in z_lines]
     cases += [dict(x_rows_per_block=r, x_threads=t) for r, t in x_shapes]
     cases += [dict(modes_per_block=64), dict(u_layout=1), dict(assemble_threads=128), dict(assemble_threads=512)]
     # hvhg: the operator tables through L1 or from shared memory, at both block sizes

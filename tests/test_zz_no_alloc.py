@@ -1,5 +1,6 @@
 """The allocation-free Helmholtz solve (kmm_helmholtz_solve_noalloc) against the existing
-handle-based path (kmm_dev_labs_lu + kmm_dev_labs_bs on a caller-built band), through the C ABI.
+handle-based path (kmm_dev_labs_lu + kmm_dev_labs_bs on a caller-built band) and against the
+oracle's packed-band LU and substitution, through the C ABI.
 
 The new entry point serves callers that may not allocate device memory (stream capture in
 progress, device memory reserved by another allocator, no tolerance for cudaMalloc's
@@ -67,6 +68,47 @@ def test_noalloc_matches_existing_path_two_calls():
             got = x.cpu().numpy()
             err = np.linalg.norm(got - ref) / np.linalg.norm(ref)
             assert err < 1e-13, (call, err)
+
+
+def test_noalloc_matches_oracle():
+    """Against the oracle directly: per mode the band a D0 - b D2 with the Dirichlet first and last
+    rows, factored and solved by oracle/labs.py (fixed_bandec / fixed_banbks in the reference's
+    loop order, module_labs.f90:3487-3636, 4252-4318), on the oracle's own operators."""
+    from oracle import kmm as okmm
+    from oracle import labs as olabs
+    from tests.helpers import make_pair
+
+    lib = _lib.load()
+    cfg, p = make_pair(nx=8, ny=65, nz=8)
+    ops = okmm.make_operators(p)
+    with Channel(cfg) as ch:
+        ny, bw = cfg.ny, ch.bw
+        assert bw == ops.bw and np.array_equal(ch.D0, ops.D0) and np.array_equal(ch.D2, ops.D2)
+        nm = 64
+        rng = np.random.default_rng(7)
+        a = 1.0 + rng.random(nm)
+        b = 0.02 * rng.random(nm)
+        rhs = rng.standard_normal((ny, nm)) + 1j * rng.standard_normal((ny, nm))
+        want = np.empty_like(rhs)
+        for m in range(nm):
+            A = a[m] * ops.D0 - b[m] * ops.D2
+            for col in (0, ny - 1):
+                diag = A[bw, col]
+                A[:, col] = 0.0
+                A[bw, col] = diag
+            want[:, m] = olabs.bs(olabs.lu(A), rhs[:, m])
+        d0 = torch.from_numpy(np.ascontiguousarray(ch.D0.T)).to(DEV)
+        d2 = torch.from_numpy(np.ascontiguousarray(ch.D2.T)).to(DEV)
+        a_d, b_d = torch.from_numpy(a).to(DEV), torch.from_numpy(b).to(DEV)
+        x = torch.from_numpy(rhs.copy()).to(DEV)
+        stream = C.c_void_p(torch.cuda.current_stream().cuda_stream)
+        rc = lib.kmm_helmholtz_solve_noalloc(ny, bw, nm, C.c_void_p(d0.data_ptr()), C.c_void_p(d2.data_ptr()),
+                                             C.c_void_p(a_d.data_ptr()), C.c_void_p(b_d.data_ptr()),
+                                             C.c_void_p(x.data_ptr()), stream)
+        assert rc == 0, lib.kmm_last_error().decode()
+        torch.cuda.synchronize()
+        got = x.cpu().numpy()
+    assert np.linalg.norm(got - want) / np.linalg.norm(want) < 1e-13
 
 
 def test_noalloc_rejects_oversize_request():
