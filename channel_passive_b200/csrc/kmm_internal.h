@@ -91,11 +91,13 @@ struct Tuning {
   int ulayout = 0;        // U factor storage: 0 = [offset][y][mode], 1 = [y][offset][mode]
   int asm_threads = 256;  // threads per block of the assembly kernel
   int stab = 0;           // 1: the hvhg kernel reads the operator tables from shared memory
+  int hvstage = 0;        // rows the hvhg sweeps stage ahead through shared memory (0: L1 prefetch)
   bool tuned = false;
   // device ms of every candidate of the last autotune (kmm_tuning's ms_* fields)
   double ms_z[3] = {}, ms_x[3] = {}, ms_modes[2] = {}, ms_layout[2] = {}, ms_assemble[3] = {}, ms_tables[2] = {};
   double ms_helm[3][2][2] = {};  // [32/64/128 modes][tables via L1 / shared][look-ahead 1 / 2]
   double ms_z_tma[3] = {};       // the z variants with TMA-staged input tiles
+  double ms_hvhg[2][2][3] = {};  // [32/64 modes][tables via L1 / shared][staging 0 / 1 / 2 rows]
 };
 
 struct Handle {
@@ -265,6 +267,7 @@ size_t solver_tables_bytes(const Handle &h);
 // (four-step length, tile within the shared-memory limit, tile map accepted by the encoder).
 bool z_tma_possible(const Handle &h, int zvar);
 bool hvhg_tables_fit(const Handle &h);
+bool hvhg_shape_fits(const Handle &h, int groups, int stab, int stage);
 bool helm_shape_fits(const Handle &h, int hgroups, int hstab, int stage);
 void default_solver_shapes(Handle &h);
 

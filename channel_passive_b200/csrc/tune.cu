@@ -6,8 +6,9 @@
 //   z transforms   kx lines per block (transforms2.cu ZVar; zinv + zfwd timed together), each
 //                  with per-thread input loads or TMA-staged input tiles,
 //   x pass         z rows per block and threads (XVar),
-//   hvhg           32 or 64 (kx, kz) systems per block (one scalar), each with the operator
-//                  tables read through L1 or copied to shared memory,
+//   hvhg           32 or 64 (kx, kz) systems per block (one scalar) x the operator tables read
+//                  through L1 or copied to shared memory x rows prefetched into L1 or staged
+//                  through a shared-memory ring 1 or 2 rows ahead,
 //   Helmholtz      32, 64 or 128 systems per block x tables through L1 / in shared memory x one
 //                  or two rows of staging look-ahead, where a block's shared memory holds the
 //                  shape; then the U factor storage layout,
@@ -149,29 +150,35 @@ int autotune(Handle &h, kmm_tuning *out) {
   auto keep_min = [](double &acc, double v) {
     if (v > 0.0 && (acc == 0.0 || v < acc)) acc = v;
   };
-  // k_hvhg: modes per block x tables through L1 / in shared memory
+  // k_hvhg: modes per block x tables through L1 / in shared memory x staging (L1 prefetch, or a
+  // shared-memory ring 1 or 2 rows ahead)
   const int ng = h.nsc == 1 ? 2 : 1;
   {
     double best_ms = 0.0;
-    int bg = 1, bs = 0;
+    int bg = 1, bs = 0, ba = 0;
     for (int g = 1; g <= ng; ++g)
-      for (int sh = 0; sh < 2; ++sh) {
-        if (sh && !hvhg_tables_fit(h)) continue;
-        h.tune.groups = g;
-        h.tune.stab = sh;
-        double ms = 0.0;
-        auto body = [&]() { return launch_ws_hvhg(h, 2, nullptr, st); };
-        if ((rc = measure(restore_joined, body, &ms))) return rc;
-        keep_min(rep.ms_modes[g - 1], ms);
-        keep_min(rep.ms_tables[sh], ms);
-        if (best_ms == 0.0 || ms < best_ms) {
-          best_ms = ms;
-          bg = g;
-          bs = sh;
+      for (int sh = 0; sh < 2; ++sh)
+        for (int sa = 0; sa <= 2; ++sa) {
+          if (!hvhg_shape_fits(h, g, sh, sa)) continue;
+          h.tune.groups = g;
+          h.tune.stab = sh;
+          h.tune.hvstage = sa;
+          double ms = 0.0;
+          auto body = [&]() { return launch_ws_hvhg(h, 2, nullptr, st); };
+          if ((rc = measure(restore_joined, body, &ms))) return rc;
+          rep.ms_hvhg[((g - 1) * 2 + sh) * 3 + sa] = ms;
+          keep_min(rep.ms_modes[g - 1], ms);
+          keep_min(rep.ms_tables[sh], ms);
+          if (best_ms == 0.0 || ms < best_ms) {
+            best_ms = ms;
+            bg = g;
+            bs = sh;
+            ba = sa;
+          }
         }
-      }
     h.tune.groups = bg;
     h.tune.stab = bs;
+    h.tune.hvstage = ba;
   }
   // k_helmholtz after the chosen hvhg: modes per block x tables x staging look-ahead, then the
   // U factor layout
@@ -244,6 +251,7 @@ int autotune(Handle &h, kmm_tuning *out) {
   std::memcpy(h.tune.ms_tables, rep.ms_tables, sizeof(rep.ms_tables));
   std::memcpy(h.tune.ms_helm, rep.ms_helm, sizeof(rep.ms_helm));
   std::memcpy(h.tune.ms_z_tma, rep.ms_z_tma, sizeof(rep.ms_z_tma));
+  std::memcpy(h.tune.ms_hvhg, rep.ms_hvhg, sizeof(rep.ms_hvhg));
   // the step graph holds the old launch shapes: capture it again at the next step
   if (h.gexec) cudaGraphExecDestroy(h.gexec);
   if (h.graph) cudaGraphDestroy(h.graph);
@@ -269,6 +277,7 @@ int kmm_get_tuning(const kmm_handle *hh, kmm_tuning *out) {
   out->helm_tables_shared = h.tune.hstab;
   out->helm_stage_ahead = h.nsc == 1 ? h.tune.stage : 1;
   out->z_tma = h.tune.ztma;
+  out->hvhg_stage_ahead = h.tune.hvstage;
   out->u_layout = h.tune.ulayout;
   out->assemble_threads = h.tune.asm_threads;
   out->tuned = h.tune.tuned ? 1 : 0;
@@ -281,6 +290,7 @@ int kmm_get_tuning(const kmm_handle *hh, kmm_tuning *out) {
   std::memcpy(out->ms_tables, h.tune.ms_tables, sizeof(out->ms_tables));
   std::memcpy(out->ms_helm, h.tune.ms_helm, sizeof(out->ms_helm));
   std::memcpy(out->ms_z_tma, h.tune.ms_z_tma, sizeof(out->ms_z_tma));
+  std::memcpy(out->ms_hvhg, h.tune.ms_hvhg, sizeof(out->ms_hvhg));
   return KMM_OK;
 }
 
@@ -298,7 +308,9 @@ int kmm_set_tuning(kmm_handle *hh, const kmm_tuning *t) {
   }
   const int g = t->modes_per_block == 32 ? 1 : t->modes_per_block == 64 ? 2 : 0;
   const bool asm_ok = t->assemble_threads == 128 || t->assemble_threads == 256 || t->assemble_threads == 512;
-  const bool tab_ok = t->tables_shared == 0 || (t->tables_shared == 1 && hvhg_tables_fit(h));
+  const bool tab_ok = (t->tables_shared == 0 || t->tables_shared == 1) &&
+                      (t->hvhg_stage_ahead >= 0 && t->hvhg_stage_ahead <= 2) && g != 0 &&
+                      hvhg_shape_fits(h, g, t->tables_shared, t->hvhg_stage_ahead);
   const int hg = t->helm_modes_per_block == 32 ? 1 : t->helm_modes_per_block == 64 ? 2
                  : t->helm_modes_per_block == 128 ? 4 : 0;
   const bool helm_ok = hg != 0 && (t->helm_tables_shared == 0 || t->helm_tables_shared == 1) &&
@@ -320,6 +332,7 @@ int kmm_set_tuning(kmm_handle *hh, const kmm_tuning *t) {
   next.hstab = t->helm_tables_shared;
   next.stage = t->helm_stage_ahead;
   next.ztma = t->z_tma;
+  next.hvstage = t->hvhg_stage_ahead;
   DeviceGuard dg(h.cfg.device);
   cudaStreamSynchronize(h.stream);
   h.tune = next;

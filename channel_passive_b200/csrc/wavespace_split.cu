@@ -165,10 +165,26 @@ __device__ __forceinline__ void vrow(const Tabs<BW> &tb, int r, int n, double k2
   for (int e = -2 * BW; e <= 2 * BW; ++e) row[e + 2 * BW] = -k2 * r0[e] + r2[e];
 }
 
+// A staged nonlinear-term unit, widened to double2.
+template <typename PT, int K, int S>
+__device__ __forceinline__ double2 ring_hv(const Ring<K, S> &ring, int step, int k) {
+  if constexpr (sizeof(PT) == sizeof(float2)) return ring.f(step, k);
+  else return ring.c(step, k);
+}
+
 // ------------------------------------------------------------------------------------------
 // k_hvhg: role ROLE of mode m; NC = 2 adds the store's D0 solve at substep 1.
-template <int BW, typename PT, int ROLE, int NC>
-__device__ __forceinline__ void hvhg_role(const SplitArgs &a, const Tabs<BW> &tb, int64_t m) {
+// SA = 0: the sweeps prefetch their rows into L1 (kPrefetchRows ahead).  SA = 1, 2: they stage
+// them through a thread-private shared-memory ring, cp.async SA rows ahead (Ring; as in
+// k_helmholtz), kHvUnits 16-byte units per row:
+//   forward   0..2 the role's products, 3 the RK store (substep 1), 4 v (the control probe);
+//   backward  0 the product chain, 1 the store chain, 2..4 the products the emission of row
+//             q = r + BW reads.
+constexpr int kHvUnits = 5;
+
+template <int BW, typename PT, int ROLE, int NC, int SA>
+__device__ __forceinline__ void hvhg_role(const SplitArgs &a, const Tabs<BW> &tb, int64_t m,
+                                          const Ring<kHvUnits, SA + 1> &ring) {
   const int n = a.ny;
   const int64_t nm = a.nmodes, ns = a.ns;
   const ModeK k = mode_k(a, m);
@@ -177,6 +193,9 @@ __device__ __forceinline__ void hvhg_role(const SplitArgs &a, const Tabs<BW> &tb
   const PT *P = reinterpret_cast<const PT *>(a.P) + m;
   auto prod = [&](int slot, int r) { return ldp<PT>(P + slot * ns + (r - 1) * (int)nm); };
   auto pfp = [&](int slot, int r) { pf_l1(P + slot * ns + (r - 1) * (int)nm); };
+  auto pat = [&](int slot, int r) { return P + slot * ns + (r - 1) * (int)nm; };
+  // a product of row r: staged (unit u of step `step`) or straight from global memory
+  auto rp = [&](int step, int u) { return ring_hv<PT>(ring, step, u); };
   // the product chain's forward results at the products' precision (PT), the store chain's
   // (substep 1, FP64 state) in double2
   const Line<PT> Z0{reinterpret_cast<PT *>(a.zl + (2 * ROLE) * ns) + m, nm};
@@ -197,58 +216,76 @@ __device__ __forceinline__ void hvhg_role(const SplitArgs &a, const Tabs<BW> &tb
   const DLine Sv{a.S + ns + m, nm};
   double2 plo = z2(0.0, 0.0), phi = z2(0.0, 0.0);
 
-  fwd_fixed<BW, NC>(tb, n,
+  constexpr int PF = SA > 0 ? SA : kPrefetchRows;
+  constexpr bool RING = SA > 0;
+  fwd_fixed<BW, NC, PF, RING>(tb, n,
       [&](int r, double2 *b) {
         if constexpr (ROLE == 0) {
-          const double2 f1 = prod(0, r), f3 = prod(2, r), f5 = prod(4, r);
+          const double2 f1 = RING ? rp(r, 0) : prod(0, r), f3 = RING ? rp(r, 1) : prod(2, r);
+          const double2 f5 = RING ? rp(r, 2) : prod(4, r);
           b[0] = zsub(zsub(zscale(-kx2, f1), zscale(2.0 * kxkz, f5)), zscale(kz2, f3));
         } else if constexpr (SCAL) {
-          b[0] = prod(s8, r);
+          b[0] = RING ? rp(r, 0) : prod(s8, r);
         } else if constexpr (ROLE == 2) {
-          b[0] = prod(1, r);
+          b[0] = RING ? rp(r, 0) : prod(1, r);
         } else {
-          b[0] = prod(3, r);
+          b[0] = RING ? rp(r, 0) : prod(3, r);
           if (probe) {
-            const double2 v = Sv.ld(r);
+            const double2 v = RING ? ring.c(r, 4) : Sv.ld(r);
             plo = zadd(plo, zscale(__ldg(a.wlo + r - 1), v));
             phi = zadd(phi, zscale(__ldg(a.whi + r - 1), v));
           }
         }
-        if constexpr (NC == 2) b[1] = Rs.ld(r);
+        if constexpr (NC == 2) b[1] = RING ? ring.c(r, 3) : Rs.ld(r);
       },
       [&](int r, const double2 *z) {
         Z0.st(r, z[0]);
         if constexpr (NC == 2) Z1.st(r, z[1]);
       },
       [&](int r) {
-        if constexpr (ROLE == 0) { pfp(0, r); pfp(2, r); pfp(4, r); }
-        else pfp(SCAL ? s8 : ROLE == 2 ? 1 : 3, r);
-        if constexpr (NC == 2) pf_l1(Rs.p + (r - 1) * (int)nm);
-        if (probe) pf_l1(Sv.p + (r - 1) * (int)nm);
+        if constexpr (RING) {
+          if constexpr (ROLE == 0) {
+            ring.get(r, 0, pat(0, r));
+            ring.get(r, 1, pat(2, r));
+            ring.get(r, 2, pat(4, r));
+          } else {
+            ring.get(r, 0, pat(SCAL ? s8 : ROLE == 2 ? 1 : 3, r));
+          }
+          if constexpr (NC == 2) ring.get(r, 3, Rs.p + (r - 1) * (int)nm);
+          if (probe) ring.get(r, 4, Sv.p + (r - 1) * (int)nm);
+        } else {
+          if constexpr (ROLE == 0) { pfp(0, r); pfp(2, r); pfp(4, r); }
+          else pfp(SCAL ? s8 : ROLE == 2 ? 1 : 3, r);
+          if constexpr (NC == 2) pf_l1(Rs.p + (r - 1) * (int)nm);
+          if (probe) pf_l1(Sv.p + (r - 1) * (int)nm);
+        }
       });
   if (probe) {
     a.vwall[m] = plo;
     a.vwall[nm + m] = phi;
   }
 
-  bwd_emit<BW, NC, 0>(n, ufix,
+  bwd_emit<BW, NC, 0, PF, RING>(n, ufix,
       [&](int r, double2 *zc, double *) {
-        zc[0] = Z0.ld(r);
-        if constexpr (NC == 2) zc[1] = Z1.ld(r);
+        zc[0] = RING ? rp(r, 0) : Z0.ld(r);
+        if constexpr (NC == 2) zc[1] = RING ? ring.c(r, 1) : Z1.ld(r);
       },
       [&](int q, int r, const double2 (&wc)[NC][2 * BW + 1], const double (&)[1][2 * BW + 1]) {
+        // the products of row q: staged with step r when q = r + BW, else from global memory
+        const bool st = RING && q == r + BW;
+        auto pq = [&](int slot, int u) { return st ? rp(r, u) : prod(slot, q); };
         if constexpr (ROLE == 0) {
           const double c2i = kx * kx * kx + kx * (kz * kz), c4i = (kx * kx) * kz + kz * kz * kz;
-          const double2 f2 = prod(1, q), f4 = prod(3, q);
+          const double2 f2 = pq(1, 2), f4 = pq(3, 3);
           const double2 ehv = z2(-c2i * f2.y - c4i * f4.y, c2i * f2.x + c4i * f4.x);
           hv(H_HV0).st(q, zadd(ehv, mvc<BW>(tb.t1, q, r, wc[0])));
         } else if constexpr (SCAL) {
-          const double2 f7 = prod(s7, q), f9 = prod(s9, q);
+          const double2 f7 = pq(s7, 2), f9 = pq(s9, 3);
           const double2 t7 = z2(-kx * f7.y - kz * f9.y, kx * f7.x + kz * f9.x);
           const double2 t = zadd(t7, mvc<BW>(tb.t1, q, r, wc[0]));
           hv(ROLE == 4 ? H_HT2 : H_HT).st(q, z2(-t.x, -t.y));
         } else if constexpr (ROLE == 2) {
-          const double2 f1 = prod(0, q), f3 = prod(2, q), f5 = prod(4, q);
+          const double2 f1 = pq(0, 2), f3 = pq(2, 3), f5 = pq(4, 4);
           const double2 a1 = zadd(zscale(kxkz, zsub(f1, f3)), zscale(kz2 - kx2, f5));
           const double2 d1 = mvc<BW>(tb.t1, q, r, wc[0]), d2 = mvc<BW>(tb.t2, q, r, wc[0]);
           hv(H_G2).st(q, zadd(a1, z2(kz * d1.y, -kz * d1.x)));
@@ -261,13 +298,32 @@ __device__ __forceinline__ void hvhg_role(const SplitArgs &a, const Tabs<BW> &tb
         if constexpr (NC == 2) hl(d2_line).st(q, mvc<BW>(tb.t2, q, r, wc[NC - 1]));
       },
       [&](int r) {
-        pf_l1(Z0.p + (r - 1) * (int)nm);
-        if constexpr (NC == 2) pf_l1(Z1.p + (r - 1) * (int)nm);
-        if (r <= n - 2 * BW) {
-          const int q = r + BW;
-          if constexpr (ROLE == 0) { pfp(1, q); pfp(3, q); }
-          else if constexpr (SCAL) { pfp(s7, q); pfp(s9, q); }
-          else if constexpr (ROLE == 2) { pfp(0, q); pfp(2, q); pfp(4, q); }
+        if constexpr (RING) {
+          ring.get(r, 0, Z0.p + (r - 1) * (int)nm);
+          if constexpr (NC == 2) ring.get(r, 1, Z1.p + (r - 1) * (int)nm);
+          if (r <= n - 2 * BW) {
+            const int q = r + BW;
+            if constexpr (ROLE == 0) {
+              ring.get(r, 2, pat(1, q));
+              ring.get(r, 3, pat(3, q));
+            } else if constexpr (SCAL) {
+              ring.get(r, 2, pat(s7, q));
+              ring.get(r, 3, pat(s9, q));
+            } else if constexpr (ROLE == 2) {
+              ring.get(r, 2, pat(0, q));
+              ring.get(r, 3, pat(2, q));
+              ring.get(r, 4, pat(4, q));
+            }
+          }
+        } else {
+          pf_l1(Z0.p + (r - 1) * (int)nm);
+          if constexpr (NC == 2) pf_l1(Z1.p + (r - 1) * (int)nm);
+          if (r <= n - 2 * BW) {
+            const int q = r + BW;
+            if constexpr (ROLE == 0) { pfp(1, q); pfp(3, q); }
+            else if constexpr (SCAL) { pfp(s7, q); pfp(s9, q); }
+            else if constexpr (ROLE == 2) { pfp(0, q); pfp(2, q); pfp(4, q); }
+          }
         }
       });
 }
@@ -276,27 +332,31 @@ __device__ __forceinline__ void hvhg_role(const SplitArgs &a, const Tabs<BW> &tb
 // blocks of one scalar's 128 threads keep 128 registers a thread; with a fifth role three blocks
 // keep 136 (four would cap it at 96 and spill about 1 KB a thread).
 // One scalar: up to two 32-mode groups per block (Tuning::groups); the bound keeps 128 registers.
-template <int BW, typename PT, int NS>
+// SA > 0 (one scalar): the staging ring of SA + 1 slots, the tables (with stab) after it.
+template <int BW, typename PT, int NS, int SA = 0>
 __global__ void __launch_bounds__(NS == 1 ? 2 * kLanes * kRoles : kLanes * (kRoles + 1), NS == 1 ? 2 : 3)
 k_hvhg(SplitArgs a) {
-  extern __shared__ double hvhg_tabs[];
+  extern __shared__ double2 hvhg_smem[];
   if (a.dsc->err) return;  // uniform over the block, like a.stab
   constexpr int R = kRoles + NS - 1;
   const int role = (threadIdx.x / kLanes) % R, grp = threadIdx.x / (kLanes * R);
   const int64_t m = ((int64_t)blockIdx.x * a.groups + grp) * kLanes + (threadIdx.x % kLanes);
+  const int ring_units = SA > 0 ? (SA + 1) * kHvUnits * (int)blockDim.x : 0;
   // T1, T2 and the D0 factor (L0, U0) are what the hvhg roles read: from T1 on
   const double *t1 = a.tabs + a.ny * (4 * BW + 1);
-  if (a.stab) t1 = tabs_to_shared<BW>(a, 1, hvhg_tabs);
+  if (a.stab) t1 = tabs_to_shared<BW>(a, 1, reinterpret_cast<double *>(hvhg_smem + ring_units));
   if (m == 0 || m >= a.nmodes) return;
   const Tabs<BW> tb = tabs_from_t1<BW>(t1, a.ny);
+  const Ring<kHvUnits, SA + 1> ring{hvhg_smem + threadIdx.x, (int)blockDim.x};
   const bool s1 = a.substep == 1;
   switch (role) {
-    case 0: s1 ? hvhg_role<BW, PT, 0, 2>(a, tb, m) : hvhg_role<BW, PT, 0, 1>(a, tb, m); break;
-    case 1: s1 ? hvhg_role<BW, PT, 1, 2>(a, tb, m) : hvhg_role<BW, PT, 1, 1>(a, tb, m); break;
-    case 2: s1 ? hvhg_role<BW, PT, 2, 2>(a, tb, m) : hvhg_role<BW, PT, 2, 1>(a, tb, m); break;
-    case 3: hvhg_role<BW, PT, 3, 1>(a, tb, m); break;
+    case 0: s1 ? hvhg_role<BW, PT, 0, 2, SA>(a, tb, m, ring) : hvhg_role<BW, PT, 0, 1, SA>(a, tb, m, ring); break;
+    case 1: s1 ? hvhg_role<BW, PT, 1, 2, SA>(a, tb, m, ring) : hvhg_role<BW, PT, 1, 1, SA>(a, tb, m, ring); break;
+    case 2: s1 ? hvhg_role<BW, PT, 2, 2, SA>(a, tb, m, ring) : hvhg_role<BW, PT, 2, 1, SA>(a, tb, m, ring); break;
+    case 3: hvhg_role<BW, PT, 3, 1, SA>(a, tb, m, ring); break;
     default:
-      if constexpr (NS == 2) s1 ? hvhg_role<BW, PT, 4, 2>(a, tb, m) : hvhg_role<BW, PT, 4, 1>(a, tb, m);
+      if constexpr (NS == 2)
+        s1 ? hvhg_role<BW, PT, 4, 2, SA>(a, tb, m, ring) : hvhg_role<BW, PT, 4, 1, SA>(a, tb, m, ring);
       break;
   }
 }
@@ -307,13 +367,6 @@ k_hvhg(SplitArgs a) {
 // to keep prefetched lines until use.  Units per step: kHelmUnits<BW>.
 template <int BW>
 constexpr int kHelmUnits = 5 + BW;
-
-// A staged nonlinear-term unit, widened to double2.
-template <typename PT, int K, int S>
-__device__ __forceinline__ double2 ring_hv(const Ring<K, S> &ring, int step, int k) {
-  if constexpr (sizeof(PT) == sizeof(float2)) return ring.f(step, k);
-  else return ring.c(step, k);
-}
 
 template <int BW, int ROLE, typename PT, int SA>
 __device__ __forceinline__ void helmholtz_role(const SplitArgs &a, const Tabs<BW> &tb, int64_t m,
@@ -889,8 +942,18 @@ cudaError_t split_bw(Handle &h, int part, int substep, const double *dt_ptr, cud
       if (h.mixed) k_hvhg<BW, float2, 2><<<blocks, kLanes * (kRoles + 1), tsm, st>>>(a);
       else k_hvhg<BW, double2, 2><<<blocks, kLanes * (kRoles + 1), tsm, st>>>(a);
     } else {
-      if (h.mixed) k_hvhg<BW, float2, 1><<<blocks, kLanes * kRoles * G, tsm, st>>>(a);
-      else k_hvhg<BW, double2, 1><<<blocks, kLanes * kRoles * G, tsm, st>>>(a);
+      const int nt = kLanes * kRoles * G, sa = h.tune.hvstage;
+      const size_t sm = (sa > 0 ? sizeof(double2) * (size_t)(sa + 1) * kHvUnits * nt : 0) + tsm;
+      if (sa == 2) {
+        if (h.mixed) k_hvhg<BW, float2, 1, 2><<<blocks, nt, sm, st>>>(a);
+        else k_hvhg<BW, double2, 1, 2><<<blocks, nt, sm, st>>>(a);
+      } else if (sa == 1) {
+        if (h.mixed) k_hvhg<BW, float2, 1, 1><<<blocks, nt, sm, st>>>(a);
+        else k_hvhg<BW, double2, 1, 1><<<blocks, nt, sm, st>>>(a);
+      } else {
+        if (h.mixed) k_hvhg<BW, float2, 1><<<blocks, nt, sm, st>>>(a);
+        else k_hvhg<BW, double2, 1><<<blocks, nt, sm, st>>>(a);
+      }
     }
     return cudaGetLastError();
   }
@@ -958,6 +1021,10 @@ cudaError_t set_smem_limit_bw(int bytes) {
   if (e == cudaSuccess) e = lim(k_helmholtz<BW, double2, 2, 1>);
   if (e == cudaSuccess) e = lim(k_hvhg<BW, float2, 1>);
   if (e == cudaSuccess) e = lim(k_hvhg<BW, double2, 1>);
+  if (e == cudaSuccess) e = lim(k_hvhg<BW, float2, 1, 1>);
+  if (e == cudaSuccess) e = lim(k_hvhg<BW, double2, 1, 1>);
+  if (e == cudaSuccess) e = lim(k_hvhg<BW, float2, 1, 2>);
+  if (e == cudaSuccess) e = lim(k_hvhg<BW, double2, 1, 2>);
   if (e == cudaSuccess) e = lim(k_hvhg<BW, float2, 2>);
   if (e == cudaSuccess) e = lim(k_hvhg<BW, double2, 2>);
   return e;
@@ -998,6 +1065,14 @@ bool hvhg_tables_fit(const Handle &h) {
   return solver_tables_bytes(h) <= (size_t)device_attr(cudaDevAttrMaxSharedMemoryPerBlockOptin);
 }
 
+bool hvhg_shape_fits(const Handle &h, int groups, int stab, int stage) {
+  if (h.nsc == 2 && (groups != 1 || stage != 0)) return false;
+  const size_t nt = (size_t)kLanes * kRoles * groups;
+  const size_t bytes = (stage > 0 ? sizeof(double2) * (size_t)(stage + 1) * kHvUnits * nt : 0) +
+                       (stab ? solver_tables_bytes(h) : 0);
+  return bytes <= (size_t)device_attr(cudaDevAttrMaxSharedMemoryPerBlockOptin);
+}
+
 bool helm_shape_fits(const Handle &h, int hgroups, int hstab, int stage) {
   if (h.nsc == 2 && (hgroups != 1 || stage != 1)) return false;
   const size_t bytes = helm_ring_bytes(h, hgroups, stage) + (hstab ? solver_tables_bytes(h) : 0);
@@ -1005,8 +1080,9 @@ bool helm_shape_fits(const Handle &h, int hgroups, int hstab, int stage) {
 }
 
 void default_solver_shapes(Handle &h) {
-  // k_hvhg: 32-mode blocks reading the tables through L1 (what the tuner measured as fastest
-  // or even with the alternatives at 192x129x192).  k_helmholtz: the largest blocks that still
+  // k_hvhg: 32-mode blocks reading the tables through L1 and staging their rows two ahead
+  // through shared memory (0.218 -> 0.212 ms against L1 prefetches at 192x129x192; one row
+  // ahead spills and is slower, and the tables in shared memory beside the ring cost more).  k_helmholtz: the largest blocks that still
   // put a block on nearly every SM, with the tables in shared memory and two steps of staging
   // look-ahead where a block holds them; else 64-mode blocks with the tables where two fit on
   // an SM; else 32-mode blocks reading the tables through L1.
@@ -1015,7 +1091,9 @@ void default_solver_shapes(Handle &h) {
   h.tune.hgroups = 1;
   h.tune.hstab = 0;
   h.tune.stage = 1;
+  h.tune.hvstage = 0;
   if (h.nsc != 1) return;
+  if (hvhg_shape_fits(h, 1, 0, 2)) h.tune.hvstage = 2;  // k_hvhg: a two-row staging ring
   const int sms = device_attr(cudaDevAttrMultiProcessorCount);
   const size_t per_sm = (size_t)device_attr(cudaDevAttrMaxSharedMemoryPerMultiprocessor);
   if (h.nmodes >= (int64_t)kLanes * 4 * sms * 9 / 10 && helm_shape_fits(h, 4, 1, 2)) {

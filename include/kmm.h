@@ -109,6 +109,9 @@ typedef struct kmm_tuning {
   int32_t helm_stage_ahead;      /* rows its sweeps stage ahead through shared memory (1, 2) */
   int32_t z_tma;              /* 1: the z transforms stage each block's input tile through TMA
                                  (cp.async.bulk.tensor into shared memory) */
+  int32_t hvhg_stage_ahead;   /* rows the hvhg sweeps stage ahead through shared memory (0: they
+                                 prefetch into L1 instead; 1, 2) */
+  int32_t reserved;
   double ms_z[3];             /* zinv + zfwd per z variant */
   double ms_x[3];             /* x pass per x variant */
   double ms_modes[2];         /* hvhg at 32 and 64 modes per block (best tables choice) */
@@ -119,6 +122,8 @@ typedef struct kmm_tuning {
                                  [look-ahead 1, 2] (row-major; 0 where a shape does not fit) */
   double ms_z_tma[3];         /* zinv + zfwd per z variant with TMA-staged input tiles (0 where
                                  the grid does not allow them) */
+  double ms_hvhg[12];         /* hvhg at [32, 64 modes][tables via L1, shared][staging 0, 1, 2
+                                 rows] (row-major; 0 where a shape was not timed) */
 } kmm_tuning;
 
 typedef struct kmm_handle kmm_handle;

@@ -37,8 +37,9 @@ def test_every_candidate_shape_is_bit_identical(precision):
     cases += [dict(z_tma=1)] + [dict(z_lines_per_block=z, z_tma=1) for z in z_lines]
     cases += [dict(x_rows_per_block=r, x_threads=t) for r, t in x_shapes]
     cases += [dict(modes_per_block=64), dict(u_layout=1), dict(assemble_threads=128), dict(assemble_threads=512)]
-    # hvhg: the operator tables through L1 or from shared memory, at both block sizes
-    cases += [dict(modes_per_block=mb, tables_shared=ts) for mb in (32, 64) for ts in (0, 1)]
+    # hvhg: block size x the operator tables through L1 or from shared memory x staging
+    cases += [dict(modes_per_block=mb, tables_shared=ts, hvhg_stage_ahead=sa)
+              for mb in (32, 64) for ts in (0, 1) for sa in (0, 1, 2)]
     # Helmholtz: block size x tables x staging look-ahead
     cases += [dict(helm_modes_per_block=mb, helm_tables_shared=ts, helm_stage_ahead=sa)
               for mb in (32, 64, 128) for ts in (0, 1) for sa in (1, 2)]
