@@ -88,6 +88,18 @@ template <typename T> int dalloc(Handle &h, T **p, size_t count) {
   return KMM_OK;
 }
 
+}  // namespace
+
+int diag_buffers(Handle &h) {
+  int rc = KMM_OK;
+  if (!h.mixed) return rc;
+  if (!h.mid64 && (rc = dalloc(h, &h.mid64, 6 * (size_t)h.nm))) return rc;
+  if (!h.p64 && (rc = dalloc(h, &h.p64, 6 * (size_t)h.ns))) return rc;
+  return rc;
+}
+
+namespace {
+
 int validate(const kmm_config &c) {
   auto bad = [](const std::string &m) { set_error(m); return KMM_ERR_CONFIG; };
   if (c.no_of_field < 10) return bad("no_of_field must be >= 10: fields 1..10 are used (wavespace.f90:29)");
@@ -580,7 +592,7 @@ int kmm_destroy(kmm_handle *hh) {
   adjoint_free(*h);
   void *ptrs[] = {h->S, h->RK, h->P, h->MID, h->dops, h->gains, h->vwall, h->zc,
                   h->ec, h->xr, h->ub, h->vf, h->dvw, h->w00, h->staging, h->stat,
-                  h->fftpos, h->tw64, h->tw32, h->dsc};
+                  h->mid64, h->p64, h->fftpos, h->tw64, h->tw32, h->dsc};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   if (h->copy) cudaStreamSynchronize(h->copy);
@@ -821,6 +833,8 @@ int kmm_get_pressure(kmm_handle *hh, double *P) {
   Handle &h = *reinterpret_cast<Handle *>(hh);
   DeviceGuard dg(h.cfg.device);
   double2 *planes = h.staging, *ref = h.staging + h.ns;
+  int rc;
+  if ((rc = diag_buffers(h))) return rc;
   // the wall values nu d2v/dy2 of the state's v into dvw (get_statistics_1's dv/dy call)
   KMM_CUDA(launch_ydiff(h, 2, h.stream));
   const cudaError_t e = launch_pressure(h, planes, h.dvw, nullptr, h.stream);
@@ -844,8 +858,9 @@ int kmm_get_statistics(kmm_handle *hh, double *lines, double *spec_kx, double *s
   Handle &h = *reinterpret_cast<Handle *>(hh);
   DeviceGuard dg(h.cfg.device);
   const StatLayout L = stat_layout(h);
+  int rc;
+  if ((rc = diag_buffers(h))) return rc;
   if (!h.stat) {
-    int rc;
     if ((rc = dalloc(h, &h.stat, L.total))) return rc;
     KMM_CUDA(cudaMemcpy(h.stat + L.center, h.ops.center.data(), sizeof(double) * (size_t)h.ny,
                         cudaMemcpyHostToDevice));

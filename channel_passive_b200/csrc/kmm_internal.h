@@ -127,6 +127,8 @@ struct Handle {
   double2 *dvw = nullptr;                  //                  wall derivatives [3][nmodes]
   double *w00 = nullptr;                   // mean-mode lines (3 threads)
   double *stat = nullptr;                  // statistics buffers (stat_layout), made on first use
+  double2 *mid64 = nullptr, *p64 = nullptr;  // mixed handles: FP64 slab [6][nm] and products [6][ns]
+                                             // of the pressure / statistics pass, made on first use
   cudaStream_t side = nullptr;             // mean-mode lines run here, forked from / joined to stream
   cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   cudaStream_t copy = nullptr;             // host <-> device copies of kmm_step_host, beside stream
@@ -154,11 +156,12 @@ struct OpsOffsets {
 OpsOffsets ops_offsets(int bw, int ny);
 
 // Kernel launchers (transforms.cu, labs_kernels.cu).
+// fp64: compute in FP64 on a mixed handle too (mid then holds double2 lines; zfwd writes double2).
 cudaError_t launch_zinv(Handle &h, const double2 *src_planes, void *mid, int nfield,
-                        cudaStream_t st);
+                        cudaStream_t st, bool fp64 = false);
 cudaError_t launch_xphys(Handle &h, void *mid, int substep, cudaStream_t st);
 cudaError_t launch_zfwd(Handle &h, const void *mid, void *dst_planes, int nfield, double scale,
-                        bool dst_fp64, cudaStream_t st);
+                        bool dst_fp64, cudaStream_t st, bool fp64 = false);
 cudaError_t launch_update_dt(Handle &h, int substep, cudaStream_t st);
 cudaError_t launch_begin_substep(Handle &h, int substep, cudaStream_t st);
 cudaError_t launch_init_stores(Handle &h, cudaStream_t st);
@@ -210,9 +213,11 @@ void tile_shapes(const Handle &h, int zvar, int xvar, int *z_lines, int *x_rows,
 // Runs the autotuner (tune.cu) on h's grid and buffers; the state is left unchanged.
 int autotune(Handle &h, kmm_tuning *out);
 // Four-step transforms (transforms2.cu); return cudaErrorNotSupported for other lengths.
-cudaError_t launch_zinv2(Handle &h, const double2 *src_planes, void *mid, int nfield, cudaStream_t st);
-// stat: the statistics-step variant (f6 = v v, no CFL); mom (stat only, may be null) receives
-// per-block moment sums [ny][xphys2_row_blocks(h)][kNumMoments].
+cudaError_t launch_zinv2(Handle &h, const double2 *src_planes, void *mid, int nfield, cudaStream_t st,
+                         bool fp64 = false);
+// stat: the statistics-step variant (f6 = v v, no CFL), in FP64 on every handle (mid holds
+// double2 lines); mom (stat only, may be null) receives per-block moment sums
+// [ny][xphys2_row_blocks(h)][kNumMoments].
 cudaError_t launch_xphys2(Handle &h, void *mid, int substep, cudaStream_t st, bool stat = false,
                           double *mom = nullptr);
 int xphys2_row_blocks(const Handle &h);
@@ -221,7 +226,7 @@ int xphys2_row_blocks(const Handle &h);
 // and slots 0..3 the lambda of u, v, w, theta on exit.
 cudaError_t launch_xadj2(Handle &h, const double2 *base_mid, double2 *lmid, double scale, cudaStream_t st);
 cudaError_t launch_zfwd2(Handle &h, const void *mid, void *dst_planes, int nfield, double scale,
-                         bool dst_fp64, cudaStream_t st);
+                         bool dst_fp64, cudaStream_t st, bool fp64 = false);
 // Per-mode solves of one substep (wavespace_split.cu): hvhg, Helmholtz and assembly kernels on
 // st, the mean lines on h.side (joined back to st before return).
 cudaError_t launch_wavespace_split(Handle &h, int substep, const double *dt_override, cudaStream_t st);
@@ -235,9 +240,13 @@ cudaError_t launch_ws_assemble(Handle &h, int substep, const double *dt_override
 cudaError_t launch_ws_assemble_only(Handle &h, int substep, const double *dt_ptr, cudaStream_t st);
 cudaError_t launch_ws_join(Handle &h, cudaStream_t st);
 // The pressure of the state (pressure.cu): p planes [y][mode] into out, with the wall values
-// bc [2][nmodes] (launch_ydiff); mom as in launch_xphys2.  Uses MID, P, the solver lines zc
-// and U region 0 as scratch; cudaErrorNotSupported for x lengths without a four-step shape.
+// bc [2][nmodes] (launch_ydiff); mom as in launch_xphys2.  The products are formed in FP64 on
+// every handle (a mixed handle's in mid64 / p64, which diag_buffers makes).  Uses MID and P (or
+// mid64 and p64), the solver lines zc and U region 0 as scratch; cudaErrorNotSupported for x
+// lengths without a four-step shape.
 cudaError_t launch_pressure(Handle &h, double2 *out, const double2 *bc, double *mom, cudaStream_t st);
+// Makes a mixed handle's mid64 and p64 (nothing on an FP64 handle); a KMM_ERR_* code.
+int diag_buffers(Handle &h);
 // y derivatives of the state (stats.cu): for each field f in {u, v, w} with bit f of mask set,
 // ec line f = D1 D0^{-1} f per mode (zc lines 0..2 scratch); with the v bit set, dvw lines 0
 // and 1 = the pressure wall values nu (D2 D0^{-1} v) on rows 1 and ny.

@@ -10,7 +10,10 @@
 //   k_ydiff computes them),
 //   (D2 - k^2 D0 with D1 rows at the walls) c = rhs,  p = D0 c,
 // and p = -<vv> for the (0,0) mode.  One thread per mode runs the six sweeps (sweeps.cuh): this
-// is a diagnostic of statistics steps, not part of the time step.
+// is a diagnostic of statistics steps, not part of the time step, and its products are formed in
+// FP64 on every handle.  In FP32 (a mixed handle's step precision) the y derivatives of the
+// third-moment and pressure-covariance averages, whose terms cancel to about 1e-2 of their size,
+// carried the rounding of the physical velocities to 1.2e-5 of the line.
 #include <cuda_runtime.h>
 
 #include "kmm_internal.h"
@@ -23,7 +26,7 @@ namespace {
 struct PpeArgs {
   int ny, nxh, nz;
   int64_t nmodes, ns;
-  const void *P;      // products f1..f6 in slots 0..5 (float2 or double2)
+  const double2 *P;   // products f1..f6 in slots 0..5
   double2 *zl;        // 2 complex scratch lines
   const double2 *bc;  // [2][nmodes] wall values of rows 1 and ny
   double *ub;         // U factor region
@@ -32,14 +35,7 @@ struct PpeArgs {
   double2 *out;       // pressure planes [y][mode]
 };
 
-template <typename PT> __device__ __forceinline__ double2 ldp(const PT *p);
-template <> __device__ __forceinline__ double2 ldp<double2>(const double2 *p) { return *p; }
-template <> __device__ __forceinline__ double2 ldp<float2>(const float2 *p) {
-  const float2 v = *p;
-  return make_double2((double)v.x, (double)v.y);
-}
-
-template <int BW, typename PT>
+template <int BW>
 __global__ void __launch_bounds__(128) k_ppe(PpeArgs a) {
   const int64_t m = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (m == 0 || m >= a.nmodes) return;
@@ -50,8 +46,8 @@ __global__ void __launch_bounds__(128) k_ppe(PpeArgs a) {
   const double kx = kxi * a.lmfxr, kz = kzint * a.lmfzr;
   const double k2 = kx * kx + kz * kz, kxkz = kx * kz;
   const Tabs<BW> tb = tabs_at<BW>(a.tabs, n);
-  const PT *P = reinterpret_cast<const PT *>(a.P) + m;
-  auto prod = [&](int slot, int r) { return ldp<PT>(P + slot * ns + (r - 1) * (int)nm); };
+  const double2 *P = a.P + m;
+  auto prod = [&](int slot, int r) { return P[slot * ns + (r - 1) * (int)nm]; };
   auto pfp = [&](int slot, int r) { pf_l1(P + slot * ns + (r - 1) * (int)nm); };
   const DLine Z{a.zl + m, nm}, Rh{a.zl + ns + m, nm}, Pout{a.out + m, nm};
   const UBand<BW> ub = make_uband<BW>(a.ub + m, nm, ns);
@@ -171,7 +167,7 @@ __global__ void __launch_bounds__(256) k_mean_vv(const double2 *__restrict__ v, 
 }
 
 template <int BW>
-cudaError_t ppe_bw(Handle &h, double2 *out, const double2 *bc, cudaStream_t st) {
+cudaError_t ppe_bw(Handle &h, const double2 *P, double2 *out, const double2 *bc, cudaStream_t st) {
   const OpsOffsets off = ops_offsets(h.bw, h.ny);
   PpeArgs a;
   a.ny = h.ny;
@@ -179,7 +175,7 @@ cudaError_t ppe_bw(Handle &h, double2 *out, const double2 *bc, cudaStream_t st) 
   a.nz = h.nz;
   a.nmodes = h.nmodes;
   a.ns = h.ns;
-  a.P = h.P;
+  a.P = P;
   a.zl = h.zc;
   a.bc = bc;
   a.ub = h.ub;
@@ -188,8 +184,7 @@ cudaError_t ppe_bw(Handle &h, double2 *out, const double2 *bc, cudaStream_t st) 
   a.lmfzr = h.lmfzr;
   a.out = out;
   const unsigned blocks = (unsigned)((h.nmodes + 127) / 128);
-  if (h.mixed) k_ppe<BW, float2><<<blocks, 128, 0, st>>>(a);
-  else k_ppe<BW, double2><<<blocks, 128, 0, st>>>(a);
+  k_ppe<BW><<<blocks, 128, 0, st>>>(a);
   return cudaGetLastError();
 }
 
@@ -200,17 +195,20 @@ cudaError_t launch_pressure(Handle &h, double2 *out, const double2 *bc, double *
   k_mean_vv<<<h.ny, 256, 0, st>>>(h.S + h.ns, out, h.nmodes, h.nxh);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return e;
-  // substep-1 products of a statistics step: f1..f6 in P slots 0..5, rescaled
-  if ((e = launch_zinv(h, h.S, h.MID, 4, st)) != cudaSuccess) return e;
-  if ((e = launch_xphys2(h, h.MID, 2, st, true, mom)) != cudaSuccess) return e;
-  if ((e = launch_zfwd(h, h.MID, h.P, 6, h.rescale, !h.mixed, st)) != cudaSuccess) return e;
+  // substep-1 products of a statistics step in FP64: f1..f6 in P slots 0..5, rescaled
+  void *mid = h.mixed ? static_cast<void *>(h.mid64) : h.MID;
+  double2 *P = h.mixed ? h.p64 : static_cast<double2 *>(h.P);
+  if (!mid || !P) return cudaErrorInvalidValue;
+  if ((e = launch_zinv(h, h.S, mid, 4, st, true)) != cudaSuccess) return e;
+  if ((e = launch_xphys2(h, mid, 2, st, true, mom)) != cudaSuccess) return e;
+  if ((e = launch_zfwd(h, mid, P, 6, h.rescale, true, st, true)) != cudaSuccess) return e;
   switch (h.bw) {
-    case 2: return ppe_bw<2>(h, out, bc, st);
-    case 3: return ppe_bw<3>(h, out, bc, st);
-    case 4: return ppe_bw<4>(h, out, bc, st);
-    case 5: return ppe_bw<5>(h, out, bc, st);
-    case 6: return ppe_bw<6>(h, out, bc, st);
-    case 7: return ppe_bw<7>(h, out, bc, st);
+    case 2: return ppe_bw<2>(h, P, out, bc, st);
+    case 3: return ppe_bw<3>(h, P, out, bc, st);
+    case 4: return ppe_bw<4>(h, P, out, bc, st);
+    case 5: return ppe_bw<5>(h, P, out, bc, st);
+    case 6: return ppe_bw<6>(h, P, out, bc, st);
+    case 7: return ppe_bw<7>(h, P, out, bc, st);
     default: return cudaErrorInvalidValue;
   }
 }

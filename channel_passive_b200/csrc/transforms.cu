@@ -292,11 +292,11 @@ static cudaError_t zinv_impl(Handle &h, const double2 *src, void *mid, int nfiel
   return cudaGetLastError();
 }
 
-cudaError_t launch_zinv(Handle &h, const double2 *src, void *mid, int nfield, cudaStream_t st) {
-  const cudaError_t e = launch_zinv2(h, src, mid, nfield, st);
+cudaError_t launch_zinv(Handle &h, const double2 *src, void *mid, int nfield, cudaStream_t st, bool fp64) {
+  const cudaError_t e = launch_zinv2(h, src, mid, nfield, st, fp64);
   if (e != cudaErrorNotSupported) return e;
-  return h.mixed ? zinv_impl<float>(h, src, mid, nfield, st)
-                 : zinv_impl<double>(h, src, mid, nfield, st);
+  return (h.mixed && !fp64) ? zinv_impl<float>(h, src, mid, nfield, st)
+                            : zinv_impl<double>(h, src, mid, nfield, st);
 }
 
 template <typename R, typename D>
@@ -313,10 +313,10 @@ static cudaError_t zfwd_impl(Handle &h, const void *mid, void *dst, int nfield, 
 }
 
 cudaError_t launch_zfwd(Handle &h, const void *mid, void *dst, int nfield, double scale,
-                        bool dst_fp64, cudaStream_t st) {
-  const cudaError_t e = launch_zfwd2(h, mid, dst, nfield, scale, dst_fp64, st);
+                        bool dst_fp64, cudaStream_t st, bool fp64) {
+  const cudaError_t e = launch_zfwd2(h, mid, dst, nfield, scale, dst_fp64, st, fp64);
   if (e != cudaErrorNotSupported) return e;
-  if (h.mixed)
+  if (h.mixed && !fp64)
     return dst_fp64 ? zfwd_impl<float, double2>(h, mid, dst, nfield, scale, st)
                     : zfwd_impl<float, float2>(h, mid, dst, nfield, scale, st);
   return zfwd_impl<double, double2>(h, mid, dst, nfield, scale, st);

@@ -616,10 +616,8 @@ cudaError_t prepare_transforms2() {
   if (e != cudaSuccess) return e;
   for (int N : {12, 24, 36, 48, 72, 96, 144, 192, 288, 384, 576}) {
     with_shape(N, [&]<int N1, int N2>() {
-      using F = TCfg<float>;
       using D = TCfg<double>;
       set_smem(k_xphys2<double, N1, N2, D::ZB, D::ZT, true>, optin);
-      set_smem(k_xphys2<float, N1, N2, F::ZB, F::ZT, true>, optin);
       set_smem(k_xadj2<N1, N2>, optin);
       for (int v = 0; v < 3; ++v)
         with_variant(v, [&]<int V>() {
@@ -713,7 +711,7 @@ bool zfwd_tma_map(const Handle &h, const void *mid, int nfield, CUtensorMap *m) 
 }
 
 // Returns cudaErrorNotSupported when the length has no four-step shape (caller falls back).
-cudaError_t launch_zinv2(Handle &h, const double2 *src, void *mid, int nfield, cudaStream_t st) {
+cudaError_t launch_zinv2(Handle &h, const double2 *src, void *mid, int nfield, cudaStream_t st, bool fp64) {
   cudaError_t err = cudaErrorNotSupported;
   auto go = [&]<typename R>() {
     with_shape(h.nz32, [&]<int N1, int N2>() {
@@ -733,13 +731,13 @@ cudaError_t launch_zinv2(Handle &h, const double2 *src, void *mid, int nfield, c
       });
     });
   };
-  if (h.mixed) go.template operator()<float>();
+  if (h.mixed && !fp64) go.template operator()<float>();
   else go.template operator()<double>();
   return err;
 }
 
 cudaError_t launch_zfwd2(Handle &h, const void *mid, void *dst, int nfield, double scale, bool dst_fp64,
-                         cudaStream_t st) {
+                         cudaStream_t st, bool fp64) {
   cudaError_t err = cudaErrorNotSupported;
   auto go = [&]<typename R, typename D>() {
     with_shape(h.nz32, [&]<int N1, int N2>() {
@@ -760,7 +758,7 @@ cudaError_t launch_zfwd2(Handle &h, const void *mid, void *dst, int nfield, doub
       });
     });
   };
-  if (h.mixed) {
+  if (h.mixed && !fp64) {
     if (dst_fp64) go.template operator()<float, double2>();
     else go.template operator()<float, float2>();
   } else {
@@ -817,7 +815,7 @@ void tile_shapes(const Handle &h, int zvar, int xvar, int *z_lines, int *x_rows,
 }
 
 int xphys2_row_blocks(const Handle &h) {
-  const int zb = h.mixed ? TCfg<float>::ZB : TCfg<double>::ZB;
+  constexpr int zb = TCfg<double>::ZB;  // the statistics x pass computes in FP64 on every handle
   return (h.nz32 + zb - 1) / zb;
 }
 
@@ -838,13 +836,15 @@ cudaError_t launch_xphys2(Handle &h, void *mid, int substep, cudaStream_t st, bo
   auto go = [&]<typename R>() {
     with_shape(h.nx32, [&]<int N1, int N2>() {
       using C = typename Cpx<R>::T;
-      if (stat) {
-        // the statistics variant keeps the default shape: its moment sums are laid out per row block
-        using T = TCfg<R>;
-        dim3 grid((unsigned)((h.nz32 + T::ZB - 1) / T::ZB), (unsigned)h.ny);
-        k_xphys2<R, N1, N2, T::ZB, T::ZT, true><<<grid, T::ZT, x_smem<R, N1, N2>(), st>>>(reinterpret_cast<C *>(mid), h.px, a);
-        err = cudaGetLastError();
-        return;
+      if constexpr (sizeof(R) == 8) {
+        if (stat) {
+          // the statistics variant keeps the default shape: its moment sums are laid out per row block
+          using T = TCfg<R>;
+          dim3 grid((unsigned)((h.nz32 + T::ZB - 1) / T::ZB), (unsigned)h.ny);
+          k_xphys2<R, N1, N2, T::ZB, T::ZT, true><<<grid, T::ZT, x_smem<R, N1, N2>(), st>>>(reinterpret_cast<C *>(mid), h.px, a);
+          err = cudaGetLastError();
+          return;
+        }
       }
       with_variant(h.tune.x, [&]<int V>() {
         constexpr int VV = tuned_variant<N1 * N2, V>();
@@ -860,7 +860,10 @@ cudaError_t launch_xphys2(Handle &h, void *mid, int substep, cudaStream_t st, bo
       });
     });
   };
-  if (h.mixed) go.template operator()<float>();
+  // the statistics products run in FP64 on every handle: a diagnostic off the step's path, whose
+  // y derivatives of third moments and pressure covariances would carry FP32 rounding of the
+  // physical velocities past 1e-5 of the line
+  if (h.mixed && !stat) go.template operator()<float>();
   else go.template operator()<double>();
   return err;
 }

@@ -202,7 +202,9 @@ int kmm_step_host(kmm_handle *h, double *U, int nf, double *rk, int nsteps, kmm_
  * D1 (Neumann) rows at the walls whose values are stat_PPE_boundary = nu d2v/dy2 of the
  * state's v at the walls (get_y_dir_deriv_of_field_with_PPE_BC, get_statistics.f90:689-719),
  * and -<vv> for the (0,0) mode.  P receives U(:,:,:,6) of the reference, (ny, nxh, nz)
- * complex128 in host memory.  The state is not changed. */
+ * complex128 in host memory.  The state is not changed.  The products are formed in FP64 on
+ * a mixed-precision handle too; there the first call allocates an FP64 slab and product
+ * planes (96 bytes per point of the 3/2 grid's kx-half plus 96 per spectral point). */
 int kmm_get_pressure(kmm_handle *h, double *P);
 
 /* Statistics of the current state, as a statistics step computes them at the start of RK
@@ -218,7 +220,9 @@ int kmm_get_pressure(kmm_handle *h, double *P);
  *                                            (write_energy_spectra.f90:218-219)
  *   centre   [2]                             U_c and T_c
  *   P        (ny, nxh, nz) complex128        the pressure (kmm_get_pressure)
- * The state is not changed.  The first call allocates the statistics buffers on the device. */
+ * The state is not changed.  The first call allocates the statistics buffers on the device
+ * (and on a mixed-precision handle the FP64 buffers of kmm_get_pressure: every statistic is
+ * computed in FP64 in both precisions). */
 #define KMM_STAT_NLINES 58
 #define KMM_STAT_NSPEC 18
 int kmm_get_statistics(kmm_handle *h, double *lines, double *spec_kx, double *spec_kz,
