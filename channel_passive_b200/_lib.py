@@ -79,14 +79,14 @@ class KmmTuning(C.Structure):
         ("modes_per_block", C.c_int32), ("u_layout", C.c_int32), ("assemble_threads", C.c_int32),
         ("tuned", C.c_int32), ("tables_shared", C.c_int32),
         ("helm_modes_per_block", C.c_int32), ("helm_tables_shared", C.c_int32), ("helm_stage_ahead", C.c_int32),
-        ("z_tma", C.c_int32), ("hvhg_stage_ahead", C.c_int32), ("reserved", C.c_int32),
+        ("z_tma", C.c_int32), ("hvhg_stage_ahead", C.c_int32), ("factor_cache", C.c_int32),
         ("ms_z", C.c_double * 3), ("ms_x", C.c_double * 3), ("ms_modes", C.c_double * 2),
         ("ms_layout", C.c_double * 2), ("ms_assemble", C.c_double * 3), ("ms_tables", C.c_double * 2),
         ("ms_helm", C.c_double * 12), ("ms_z_tma", C.c_double * 3), ("ms_hvhg", C.c_double * 12),
     ]
 
     def as_dict(self):
-        d = {f: getattr(self, f) for f, _ in self._fields_ if f != "reserved"}
+        d = {f: getattr(self, f) for f, _ in self._fields_}
         for k, v in d.items():
             if not isinstance(v, (int, float)):
                 d[k] = list(v)

@@ -533,6 +533,18 @@ int kmm_create(const kmm_config *cfg, kmm_handle **out) {
   if ((rc = dalloc(*h, &h->ub, (3 + x2) * (size_t)split_ub_role(*h)))) return fail(rc);
   if ((rc = dalloc(*h, &h->vf, (size_t)vop_factor_doubles(*h)))) return fail(rc);
   if ((rc = dalloc(*h, &h->dvw, 3 * (size_t)h->nmodes))) return fail(rc);
+  if (factor_cache_possible(*h)) {
+    // per substep: the two Helmholtz operators' factors, the four influence lines, v_h's walls
+    if ((rc = dalloc(*h, &h->hf, 6 * (size_t)vop_factor_doubles(*h)))) return fail(rc);
+    if ((rc = dalloc(*h, &h->hinf, 12 * (size_t)h->ns))) return fail(rc);
+    if ((rc = dalloc(*h, &h->hdvh, 3 * (size_t)h->nmodes))) return fail(rc);
+    if ((rc = dalloc(*h, &h->fcdt, 3))) return fail(rc);
+    const double none[3] = {NAN, NAN, NAN};  // no dt cached yet
+    if (cudaMemcpy(h->fcdt, none, sizeof(none), cudaMemcpyHostToDevice) != cudaSuccess) {
+      set_error("factor cache set-up failed");
+      return fail(KMM_ERR_CUDA);
+    }
+  }
   if ((rc = dalloc(*h, &h->w00, (3 + x2) * (size_t)h->ny * (8 + 2 * h->bw)))) return fail(rc);
   if ((rc = dalloc(*h, &h->staging, 10 * h->ns))) return fail(rc);
   if ((rc = dalloc(*h, &h->dsc, 1))) return fail(rc);
@@ -573,6 +585,8 @@ int kmm_create(const kmm_config *cfg, kmm_handle **out) {
     }
   }
   default_solver_shapes(*h);  // the untuned solver launch shapes
+  // with a fixed time step the Helmholtz sweeps read their operators' cached factors
+  h->tune.fcache = h->hf ? 1 : 0;
   // the z transforms stage their input tiles through TMA where the grid allows the tile map
   // (0.062 -> 0.054 ms y_to_x, 312 -> 315 steps/s at 192x129x192 mixed, same-box A/B)
   h->tune.ztma = z_tma_possible(*h, h->tune.z) ? 1 : 0;
@@ -592,7 +606,7 @@ int kmm_destroy(kmm_handle *hh) {
   adjoint_free(*h);
   void *ptrs[] = {h->S, h->RK, h->P, h->MID, h->dops, h->gains, h->vwall, h->zc,
                   h->ec, h->xr, h->ub, h->vf, h->dvw, h->w00, h->staging, h->stat,
-                  h->mid64, h->p64, h->fftpos, h->tw64, h->tw32, h->dsc};
+                  h->mid64, h->p64, h->hf, h->hinf, h->hdvh, h->fcdt, h->fftpos, h->tw64, h->tw32, h->dsc};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   if (h->copy) cudaStreamSynchronize(h->copy);

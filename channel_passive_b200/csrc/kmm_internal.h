@@ -92,6 +92,8 @@ struct Tuning {
   int asm_threads = 256;  // threads per block of the assembly kernel
   int stab = 0;           // 1: the hvhg kernel reads the operator tables from shared memory
   int hvstage = 0;        // rows the hvhg sweeps stage ahead through shared memory (0: L1 prefetch)
+  int fcache = 0;         // 1: the Helmholtz sweeps read the per-substep operator factors and
+                          // influence solutions cached for the current dt (fixed time step only)
   bool tuned = false;
   // device ms of every candidate of the last autotune (kmm_tuning's ms_* fields)
   double ms_z[3] = {}, ms_x[3] = {}, ms_modes[2] = {}, ms_layout[2] = {}, ms_assemble[3] = {}, ms_tables[2] = {};
@@ -126,6 +128,14 @@ struct Handle {
   double *vf = nullptr;                    //                  v operator LU per mode (vop_factor_doubles)
   double2 *dvw = nullptr;                  //                  wall derivatives [3][nmodes]
   double *w00 = nullptr;                   // mean-mode lines (3 threads)
+  // With a fixed time step the Helmholtz operators of each substep (theta's and the one g and
+  // phi share) do not change between steps: their profile LU per mode, the influence solutions
+  // phi_h, D2 phi_h, v_h, dv_h / dy and v_h's wall derivatives, cached for the dt in fcdt
+  // (factor_cache_possible; made at kmm_create).
+  double *hf = nullptr;                    // [substep][theta, g/phi] LBand then UBand (vop_factor_doubles)
+  double *hinf = nullptr;                  // [substep][4][ny][nmodes] influence lines
+  double2 *hdvh = nullptr;                 // [substep][nmodes] (dv_h(1), dv_h(n))
+  double *fcdt = nullptr;                  // [substep] the dt the cache holds (NaN: none)
   double *stat = nullptr;                  // statistics buffers (stat_layout), made on first use
   double2 *mid64 = nullptr, *p64 = nullptr;  // mixed handles: FP64 slab [6][nm] and products [6][ns]
                                              // of the pressure / statistics pass, made on first use
@@ -265,6 +275,8 @@ cudaError_t launch_statistics(Handle &h, cudaStream_t st);
 // whole (L then U), and the kernel that fills it once per handle.
 int64_t vop_lband_doubles(const Handle &h);
 int64_t vop_factor_doubles(const Handle &h);
+// Whether the handle can cache the Helmholtz factors: a fixed time step and one scalar.
+bool factor_cache_possible(const Handle &h);
 cudaError_t launch_vop_factor(Handle &h, cudaStream_t st);
 // Doubles of U factor storage per solver role.
 int64_t split_ub_role(const Handle &h);

@@ -282,6 +282,7 @@ int kmm_get_tuning(const kmm_handle *hh, kmm_tuning *out) {
   out->assemble_threads = h.tune.asm_threads;
   out->tuned = h.tune.tuned ? 1 : 0;
   out->tables_shared = h.tune.stab;
+  out->factor_cache = h.tune.fcache;
   std::memcpy(out->ms_z, h.tune.ms_z, sizeof(out->ms_z));
   std::memcpy(out->ms_x, h.tune.ms_x, sizeof(out->ms_x));
   std::memcpy(out->ms_modes, h.tune.ms_modes, sizeof(out->ms_modes));
@@ -317,8 +318,9 @@ int kmm_set_tuning(kmm_handle *hh, const kmm_tuning *t) {
                        (t->helm_stage_ahead == 1 || t->helm_stage_ahead == 2) &&
                        helm_shape_fits(h, hg, t->helm_tables_shared, t->helm_stage_ahead);
   const bool tma_ok = t->z_tma == 0 || (t->z_tma == 1 && zv >= 0 && z_tma_possible(h, zv));
+  const bool fc_ok = t->factor_cache == 0 || (t->factor_cache == 1 && h.hf);
   if (zv < 0 || xv < 0 || g == 0 || (g == 2 && h.nsc != 1) || (t->u_layout != 0 && t->u_layout != 1) || !asm_ok ||
-      !tab_ok || !helm_ok || !tma_ok) {
+      !tab_ok || !helm_ok || !tma_ok || !fc_ok) {
     set_error("kmm_set_tuning: a requested shape is not among this grid's candidates (see kmm_autotune)");
     return KMM_ERR_ARG;
   }
@@ -333,6 +335,7 @@ int kmm_set_tuning(kmm_handle *hh, const kmm_tuning *t) {
   next.stage = t->helm_stage_ahead;
   next.ztma = t->z_tma;
   next.hvstage = t->hvhg_stage_ahead;
+  next.fcache = t->factor_cache;
   DeviceGuard dg(h.cfg.device);
   cudaStreamSynchronize(h.stream);
   h.tune = next;

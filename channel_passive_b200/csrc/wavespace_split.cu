@@ -80,6 +80,14 @@ struct SplitArgs {
   int ulayout;       // U factor layout of the per-role regions (Tuning::ulayout)
   int stab;          // 1: k_hvhg copies the operator tables it reads to shared memory
   int hstab;         // 1: k_helmholtz does (Tuning::hstab)
+  // this substep's influence lines phi_h, D2 phi_h, v_h, dv_h / dy [4][ny][nm] and v_h's wall
+  // derivatives [nm] (the factor cache's slots with Tuning::fcache, else xr lines 1..4, dv line 2)
+  double *xinf;
+  double2 *dvh;
+  // Tuning::fcache: this substep's cached LU of theta's operator (fth) and of the one g and phi
+  // share (fgp), each an LBand with its UBand vf_l doubles on, and the dt they hold (fcdt)
+  double *fth, *fgp;
+  double *fcdt;
 };
 
 // Operator tables in shared memory (SplitArgs::stab).  Every lane of a warp reads the same table
@@ -368,7 +376,10 @@ k_hvhg(SplitArgs a) {
 template <int BW>
 constexpr int kHelmUnits = 5 + BW;
 
-template <int BW, int ROLE, typename PT, int SA>
+// FC: the operator's LU comes from the factor cache (Tuning::fcache), so the forward sweep is a
+// substitution with the cached L (fwd_lband, the arithmetic of the LuSweep chains it replaces)
+// and the backward sweep reads the cached U.
+template <int BW, int ROLE, typename PT, int SA, bool FC = false>
 __device__ __forceinline__ void helmholtz_role(const SplitArgs &a, const Tabs<BW> &tb, int64_t m,
                                                const Ring<kHelmUnits<BW>, SA + 1> &ring) {
   const int n = a.ny, s = a.substep;
@@ -377,7 +388,8 @@ __device__ __forceinline__ void helmholtz_role(const SplitArgs &a, const Tabs<BW
   const double k2 = mode_k(a, m).k2;
   auto hl = [&](int i) { return DLine{a.hl + i * ns + m, nm}; };
   auto row = [&](const auto *base, int r) { return base + (r - 1) * (int)nm; };
-  const UBand<BW> ub = role_uband<BW>(a, ROLE, m);
+  double *const fset = ROLE == 0 ? a.fth : a.fgp;  // (FC; roles 0 and 1 only)
+  const UBand<BW> ub = FC ? make_uband<BW>(fset + a.vf_l + m, nm, ns) : role_uband<BW>(a, ROLE, m);
   const DLine Zr{a.zl + ROLE * ns + m, nm};
 
   // RK right-hand side (solve_g.f90:84-123): rows 1 and n are the Dirichlet rows (zero)
@@ -413,19 +425,30 @@ __device__ __forceinline__ void helmholtz_role(const SplitArgs &a, const Tabs<BW
     else return zadd(hv(H_G2).ld(r), hv(H_G3).ld(r));
   };
   auto rh = [&](int step, int k) { return ring_hv<PT>(ring, step, k); };
-  // forward units: 0 store, 1 hA, 2 hB, 3 D2 store (substep 1)
-  lu_fwd<BW, 1, 0, SA, true>(n, [&](int r, double *rw, bool c) { helm_row<BW>(tb, r, n, dummy, beta, rw, c); },
-      [&](int r, double2 *bc, double *) {
-        const double2 h = SCAL ? rh(r, 1) : zadd(rh(r, 1), rh(r, 2));
-        bc[0] = rhs(ring.c(r, 0), h, s == 1 ? ring.c(r, 3) : z2(0.0, 0.0), visc, r);
-      },
-      [&](int r, const double2 *zc, const double *) { Zr.st(r, zc[0]); }, ub,
-      [&](int r) {
-        ring.get(r, 0, row(store.p, r));
-        ring.get(r, 1, row(hA, r));
-        if (ROLE == 1) ring.get(r, 2, row(hB, r));
-        if (s == 1) ring.get(r, 3, row(d2l.p, r));
-      });
+  // forward units: 0 store, 1 hA, 2 hB, 3 D2 store (substep 1); FC: 4..4+BW L(r, r-d)
+  auto fin = [&](int r, double2 *bc, double *) {
+    const double2 h = SCAL ? rh(r, 1) : zadd(rh(r, 1), rh(r, 2));
+    bc[0] = rhs(ring.c(r, 0), h, s == 1 ? ring.c(r, 3) : z2(0.0, 0.0), visc, r);
+  };
+  auto fout = [&](int r, const double2 *zc, const double *) { Zr.st(r, zc[0]); };
+  auto fpf = [&](int r) {
+    ring.get(r, 0, row(store.p, r));
+    ring.get(r, 1, row(hA, r));
+    if (ROLE == 1) ring.get(r, 2, row(hB, r));
+    if (s == 1) ring.get(r, 3, row(d2l.p, r));
+    if constexpr (FC) {
+#pragma unroll
+      for (int d = 0; d <= BW; ++d) ring.get(r, 4 + d, fset + m + d * (int)ns + (r - 1) * (int)nm);
+    }
+  };
+  if constexpr (FC) {
+    const LBand<BW> fl = make_lband<BW>(fset + m, nm, ns, n);
+    fwd_lband<BW, 1, 0, SA, true>([&](int r, int d) { return d <= BW ? ring.d(r, 4 + d) : fl.get(r, d); }, n, fin,
+                                  fout, fpf);
+  } else {
+    lu_fwd<BW, 1, 0, SA, true>(n, [&](int r, double *rw, bool c) { helm_row<BW>(tb, r, n, dummy, beta, rw, c); },
+                               fin, fout, ub, fpf);
+  }
   // backward units: 0 Z(r), 1..BW U(r, e), BW+1 hA(q), BW+2 hB(q) with q = r + BW
   const DLine out{ROLE == 0 ? a.S + 3 * ns + m : ROLE == 3 ? a.S + 4 * ns + m : a.S + m, nm};
   bwd_emit<BW, 1, 0, SA, true>(n, [&](int r, int e) { return e <= BW ? ring.d(r, e) : ub.get(r, e); },
@@ -457,7 +480,9 @@ __device__ __forceinline__ void helmholtz_role(const SplitArgs &a, const Tabs<BW
 //     (solve_v_f.f90:140-153, the LU of solve_g.f90:42-71);
 //   (D2 - k^2 D0) v_p = phi_p with the wall velocities at rows 1 and n, and v_h = phi_h with zero
 //     walls (solve_v_f.f90:202-272).
-template <int BW, typename PT, int SA>
+// FC: both operators' factors are cached, and so are the influence solutions (k_helm_factor):
+// each sweep carries the complex chain alone.
+template <int BW, typename PT, int SA, bool FC = false>
 __device__ __forceinline__ void helmholtz_phi_v(const SplitArgs &a, const Tabs<BW> &tb, int64_t m,
                                                 const Ring<kHelmUnits<BW>, SA + 1> &ring) {
   const int n = a.ny, s = a.substep;
@@ -466,10 +491,11 @@ __device__ __forceinline__ void helmholtz_phi_v(const SplitArgs &a, const Tabs<B
   const double k2 = mode_k(a, m).k2;
   auto hl = [&](int i) { return DLine{a.hl + i * ns + m, nm}; };
   auto row = [&](const auto *base, int r) { return base + (r - 1) * (int)nm; };
-  const UBand<BW> ub = role_uband<BW>(a, 2, m);
+  const UBand<BW> ub = FC ? make_uband<BW>(a.fgp + a.vf_l + m, nm, ns) : role_uband<BW>(a, 2, m);
   const DLine Zr{a.zl + 2 * ns + m, nm};
-  const RLine Xz{a.xr + m, nm}, X1{a.xr + ns + m, nm}, X2{a.xr + 2 * ns + m, nm};
-  const RLine X4{a.xr + 3 * ns + m, nm}, X5{a.xr + 4 * ns + m, nm};
+  const RLine Xz{a.xr + m, nm}, X1{a.xinf + m, nm}, X2{a.xinf + ns + m, nm};
+  const RLine X4{a.xinf + 2 * ns + m, nm}, X5{a.xinf + 3 * ns + m, nm};
+  constexpr int XO = FC ? 0 : 1;  // units the influence chains take in a sweep
 
   const double beta = dt * rkc(2, s) * nu;
   const double dummy = 1.0 + beta * k2;
@@ -494,49 +520,73 @@ __device__ __forceinline__ void helmholtz_phi_v(const SplitArgs &a, const Tabs<B
     const double alpha = dt * rkc(1, s + 1) * nu, zeta = dt * rkc(4, s + 1);
     return zadd(zadd(zscale(zeta, h), zscale(1.0 - alpha * k2, f)), zscale(alpha, d2f));
   };
-  // phi forward units: 0 store, 1..3 HV0, V2, V3, 4 D2 store (substep 1)
-  lu_fwd<BW, 1, 1, SA, true>(n, [&](int r, double *rw, bool c) { helm_row<BW>(tb, r, n, dummy, beta, rw, c); },
-      [&](int r, double2 *bc, double *br) {
-        const double2 h = zadd(rh(r, 1), zadd(rh(r, 2), rh(r, 3)));
-        bc[0] = rhs(ring.c(r, 0), h, s == 1 ? ring.c(r, 4) : z2(0.0, 0.0), r);
-        br[0] = (r == 1) ? p0 : 0.0;
-      },
-      [&](int r, const double2 *zc, const double *zr) {
-        Zr.st(r, zc[0]);
-        Xz.st(r, zr[0]);
-      },
-      ub,
-      [&](int r) {
-        ring.get(r, 0, row(store.p, r));
-        ring.get(r, 1, row(h0, r));
-        ring.get(r, 2, row(h1, r));
-        ring.get(r, 3, row(h2, r));
-        if (s == 1) ring.get(r, 4, row(d2l.p, r));
-      });
+  // phi forward units: 0 store, 1..3 HV0, V2, V3, 4 D2 store (substep 1).  FC: 4..4+BW
+  // L(r, r-d) of the cached factor instead, and the D2 store (substep 1) prefetched into L1
+  if constexpr (FC) {
+    const LBand<BW> fl = make_lband<BW>(a.fgp + m, nm, ns, n);
+    fwd_lband<BW, 1, 0, SA, true>([&](int r, int d) { return d <= BW ? ring.d(r, 4 + d) : fl.get(r, d); }, n,
+        [&](int r, double2 *bc, double *) {
+          const double2 h = zadd(rh(r, 1), zadd(rh(r, 2), rh(r, 3)));
+          bc[0] = rhs(ring.c(r, 0), h, s == 1 ? d2l.ld(r) : z2(0.0, 0.0), r);
+        },
+        [&](int r, const double2 *zc, const double *) { Zr.st(r, zc[0]); },
+        [&](int r) {
+          ring.get(r, 0, row(store.p, r));
+          ring.get(r, 1, row(h0, r));
+          ring.get(r, 2, row(h1, r));
+          ring.get(r, 3, row(h2, r));
+          if (s == 1) pf_l1(row(d2l.p, r));
+#pragma unroll
+          for (int d = 0; d <= BW; ++d) ring.get(r, 4 + d, a.fgp + m + d * (int)ns + (r - 1) * (int)nm);
+        });
+  } else {
+    lu_fwd<BW, 1, 1, SA, true>(n, [&](int r, double *rw, bool c) { helm_row<BW>(tb, r, n, dummy, beta, rw, c); },
+        [&](int r, double2 *bc, double *br) {
+          const double2 h = zadd(rh(r, 1), zadd(rh(r, 2), rh(r, 3)));
+          bc[0] = rhs(ring.c(r, 0), h, s == 1 ? ring.c(r, 4) : z2(0.0, 0.0), r);
+          br[0] = (r == 1) ? p0 : 0.0;
+        },
+        [&](int r, const double2 *zc, const double *zr) {
+          Zr.st(r, zc[0]);
+          Xz.st(r, zr[0]);
+        },
+        ub,
+        [&](int r) {
+          ring.get(r, 0, row(store.p, r));
+          ring.get(r, 1, row(h0, r));
+          ring.get(r, 2, row(h1, r));
+          ring.get(r, 3, row(h2, r));
+          if (s == 1) ring.get(r, 4, row(d2l.p, r));
+        });
+  }
   // phi backward units: 0 Z(r), 1 Xz(r), 2..BW+1 U(r, e), BW+2..BW+4 HV0, V2, V3 at q = r + BW
+  // (FC: no Xz, the others one unit lower)
   const DLine out{a.zl + 4 * ns + m, nm};
-  bwd_emit<BW, 1, 1, SA, true>(n, [&](int r, int e) { return e <= BW ? ring.d(r, 1 + e) : ub.get(r, e); },
+  bwd_emit<BW, 1, FC ? 0 : 1, SA, true>(n, [&](int r, int e) { return e <= BW ? ring.d(r, XO + e) : ub.get(r, e); },
       [&](int r, double2 *zc, double *zr) {
         zc[0] = ring.c(r, 0);
-        zr[0] = ring.d(r, 1);
+        if constexpr (!FC) zr[0] = ring.d(r, 1);
       },
       [&](int q, int r, const double2 (&wc)[1][2 * BW + 1], const double (&wr)[1][2 * BW + 1]) {
         const double2 f = mvc<BW>(tb.t0, q, r, wc[0]), d2f = mvc<BW>(tb.t2, q, r, wc[0]);
         out.st(q, f);
-        const double2 h = (q == r + BW) ? zadd(rh(r, BW + 2), zadd(rh(r, BW + 3), rh(r, BW + 4))) : hsum(q);
+        const double2 h = (q == r + BW) ? zadd(rh(r, BW + 1 + XO), zadd(rh(r, BW + 2 + XO), rh(r, BW + 3 + XO)))
+                                        : hsum(q);
         store.st(q, store_new(h, f, d2f));
-        X1.st(q, mvr<BW>(tb.t0, q, r, wr[0]));  // phi_h (real part = imaginary part)
-        X2.st(q, mvr<BW>(tb.t2, q, r, wr[0]));  // D2 phi_h
+        if constexpr (!FC) {
+          X1.st(q, mvr<BW>(tb.t0, q, r, wr[0]));  // phi_h (real part = imaginary part)
+          X2.st(q, mvr<BW>(tb.t2, q, r, wr[0]));  // D2 phi_h
+        }
       },
       [&](int r) {
         ring.get(r, 0, row(Zr.p, r));
-        ring.get(r, 1, row(Xz.p, r));
+        if constexpr (!FC) ring.get(r, 1, row(Xz.p, r));
 #pragma unroll
-        for (int e = 1; e <= BW; ++e) ring.get(r, 1 + e, ub.p + (e - 1) * (int)ub.es + (r - 1) * (int)ub.s);
+        for (int e = 1; e <= BW; ++e) ring.get(r, XO + e, ub.p + (e - 1) * (int)ub.es + (r - 1) * (int)ub.s);
         if (r <= n - 2 * BW) {
-          ring.get(r, BW + 2, row(h0, r + BW));
-          ring.get(r, BW + 3, row(h1, r + BW));
-          ring.get(r, BW + 4, row(h2, r + BW));
+          ring.get(r, BW + 1 + XO, row(h0, r + BW));
+          ring.get(r, BW + 2 + XO, row(h1, r + BW));
+          ring.get(r, BW + 3 + XO, row(h2, r + BW));
         }
       });
   // (D2 - k^2 D0) v = phi with v_p = the wall velocity at rows 1 and n, v_h = 0 there.
@@ -564,30 +614,31 @@ __device__ __forceinline__ void helmholtz_phi_v(const SplitArgs &a, const Tabs<B
   // the v operator does not change during a run: its factors come from k_vop_factor
   const LBand<BW> vl = make_lband<BW>(a.vf + m, nm, ns, n);
   const UBand<BW> vu = make_uband<BW>(a.vf + a.vf_l + m, nm, ns);
-  // v forward units: 0 phi_p(r), 1 phi_h(r), 2..BW+2 L(r, r-d) for d = 0..BW
-  fwd_lband<BW, 1, 1, SA, true>([&](int r, int d) { return d <= BW ? ring.d(r, 2 + d) : vl.get(r, d); }, n,
+  // v forward units: 0 phi_p(r), 1 phi_h(r), 2..BW+2 L(r, r-d) for d = 0..BW (FC: no phi_h)
+  fwd_lband<BW, 1, FC ? 0 : 1, SA, true>(
+      [&](int r, int d) { return d <= BW ? ring.d(r, 1 + XO + d) : vl.get(r, d); }, n,
       [&](int r, double2 *bc, double *br) {
         const bool wall = (r == 1 || r == n);
         bc[0] = (r == 1) ? vlo : (r == n) ? vhi : ring.c(r, 0);
-        br[0] = wall ? 0.0 : ring.d(r, 1);
+        if constexpr (!FC) br[0] = wall ? 0.0 : ring.d(r, 1);
       },
       [&](int r, const double2 *zc, const double *zr) {
         Zr.st(r, zc[0]);
-        Xz.st(r, zr[0]);
+        if constexpr (!FC) Xz.st(r, zr[0]);
       },
       [&](int r) {
         ring.get(r, 0, row(out.p, r));
-        ring.get(r, 1, row(X1.p, r));
+        if constexpr (!FC) ring.get(r, 1, row(X1.p, r));
 #pragma unroll
-        for (int d = 0; d <= BW; ++d) ring.get(r, 2 + d, vl.p + d * (int)ns + (r - 1) * (int)nm);
+        for (int d = 0; d <= BW; ++d) ring.get(r, 1 + XO + d, vl.p + d * (int)ns + (r - 1) * (int)nm);
       });
-  // v backward units: 0 Z(r), 1 Xz(r), 2..BW+1 U(r, e)
+  // v backward units: 0 Z(r), 1 Xz(r), 2..BW+1 U(r, e) (FC: no Xz)
   const DLine Sv{a.S + ns + m, nm}, Sw{a.S + 2 * ns + m, nm};
   double dh1 = 0.0, dhn = 0.0;
-  bwd_emit<BW, 1, 1, SA, true>(n, [&](int r, int e) { return e <= BW ? ring.d(r, 1 + e) : vu.get(r, e); },
+  bwd_emit<BW, 1, FC ? 0 : 1, SA, true>(n, [&](int r, int e) { return e <= BW ? ring.d(r, XO + e) : vu.get(r, e); },
       [&](int r, double2 *zc, double *zr) {
         zc[0] = ring.c(r, 0);
-        zr[0] = ring.d(r, 1);
+        if constexpr (!FC) zr[0] = ring.d(r, 1);
       },
       [&](int q, int r, const double2 (&wc)[1][2 * BW + 1], const double (&wr)[1][2 * BW + 1]) {
         const double2 vp = mvc<BW>(tb.t0, q, r, wc[0]), dvp = mvc<BW>(tb.t1, q, r, wc[0]);
@@ -595,19 +646,21 @@ __device__ __forceinline__ void helmholtz_phi_v(const SplitArgs &a, const Tabs<B
         Sw.st(q, dvp);
         if (q == 1) a.dv[m] = dvp;
         if (q == n) a.dv[nm + m] = dvp;
-        const double vh = mvr<BW>(tb.t0, q, r, wr[0]), dvh = mvr<BW>(tb.t1, q, r, wr[0]);
-        X4.st(q, vh);
-        X5.st(q, dvh);
-        if (q == 1) dh1 = dvh;
-        if (q == n) dhn = dvh;
+        if constexpr (!FC) {
+          const double vh = mvr<BW>(tb.t0, q, r, wr[0]), dvh = mvr<BW>(tb.t1, q, r, wr[0]);
+          X4.st(q, vh);
+          X5.st(q, dvh);
+          if (q == 1) dh1 = dvh;
+          if (q == n) dhn = dvh;
+        }
       },
       [&](int r) {
         ring.get(r, 0, row(Zr.p, r));
-        ring.get(r, 1, row(Xz.p, r));
+        if constexpr (!FC) ring.get(r, 1, row(Xz.p, r));
 #pragma unroll
-        for (int e = 1; e <= BW; ++e) ring.get(r, 1 + e, vu.p + (e - 1) * (int)vu.es + (r - 1) * (int)vu.s);
+        for (int e = 1; e <= BW; ++e) ring.get(r, XO + e, vu.p + (e - 1) * (int)vu.es + (r - 1) * (int)vu.s);
       });
-  a.dv[2 * nm + m] = z2(dh1, dhn);
+  if constexpr (!FC) a.dvh[m] = z2(dh1, dhn);
 }
 
 // The profile LU of the v operator (D2 - k^2 D0 with Dirichlet first and last rows, the matrix
@@ -647,11 +700,16 @@ constexpr size_t helm_smem() {
 // look-ahead (Tuning::stage); the bound (384 threads) keeps 168 registers.  Four groups with the
 // tables in shared memory and two steps of look-ahead hold 218 KB at ny = 129, one block (12
 // warps) per SM.
-template <int BW, typename PT, int NS, int SA>
+// FC (one scalar): the sweeps read the factor cache that k_helm_factor filled for this dt, and
+// the kernel records that dt as the one the cache holds.
+template <int BW, typename PT, int NS, int SA, bool FC = false>
 __global__ void __launch_bounds__(NS == 1 ? 4 * kLanes * kHelmRoles : kLanes * (kHelmRoles + 1), NS == 1 ? 1 : 3)
 k_helmholtz(SplitArgs a) {
   extern __shared__ double2 helm_ring[];
   if (a.dsc->err) return;  // a failed dt update leaves the state untouched (uniform over the block)
+  if constexpr (FC) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) *a.fcdt = *a.dt_ptr;  // read by the next k_helm_factor only
+  }
   constexpr int R = kHelmRoles + NS - 1;
   const int role = (threadIdx.x / kLanes) % R, grp = threadIdx.x / (kLanes * R);
   const int64_t m = ((int64_t)blockIdx.x * a.hgroups + grp) * kLanes + (threadIdx.x % kLanes);
@@ -663,13 +721,86 @@ k_helmholtz(SplitArgs a) {
   const Tabs<BW> tb = tabs_at<BW>(t0, a.ny);  // (its L0 and U0 are not read here)
   const Ring<kHelmUnits<BW>, SA + 1> ring{helm_ring + threadIdx.x, (int)blockDim.x};
   switch (role) {
-    case 0: helmholtz_role<BW, 0, PT, SA>(a, tb, m, ring); break;
-    case 1: helmholtz_role<BW, 1, PT, SA>(a, tb, m, ring); break;
-    case 2: helmholtz_phi_v<BW, PT, SA>(a, tb, m, ring); break;
+    case 0: helmholtz_role<BW, 0, PT, SA, FC>(a, tb, m, ring); break;
+    case 1: helmholtz_role<BW, 1, PT, SA, FC>(a, tb, m, ring); break;
+    case 2: helmholtz_phi_v<BW, PT, SA, FC>(a, tb, m, ring); break;
     default:
-      if constexpr (NS == 2) helmholtz_role<BW, 3, PT, SA>(a, tb, m, ring);
+      if constexpr (NS == 2 && !FC) helmholtz_role<BW, 3, PT, SA>(a, tb, m, ring);
       break;
   }
+}
+
+// The factor cache of a substep with a fixed time step (Tuning::fcache), for every mode: the
+// profile LU of theta's operator and of the one g and phi share (alpha D0 - beta D2 with the
+// Dirichlet rows), and the influence solutions phi_h (through that LU) and v_h (through the v
+// operator's factors) with their emitted lines, as k_helmholtz computes them otherwise: the same
+// LuSweep arithmetic, so the same numbers.  A no-op while the cache holds this dt; with a
+// fixed time step it runs once per substep of the run (and again after a change of dt).
+template <int BW>
+__global__ void __launch_bounds__(128) k_helm_factor(SplitArgs a) {
+  if (a.dsc->err || *a.fcdt == *a.dt_ptr) return;
+  const int64_t m = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (m == 0 || m >= a.nmodes) return;
+  const int n = a.ny, s = a.substep;
+  const int64_t nm = a.nmodes, ns = a.ns;
+  const Tabs<BW> tb = tabs_at<BW>(a.tabs, n);
+  const double dt = *a.dt_ptr, k2 = mode_k(a, m).k2;
+  const double2 zero[1] = {z2(0.0, 0.0)};
+  double2 zc[1];
+  double zr[1];
+  {  // theta: nu / pr (solve_t.f90:42-71)
+    const double beta = dt * rkc(2, s) * (a.nu / a.pr), dummy = 1.0 + beta * k2;
+    const LBand<BW> lb = make_lband<BW>(a.fth + m, nm, ns, n);
+    LuSweep<BW, 0, 0, true> lu;
+    lu.init(n, make_uband<BW>(a.fth + a.vf_l + m, nm, ns));
+    for (int r = 1; r <= n; ++r) {
+      const double br[1] = {0.0};
+      lu.step(r, [&](int rr, double *row, bool c) { helm_row<BW>(tb, rr, n, dummy, beta, row, c); }, zero, br, zc, zr);
+#pragma unroll
+      for (int d = 0; d <= 2 * BW; ++d) lb.set(r, d, lu.Lk[d]);
+    }
+  }
+  // g and phi: nu (solve_g.f90:42-71, solve_v_f.f90:140-153), with phi_h = p0 e_1 through it
+  const RLine Xz{a.xr + m, nm};
+  const RLine X1{a.xinf + m, nm}, X2{a.xinf + ns + m, nm}, X4{a.xinf + 2 * ns + m, nm}, X5{a.xinf + 3 * ns + m, nm};
+  {
+    const double beta = dt * rkc(2, s) * a.nu, dummy = 1.0 + beta * k2;
+    const double p0 = dummy * trow<BW>(tb.t0, 1)[0] - beta * trow<BW>(tb.t2, 1)[0];  // A_g(1,1)
+    const LBand<BW> lb = make_lband<BW>(a.fgp + m, nm, ns, n);
+    LuSweep<BW, 0, 1, true> lu;
+    lu.init(n, make_uband<BW>(a.fgp + a.vf_l + m, nm, ns));
+    for (int r = 1; r <= n; ++r) {
+      const double br[1] = {(r == 1) ? p0 : 0.0};
+      lu.step(r, [&](int rr, double *row, bool c) { helm_row<BW>(tb, rr, n, dummy, beta, row, c); }, zero, br, zc, zr);
+#pragma unroll
+      for (int d = 0; d <= 2 * BW; ++d) lb.set(r, d, lu.Lk[d]);
+      Xz.st(r, zr[0]);
+    }
+  }
+  const UBand<BW> ug = make_uband<BW>(a.fgp + a.vf_l + m, nm, ns);
+  bwd_emit<BW, 0, 1>(n, [&](int r, int e) { return ug.get(r, e); },
+      [&](int r, double2 *, double *z) { z[0] = Xz.ld(r); },
+      [&](int q, int r, const double2 (&)[1][2 * BW + 1], const double (&wr)[1][2 * BW + 1]) {
+        X1.st(q, mvr<BW>(tb.t0, q, r, wr[0]));  // phi_h
+        X2.st(q, mvr<BW>(tb.t2, q, r, wr[0]));  // D2 phi_h
+      });
+  // v_h: (D2 - k^2 D0) v_h = phi_h with v_h = 0 at the walls (solve_v_f.f90:202-272)
+  const LBand<BW> vl = make_lband<BW>(a.vf + m, nm, ns, n);
+  const UBand<BW> vu = make_uband<BW>(a.vf + a.vf_l + m, nm, ns);
+  fwd_lband<BW, 0, 1>([&](int r, int d) { return vl.get(r, d); }, n,
+      [&](int r, double2 *, double *b) { b[0] = (r == 1 || r == n) ? 0.0 : X1.ld(r); },
+      [&](int r, const double2 *, const double *z) { Xz.st(r, z[0]); });
+  double dh1 = 0.0, dhn = 0.0;
+  bwd_emit<BW, 0, 1>(n, [&](int r, int e) { return vu.get(r, e); },
+      [&](int r, double2 *, double *z) { z[0] = Xz.ld(r); },
+      [&](int q, int r, const double2 (&)[1][2 * BW + 1], const double (&wr)[1][2 * BW + 1]) {
+        const double vh = mvr<BW>(tb.t0, q, r, wr[0]), dvh = mvr<BW>(tb.t1, q, r, wr[0]);
+        X4.st(q, vh);
+        X5.st(q, dvh);
+        if (q == 1) dh1 = dvh;
+        if (q == n) dhn = dvh;
+      });
+  a.dvh[m] = z2(dh1, dhn);
 }
 
 // ------------------------------------------------------------------------------------------
@@ -683,7 +814,7 @@ __global__ void __launch_bounds__(512) k_assemble(SplitArgs a) {
   const int n = a.ny, s = a.substep, rr = n + 1 - r;
   const ModeK k = mode_k(a, m);
   // C1, C2 (solve_v_f.f90:293-294); the homogeneous derivative is dvh * (1 + i)
-  const double2 dvh = a.dv[2 * nm + m];
+  const double2 dvh = a.dvh[m];
   const double2 h1 = z2(dvh.x, dvh.x), hn = z2(dvh.y, dvh.y);
   const double2 d1 = a.dv[m], dn = a.dv[nm + m];
   const double2 den = zsub(zmul(h1, h1), zmul(hn, hn));
@@ -696,8 +827,8 @@ __global__ void __launch_bounds__(512) k_assemble(SplitArgs a) {
     cd = 1.0 - alpha * k.k2;
     ca = alpha;
   }
-  const double *xr = a.xr + m;
-  auto X = [&](int i, int row) { return xr[i * ns + (row - 1) * (int)nm]; };
+  const double *xr = a.xinf + m;  // phi_h, D2 phi_h, v_h, dv_h / dy
+  auto X = [&](int i, int row) { return xr[(i - 1) * ns + (row - 1) * (int)nm]; };
   const int64_t o = (r - 1) * (int)nm + m;
   double2 *S = a.S, *Rp = a.RK + ns;
   const double2 v = zadd(zadd(S[ns + o], zscale(X(3, r), C1c)), zscale(X(3, rr), C2c));
@@ -902,6 +1033,13 @@ cudaError_t split_bw(Handle &h, int part, int substep, const double *dt_ptr, cud
   a.ulayout = h.tune.ulayout;
   a.stab = h.tune.stab;
   a.hstab = h.tune.hstab;
+  const bool fc = h.tune.fcache && h.hf;
+  const int64_t fset = vop_factor_doubles(h);
+  a.fth = fc ? h.hf + 2 * (int64_t)(substep - 1) * fset : nullptr;
+  a.fgp = fc ? a.fth + fset : nullptr;
+  a.fcdt = fc ? h.fcdt + (substep - 1) : nullptr;
+  a.xinf = fc ? h.hinf + 4 * (int64_t)(substep - 1) * h.ns : h.xr + h.ns;
+  a.dvh = fc ? h.hdvh + (int64_t)(substep - 1) * h.nmodes : h.dvw + 2 * h.nmodes;
 
   MeanArgs ma;
   ma.ny = h.ny;
@@ -966,14 +1104,28 @@ cudaError_t split_bw(Handle &h, int part, int substep, const double *dt_ptr, cud
       const int HG = a.hgroups;
       const unsigned hb = (unsigned)((h.nmodes + (int64_t)kLanes * HG - 1) / ((int64_t)kLanes * HG));
       const int nt = kLanes * kHelmRoles * HG;
+      if (fc) {
+        k_helm_factor<BW><<<(unsigned)((h.nmodes + 127) / 128), 128, 0, st>>>(a);
+        if ((e = cudaGetLastError()) != cudaSuccess) return e;
+      }
       if (h.tune.stage == 2) {
         const size_t sm = HG * helm_smem<BW, 1, 2>() + htsm;
-        if (h.mixed) k_helmholtz<BW, float2, 1, 2><<<hb, nt, sm, st>>>(a);
-        else k_helmholtz<BW, double2, 1, 2><<<hb, nt, sm, st>>>(a);
+        if (fc) {
+          if (h.mixed) k_helmholtz<BW, float2, 1, 2, true><<<hb, nt, sm, st>>>(a);
+          else k_helmholtz<BW, double2, 1, 2, true><<<hb, nt, sm, st>>>(a);
+        } else {
+          if (h.mixed) k_helmholtz<BW, float2, 1, 2><<<hb, nt, sm, st>>>(a);
+          else k_helmholtz<BW, double2, 1, 2><<<hb, nt, sm, st>>>(a);
+        }
       } else {
         const size_t sm = HG * helm_smem<BW>() + htsm;
-        if (h.mixed) k_helmholtz<BW, float2, 1, 1><<<hb, nt, sm, st>>>(a);
-        else k_helmholtz<BW, double2, 1, 1><<<hb, nt, sm, st>>>(a);
+        if (fc) {
+          if (h.mixed) k_helmholtz<BW, float2, 1, 1, true><<<hb, nt, sm, st>>>(a);
+          else k_helmholtz<BW, double2, 1, 1, true><<<hb, nt, sm, st>>>(a);
+        } else {
+          if (h.mixed) k_helmholtz<BW, float2, 1, 1><<<hb, nt, sm, st>>>(a);
+          else k_helmholtz<BW, double2, 1, 1><<<hb, nt, sm, st>>>(a);
+        }
       }
     }
     return cudaGetLastError();
@@ -1008,6 +1160,8 @@ int64_t vop_lband_doubles(const Handle &h) {
 
 int64_t vop_factor_doubles(const Handle &h) { return vop_lband_doubles(h) + split_ub_role(h); }
 
+bool factor_cache_possible(const Handle &h) { return h.cfg.fixed_dt != 0 && h.nsc == 1; }
+
 namespace {
 
 template <int BW>
@@ -1017,6 +1171,10 @@ cudaError_t set_smem_limit_bw(int bytes) {
   if (e == cudaSuccess) e = lim(k_helmholtz<BW, double2, 1, 1>);
   if (e == cudaSuccess) e = lim(k_helmholtz<BW, float2, 1, 2>);
   if (e == cudaSuccess) e = lim(k_helmholtz<BW, double2, 1, 2>);
+  if (e == cudaSuccess) e = lim(k_helmholtz<BW, float2, 1, 1, true>);
+  if (e == cudaSuccess) e = lim(k_helmholtz<BW, double2, 1, 1, true>);
+  if (e == cudaSuccess) e = lim(k_helmholtz<BW, float2, 1, 2, true>);
+  if (e == cudaSuccess) e = lim(k_helmholtz<BW, double2, 1, 2, true>);
   if (e == cudaSuccess) e = lim(k_helmholtz<BW, float2, 2, 1>);
   if (e == cudaSuccess) e = lim(k_helmholtz<BW, double2, 2, 1>);
   if (e == cudaSuccess) e = lim(k_hvhg<BW, float2, 1>);

@@ -273,8 +273,8 @@ class Channel:
     def set_tuning(self, **shapes):
         """kmm_set_tuning: pin launch shapes (z_lines_per_block, x_rows_per_block, x_threads,
         modes_per_block, u_layout, assemble_threads, tables_shared, helm_modes_per_block,
-        helm_tables_shared, helm_stage_ahead, z_tma, hvhg_stage_ahead); unnamed ones keep their
-        current values."""
+        helm_tables_shared, helm_stage_ahead, z_tma, hvhg_stage_ahead, factor_cache); unnamed ones
+        keep their current values."""
         t = KmmTuning()
         check(self._lib.kmm_get_tuning(self._h, C.byref(t)))
         for k, v in shapes.items():

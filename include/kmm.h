@@ -111,7 +111,10 @@ typedef struct kmm_tuning {
                                  (cp.async.bulk.tensor into shared memory) */
   int32_t hvhg_stage_ahead;   /* rows the hvhg sweeps stage ahead through shared memory (0: they
                                  prefetch into L1 instead; 1, 2) */
-  int32_t reserved;
+  int32_t factor_cache;       /* 1 (fixed time step, one scalar; the default there): the Helmholtz
+                                 sweeps read each substep's operator factors and influence
+                                 solutions, computed once for the current dt (again after dt
+                                 changes) instead of every substep; same numbers.  0 elsewhere */
   double ms_z[3];             /* zinv + zfwd per z variant */
   double ms_x[3];             /* x pass per x variant */
   double ms_modes[2];         /* hvhg at 32 and 64 modes per block (best tables choice) */
