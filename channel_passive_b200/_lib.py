@@ -83,6 +83,7 @@ class KmmTuning(C.Structure):
         ("ms_z", C.c_double * 3), ("ms_x", C.c_double * 3), ("ms_modes", C.c_double * 2),
         ("ms_layout", C.c_double * 2), ("ms_assemble", C.c_double * 3), ("ms_tables", C.c_double * 2),
         ("ms_helm", C.c_double * 12), ("ms_z_tma", C.c_double * 3), ("ms_hvhg", C.c_double * 12),
+        ("ms_step", C.c_double * 2),
     ]
 
     def as_dict(self):

@@ -14,8 +14,11 @@
 //                  shape; then the U factor storage layout,
 //   assembly       threads per block.
 // Each candidate runs once to warm up, then kReps times between CUDA events on the handle's
-// stream; the minimum of the means wins.  The solver runs mutate the state, so the state, the
-// stores and the device scalars are saved first and put back after every run and at the end.
+// stream; the minimum of the means wins.  Last, whole steps through the step graph decide
+// between the shapes picked kernel by kernel and the ones the handle had before: in the step the
+// solver kernels share the GPU with the mean lines on the side stream, which the per-kernel
+// timings do not see.  The solver runs mutate the state, so the state, the stores and the device
+// scalars are saved first and put back after every run and at the end.
 #include <cuda_runtime.h>
 
 #include <cstddef>
@@ -29,6 +32,7 @@ namespace kmm {
 namespace {
 
 constexpr int kReps = 5;
+constexpr int kSteps = 3;  // graph steps per timed run of the final comparison
 
 #define TUNE_CUDA(call)                                                                  \
   do {                                                                                   \
@@ -51,6 +55,7 @@ struct Timer {
 
 int autotune(Handle &h, kmm_tuning *out) {
   cudaStream_t st = h.stream;
+  const Tuning entry = h.tune;  // the shapes the handle had before
   Timer t;
   TUNE_CUDA(cudaEventCreate(&t.a));
   TUNE_CUDA(cudaEventCreate(&t.b));
@@ -239,6 +244,34 @@ int autotune(Handle &h, kmm_tuning *out) {
     if ((rc = measure(prep, body, &rep.ms_assemble[i]))) return rc;
   }
   h.tune.asm_threads = athreads[best(rep.ms_assemble, 3)];
+  // whole steps: the per-kernel choices against the entry shapes; the faster set stays
+  auto drop_graph = [&]() {
+    if (h.gexec) cudaGraphExecDestroy(h.gexec);
+    if (h.graph) cudaGraphDestroy(h.graph);
+    h.gexec = nullptr;
+    h.graph = nullptr;
+  };
+  auto time_steps = [&](const Tuning &shapes, double *ms) -> int {
+    h.tune = shapes;
+    drop_graph();
+    int r = capture_step_graph(h);
+    if (r) return r;
+    // the capture leaves the join event's last record inside the graph: record it outside again
+    TUNE_CUDA(cudaEventRecord(h.ev_join, h.side));
+    auto body = [&]() {
+      cudaError_t e = cudaSuccess;
+      for (int i = 0; i < kSteps && e == cudaSuccess; ++i) e = cudaGraphLaunch(h.gexec, st);
+      return e;
+    };
+    if ((r = measure(restore_joined, body, ms))) return r;
+    *ms /= kSteps;
+    return KMM_OK;
+  };
+  const Tuning picked = h.tune;
+  if ((rc = time_steps(picked, &rep.ms_step[0]))) return rc;
+  if ((rc = time_steps(entry, &rep.ms_step[1]))) return rc;
+  h.tune = rep.ms_step[0] <= rep.ms_step[1] ? picked : entry;
+  drop_graph();
   if ((rc = restore_joined())) return rc;
   TUNE_CUDA(cudaStreamSynchronize(st));
   TUNE_CUDA(cudaStreamSynchronize(h.side));
@@ -252,11 +285,7 @@ int autotune(Handle &h, kmm_tuning *out) {
   std::memcpy(h.tune.ms_helm, rep.ms_helm, sizeof(rep.ms_helm));
   std::memcpy(h.tune.ms_z_tma, rep.ms_z_tma, sizeof(rep.ms_z_tma));
   std::memcpy(h.tune.ms_hvhg, rep.ms_hvhg, sizeof(rep.ms_hvhg));
-  // the step graph holds the old launch shapes: capture it again at the next step
-  if (h.gexec) cudaGraphExecDestroy(h.gexec);
-  if (h.graph) cudaGraphDestroy(h.graph);
-  h.gexec = nullptr;
-  h.graph = nullptr;
+  std::memcpy(h.tune.ms_step, rep.ms_step, sizeof(rep.ms_step));
   if (out) kmm_get_tuning(reinterpret_cast<const kmm_handle *>(&h), out);
   return KMM_OK;
 }
@@ -292,6 +321,7 @@ int kmm_get_tuning(const kmm_handle *hh, kmm_tuning *out) {
   std::memcpy(out->ms_helm, h.tune.ms_helm, sizeof(out->ms_helm));
   std::memcpy(out->ms_z_tma, h.tune.ms_z_tma, sizeof(out->ms_z_tma));
   std::memcpy(out->ms_hvhg, h.tune.ms_hvhg, sizeof(out->ms_hvhg));
+  std::memcpy(out->ms_step, h.tune.ms_step, sizeof(out->ms_step));
   return KMM_OK;
 }
 

@@ -127,6 +127,9 @@ typedef struct kmm_tuning {
                                  the grid does not allow them) */
   double ms_hvhg[12];         /* hvhg at [32, 64 modes][tables via L1, shared][staging 0, 1, 2
                                  rows] (row-major; 0 where a shape was not timed) */
+  double ms_step[2];          /* one step through the step graph with the shapes picked kernel
+                                 by kernel, and with the shapes the handle had before tuning;
+                                 the faster set is kept */
 } kmm_tuning;
 
 typedef struct kmm_handle kmm_handle;

@@ -73,6 +73,7 @@ def test_autotune_keeps_the_state_and_reports_its_choice():
     # every Helmholtz shape that fits this grid was timed, and the chosen one is the fastest
     helm = [x for x in rep["ms_helm"] if x > 0]
     assert len(helm) >= 8 and min(helm) == rep["ms_layout"][0]
+    assert rep["ms_step"][0] > 0 and rep["ms_step"][1] > 0
     assert t["helm_modes_per_block"] in (32, 64, 128)
     with pytest.raises(KmmError) as e:
         with Channel(cfg) as ch:
@@ -86,4 +87,47 @@ def test_create_with_autotune_flag():
         t = ch.tuning
     # the timings of the tuning run at creation stay with the handle
     assert t["tuned"] == 1 and all(x > 0 for x in t["ms_z"] + t["ms_x"] + t["ms_modes"] + t["ms_assemble"])
-    assert t["ms_layout"][t["u_layout"]] == min(t["ms_layout"])
+    # whole graph steps decide between the per-kernel picks and the shapes the handle had before
+    assert t["ms_step"][0] > 0 and t["ms_step"][1] > 0
+    if t["ms_step"][0] <= t["ms_step"][1]:
+        assert t["ms_layout"][t["u_layout"]] == min(t["ms_layout"])
+    else:  # the shapes of an untuned handle
+        cfg0, _ = make_pair(nx=64, ny=65, nz=64, precision=1)
+        with Channel(cfg0) as ch0:
+            t0 = ch0.tuning
+        assert all(t[k] == t0[k] for k in t0 if not k.startswith("ms_") and k != "tuned")
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+def test_factor_cache_gives_the_same_numbers_across_dt_changes(precision):
+    """factor_cache (fixed time step, the default there): the Helmholtz sweeps that read each
+    substep's cached operator factors and influence solutions give the per-substep factorisation's
+    results bit for bit, also when dt changes between steps (the cache is rebuilt for the new dt)
+    and changes back."""
+    cfg, p = make_pair(nx=32, ny=33, nz=32, control_amp=-1.0, precision=precision)
+    U = seeded_state(cfg, okmm.make_operators(p).y)
+    out = {}
+    for fc in (0, 1):
+        with Channel(cfg) as ch:
+            assert ch.tuning["factor_cache"] == 1
+            ch.set_tuning(factor_cache=fc)
+            assert ch.tuning["factor_cache"] == fc
+            ch.set_initial_data_uvw(U, 0.01)
+            ch.step(2)
+            ch.dt = 0.005
+            ch.step(2)
+            ch.dt = 0.01
+            ch.step(1)
+            out[fc] = ch.download_state(10)
+    for f in STATE_SLOTS:
+        assert np.array_equal(out[0][0][f], out[1][0][f]), f
+    assert np.array_equal(out[0][1], out[1][1])  # the RK stores
+
+
+def test_factor_cache_needs_a_fixed_time_step():
+    cfg, _ = make_pair(nx=16, ny=33, nz=16, fixed_dt=0)
+    with Channel(cfg) as ch:
+        assert ch.tuning["factor_cache"] == 0
+        with pytest.raises(KmmError) as e:
+            ch.set_tuning(factor_cache=1)
+        assert e.value.code == _lib.KMM_ERR_ARG
