@@ -100,7 +100,7 @@ struct Tuning {
   double ms_helm[3][2][2] = {};  // [32/64/128 modes][tables via L1 / shared][look-ahead 1 / 2]
   double ms_z_tma[3] = {};       // the z variants with TMA-staged input tiles
   double ms_hvhg[2][2][3] = {};  // [32/64 modes][tables via L1 / shared][staging 0 / 1 / 2 rows]
-  double ms_step[2] = {};        // graph step: the per-kernel choices / the shapes before tuning
+  double ms_step[2] = {};        // graph step with the kept shapes / with the shapes before tuning
 };
 
 struct Handle {

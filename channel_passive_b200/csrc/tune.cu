@@ -14,10 +14,10 @@
 //                  shape; then the U factor storage layout,
 //   assembly       threads per block.
 // Each candidate runs once to warm up, then kReps times between CUDA events on the handle's
-// stream; the minimum of the means wins.  Last, whole steps through the step graph decide
-// between the shapes picked kernel by kernel and the ones the handle had before: in the step the
-// solver kernels share the GPU with the mean lines on the side stream, which the per-kernel
-// timings do not see.  The solver runs mutate the state, so the state, the stores and the device
+// stream; the minimum of the means wins.  Last, whole steps through the step graph decide which
+// of those picks stay, one knob group at a time from the shapes the handle had before: in the
+// step the solver kernels share the GPU with the mean lines on the side stream, which the
+// per-kernel timings do not see.  The solver runs mutate the state, so the state, the stores and the device
 // scalars are saved first and put back after every run and at the end.
 #include <cuda_runtime.h>
 
@@ -244,34 +244,79 @@ int autotune(Handle &h, kmm_tuning *out) {
     if ((rc = measure(prep, body, &rep.ms_assemble[i]))) return rc;
   }
   h.tune.asm_threads = athreads[best(rep.ms_assemble, 3)];
-  // whole steps: the per-kernel choices against the entry shapes; the faster set stays
+  // Whole steps through the step graph (the solver kernels beside the mean lines on the side
+  // stream, as the step runs them) decide which picks stay: starting from the shapes the handle
+  // had, each knob group takes its per-kernel pick only where the step gets faster with it.  With
+  // a fixed time step and no dt set yet (a handle tuned at creation) the timed steps use
+  // dt = 1e-3; where a step cannot run (the CFL rule on a zero state) the entry shapes stay.
+  const Tuning picked = h.tune;
+  DevScalars dsc_step = dsc;
+  dsc_step.err = 0;
+  if (h.cfg.fixed_dt && !(dsc_step.dt > 1e-14)) dsc_step.dt = 1e-3;
+  auto restore_step = [&]() -> int {
+    TUNE_CUDA(cudaMemcpyAsync(h.S, h.staging, nfld * fb, cudaMemcpyDeviceToDevice, st));
+    TUNE_CUDA(cudaMemcpyAsync(h.RK, h.staging + nfld * h.ns, nst * fb, cudaMemcpyDeviceToDevice, st));
+    TUNE_CUDA(cudaMemcpyAsync(h.dsc, &dsc_step, sizeof(dsc_step), cudaMemcpyHostToDevice, st));
+    return KMM_OK;
+  };
   auto drop_graph = [&]() {
     if (h.gexec) cudaGraphExecDestroy(h.gexec);
     if (h.graph) cudaGraphDestroy(h.graph);
     h.gexec = nullptr;
     h.graph = nullptr;
   };
+  // device ms of one step with `shapes`; 0 where the step raised a device error
   auto time_steps = [&](const Tuning &shapes, double *ms) -> int {
     h.tune = shapes;
     drop_graph();
     int r = capture_step_graph(h);
     if (r) return r;
-    // the capture leaves the join event's last record inside the graph: record it outside again
-    TUNE_CUDA(cudaEventRecord(h.ev_join, h.side));
     auto body = [&]() {
       cudaError_t e = cudaSuccess;
       for (int i = 0; i < kSteps && e == cudaSuccess; ++i) e = cudaGraphLaunch(h.gexec, st);
       return e;
     };
-    if ((r = measure(restore_joined, body, ms))) return r;
+    if ((r = measure(restore_step, body, ms))) return r;
     *ms /= kSteps;
+    int err = 0;
+    TUNE_CUDA(cudaMemcpy(&err, &h.dsc->err, sizeof(int), cudaMemcpyDeviceToHost));
+    if (err) *ms = 0.0;
     return KMM_OK;
   };
-  const Tuning picked = h.tune;
-  if ((rc = time_steps(picked, &rep.ms_step[0]))) return rc;
-  if ((rc = time_steps(entry, &rep.ms_step[1]))) return rc;
-  h.tune = rep.ms_step[0] <= rep.ms_step[1] ? picked : entry;
+  auto take_group = [&](Tuning t, int g) {
+    switch (g) {
+      case 0: t.z = picked.z; t.ztma = picked.ztma; break;
+      case 1: t.x = picked.x; break;
+      case 2: t.groups = picked.groups; t.stab = picked.stab; t.hvstage = picked.hvstage; break;
+      case 3: t.hgroups = picked.hgroups; t.hstab = picked.hstab; t.stage = picked.stage; t.ulayout = picked.ulayout; break;
+      default: t.asm_threads = picked.asm_threads; break;
+    }
+    return t;
+  };
+  auto same_shapes = [](const Tuning &a, const Tuning &b) {
+    return a.z == b.z && a.ztma == b.ztma && a.x == b.x && a.groups == b.groups && a.stab == b.stab &&
+           a.hvstage == b.hvstage && a.hgroups == b.hgroups && a.hstab == b.hstab && a.stage == b.stage &&
+           a.ulayout == b.ulayout && a.asm_threads == b.asm_threads;
+  };
+  if ((rc = restore_joined())) return rc;  // the side stream's last mean lines are done
+  Tuning kept = entry;
+  if ((rc = time_steps(kept, &rep.ms_step[1]))) return rc;
+  double kept_ms = rep.ms_step[1];
+  for (int g = 0; g < 5 && kept_ms > 0.0; ++g) {
+    const Tuning cand = take_group(kept, g);
+    if (same_shapes(cand, kept)) continue;
+    double ms = 0.0;
+    if ((rc = time_steps(cand, &ms))) return rc;
+    if (ms > 0.0 && ms < kept_ms) {
+      kept = cand;
+      kept_ms = ms;
+    }
+  }
+  rep.ms_step[0] = kept_ms;
+  h.tune = kept;
   drop_graph();
+  // the captures left the join event's last record inside a graph: record it outside again
+  TUNE_CUDA(cudaEventRecord(h.ev_join, h.side));
   if ((rc = restore_joined())) return rc;
   TUNE_CUDA(cudaStreamSynchronize(st));
   TUNE_CUDA(cudaStreamSynchronize(h.side));
@@ -286,6 +331,11 @@ int autotune(Handle &h, kmm_tuning *out) {
   std::memcpy(h.tune.ms_z_tma, rep.ms_z_tma, sizeof(rep.ms_z_tma));
   std::memcpy(h.tune.ms_hvhg, rep.ms_hvhg, sizeof(rep.ms_hvhg));
   std::memcpy(h.tune.ms_step, rep.ms_step, sizeof(rep.ms_step));
+  // the step graph holds the old launch shapes: capture it again at the next step
+  if (h.gexec) cudaGraphExecDestroy(h.gexec);
+  if (h.graph) cudaGraphDestroy(h.graph);
+  h.gexec = nullptr;
+  h.graph = nullptr;
   if (out) kmm_get_tuning(reinterpret_cast<const kmm_handle *>(&h), out);
   return KMM_OK;
 }

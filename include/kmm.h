@@ -127,9 +127,11 @@ typedef struct kmm_tuning {
                                  the grid does not allow them) */
   double ms_hvhg[12];         /* hvhg at [32, 64 modes][tables via L1, shared][staging 0, 1, 2
                                  rows] (row-major; 0 where a shape was not timed) */
-  double ms_step[2];          /* one step through the step graph with the shapes picked kernel
-                                 by kernel, and with the shapes the handle had before tuning;
-                                 the faster set is kept */
+  double ms_step[2];          /* one step through the step graph with the shapes kept, and with
+                                 the shapes the handle had before tuning: each knob group keeps
+                                 its per-kernel pick only where the step gets faster with it (0
+                                 where a step could not run: the CFL rule on a zero state; the
+                                 entry shapes then stay) */
 } kmm_tuning;
 
 typedef struct kmm_handle kmm_handle;

@@ -87,15 +87,10 @@ def test_create_with_autotune_flag():
         t = ch.tuning
     # the timings of the tuning run at creation stay with the handle
     assert t["tuned"] == 1 and all(x > 0 for x in t["ms_z"] + t["ms_x"] + t["ms_modes"] + t["ms_assemble"])
-    # whole graph steps decide between the per-kernel picks and the shapes the handle had before
-    assert t["ms_step"][0] > 0 and t["ms_step"][1] > 0
-    if t["ms_step"][0] <= t["ms_step"][1]:
-        assert t["ms_layout"][t["u_layout"]] == min(t["ms_layout"])
-    else:  # the shapes of an untuned handle
-        cfg0, _ = make_pair(nx=64, ny=65, nz=64, precision=1)
-        with Channel(cfg0) as ch0:
-            t0 = ch0.tuning
-        assert all(t[k] == t0[k] for k in t0 if not k.startswith("ms_") and k != "tuned")
+    # whole substeps decide, knob group by knob group, which per-kernel picks stay: the kept set is
+    # never slower than the shapes the handle had, and each group is either its pick or those
+    assert 0 < t["ms_step"][0] <= t["ms_step"][1]
+    assert t["u_layout"] in (0, int(np.argmin(t["ms_layout"])))
 
 
 @pytest.mark.parametrize("precision", [0, 1])
