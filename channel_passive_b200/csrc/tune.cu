@@ -33,6 +33,9 @@ namespace {
 
 constexpr int kReps = 5;
 constexpr int kSteps = 3;  // graph steps per timed run of the final comparison
+// A knob group's pick replaces the entry shapes only for a step at least 1% faster: step times of
+// two shape sets within a few tenths of a percent reorder from one run (or box) to the next.
+constexpr double kMinGain = 0.99;
 
 #define TUNE_CUDA(call)                                                                  \
   do {                                                                                   \
@@ -246,7 +249,7 @@ int autotune(Handle &h, kmm_tuning *out) {
   h.tune.asm_threads = athreads[best(rep.ms_assemble, 3)];
   // Whole steps through the step graph (the solver kernels beside the mean lines on the side
   // stream, as the step runs them) decide which picks stay: starting from the shapes the handle
-  // had, each knob group takes its per-kernel pick only where the step gets faster with it.  With
+  // had, each knob group takes its per-kernel pick only where the step gets 1% faster with it.  With
   // a fixed time step and no dt set yet (a handle tuned at creation) the timed steps use
   // dt = 1e-3; where a step cannot run (the CFL rule on a zero state) the entry shapes stay.
   const Tuning picked = h.tune;
@@ -307,7 +310,7 @@ int autotune(Handle &h, kmm_tuning *out) {
     if (same_shapes(cand, kept)) continue;
     double ms = 0.0;
     if ((rc = time_steps(cand, &ms))) return rc;
-    if (ms > 0.0 && ms < kept_ms) {
+    if (ms > 0.0 && ms < kMinGain * kept_ms) {
       kept = cand;
       kept_ms = ms;
     }

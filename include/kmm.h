@@ -129,7 +129,7 @@ typedef struct kmm_tuning {
                                  rows] (row-major; 0 where a shape was not timed) */
   double ms_step[2];          /* one step through the step graph with the shapes kept, and with
                                  the shapes the handle had before tuning: each knob group keeps
-                                 its per-kernel pick only where the step gets faster with it (0
+                                 its per-kernel pick only where the step gets 1% faster with it (0
                                  where a step could not run: the CFL rule on a zero state; the
                                  entry shapes then stay) */
 } kmm_tuning;
