@@ -46,7 +46,12 @@ struct Adjoint {
   double2 *lmid = nullptr;    // [8 nm]
   double2 *tmp = nullptr;     // [4 ns]
   double2 *X = nullptr;       // per-mode scratch lines [kAdjLines ns]
-  double *B = nullptr;        // per-mode bands [3][(2bw+1) ns]
+  // per substep, for the dt in cdt: the factored bands of theta's, g's (= phi's) and v's operators
+  // [3][3][(2bw+1) ns] and the state-independent influence lines of solve_v_f [3][6 ns]
+  double *B = nullptr;
+  double2 *Xc = nullptr;
+  double cdt[3] = {0.0, 0.0, 0.0};
+  bool cvalid[3] = {false, false, false};
   double2 *ml = nullptr;      // mean-line scratch [3][8][ny] complex
   double *mb = nullptr;       // mean-line bands [3][(2bw+1) ny]
   double2 *lvw = nullptr;     // [2][nmodes] lambda of the wall values
@@ -158,24 +163,23 @@ struct AdjArgs {
   const double2 *lS, *lRK;   // lambda of the substep's outputs (u, v, w, theta; the three stores)
   double2 *lP, *lRK0, *lvw;  // out: lambda of the products, of the starting stores, of the wall values
   double2 *X;
-  double *B;
+  double *B;                 // this substep's factored bands (k_adj_factor)
+  double2 *Xc;               // this substep's influence lines c2, D0 c2, D2 c2, ch, D1 ch, D0 ch
   double2 *ml;
   double *mb;
   double w_tau, w_q;         // objective weights of this substep (zero unless substep 3)
 };
 
 // The transpose of solve_g.f90:28-201 (VT = nu) or solve_t.f90:28-201 (VT = nu / pr) for one
-// mode: lf, lst = lambda of the new field and store; lh (out), lstore (out); A = scratch band
-// (receives the factored operator); t0, t1 scratch lines.
+// mode: lf, lst = lambda of the new field and store; lh (out), lstore (out); A = the operator's
+// factored band (k_adj_factor); t0, t1 scratch lines.
 template <int BW>
 __device__ void helm_t(const AdjArgs &a, double visc, double k2, DLine lf, DLine lst, DLine lh, DLine lstore,
                        BandM<BW> A, DLine t0, DLine t1) {
   const int n = a.ny, s = a.substep;
   const double dt = a.dt;
   const BandS<BW> D0{a.d0}, D2{a.d2}, D0lu{a.d0lu};
-  const double beta = dt * rka(2, s) * visc, alpha = dt * rka(1, s) * visc, gamma = dt * rka(3, s);
-  fill_rows<BW>(A, D0, D2, 1.0 + beta * k2, -beta, 1.0 + beta * k2, -beta, n);
-  labs_lu<BW>(A, n);
+  const double alpha = dt * rka(1, s) * visc, gamma = dt * rka(3, s);
   if (s != 3) {
     const double a1 = dt * rka(1, s + 1) * visc, z1 = dt * rka(4, s + 1);
     for (int y = 1; y <= n; ++y) {
@@ -201,6 +205,48 @@ __device__ void helm_t(const AdjArgs &a, double visc, double k2, DLine lf, DLine
     for (int y = 1; y <= n; ++y) lstore.st(y, t1.ld(y));
   }
   for (int y = 1; y <= n; ++y) lh.st(y, zadd(lh.ld(y), zscale(gamma, t1.ld(y))));
+}
+
+// The factored bands and state-independent lines of one substep, per mode (modes other than
+// (0,0)): they depend on dt and k^2 alone, and the adjoint runs at a fixed time step, so the
+// backward sweep makes them once per substep (Adjoint::cdt) instead of at every step.  Same
+// routines as before in the same order, so the same numbers.
+template <int BW>
+__global__ void __launch_bounds__(64) k_adj_factor(AdjArgs a) {
+  const int64_t m = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (m == 0 || m >= a.nmodes) return;
+  const int n = a.ny, s = a.substep;
+  const int64_t nm = a.nmodes, ns = a.ns;
+  const double dt = a.dt;
+  const int kzi = (int)(m / a.nxh), kxi = (int)(m - (int64_t)kzi * a.nxh);
+  const int kzint = (kzi <= a.nz / 2) ? kzi : kzi - a.nz;
+  const double kx = kxi * a.lmfxr, kz = kzint * a.lmfzr, k2 = kx * kx + kz * kz;
+  const BandS<BW> D0{a.d0}, D1{a.d1}, D2{a.d2};
+  const int64_t bsz = (int64_t)(2 * BW + 1) * n * nm;
+  const BandM<BW> At{a.B + m, nm}, Ag{a.B + bsz + m, nm}, Vb{a.B + 2 * bsz + m, nm};
+  {  // theta's operator (solve_t.f90:42-71)
+    const double visc = a.nu / a.pr, beta = dt * rka(2, s) * visc;
+    fill_rows<BW>(At, D0, D2, 1.0 + beta * k2, -beta, 1.0 + beta * k2, -beta, n);
+    labs_lu<BW>(At, n);
+  }
+  const double beta = dt * rka(2, s) * a.nu;
+  fill_rows<BW>(Ag, D0, D2, 1.0 + beta * k2, -beta, 1.0 + beta * k2, -beta, n);
+  labs_lu<BW>(Ag, n);
+  fill_rows<BW>(Vb, D2, D0, 1.0, -k2, 0.0, 1.0, n);  // D2 - k^2 D0, D0 at the walls
+  labs_lu<BW>(Vb, n);
+  // c2 = Ag^-1 (p0 + i p0) e_1, buf3 = D0 c2, d2h = D2 c2, ch = V^-1 buf3 (walls zero),
+  // hh = D1 ch, hm = D0 ch
+  auto C = [&](int i) { return DLine{a.Xc + i * ns + m, nm}; };
+  const DLine c2 = C(0), buf3 = C(1), d2h = C(2), ch = C(3), hh = C(4), hm = C(5);
+  const double p0 = Ag.g(BW + 1, 1);
+  for (int y = 1; y <= n; ++y) c2.st(y, y == 1 ? make_double2(p0, p0) : make_double2(0.0, 0.0));
+  labs_bs<BW>(Ag, c2, n);
+  labs_mat_mul<BW>(D0, c2, buf3, n);
+  labs_mat_mul<BW>(D2, c2, d2h, n);
+  for (int y = 1; y <= n; ++y) ch.st(y, (y == 1 || y == n) ? make_double2(0.0, 0.0) : buf3.ld(y));
+  labs_bs<BW>(Vb, ch, n);
+  labs_mat_mul<BW>(D1, ch, hh, n);
+  labs_mat_mul<BW>(D0, ch, hm, n);
 }
 
 // Per-mode transpose of wavespace (modes other than (0,0)).
@@ -233,26 +279,12 @@ __global__ void __launch_bounds__(64) k_adj_modes(AdjArgs a) {
   // solve_t^T: lambda h_theta -> X2, lambda of the theta store -> ot
   helm_t<BW>(a, a.nu / a.pr, k2, lth, lst, X(2), ot, At, X(3), X(4));
 
-  // solve_v_f^T
+  // solve_v_f^T (Ag, Vb and the state-independent lines from k_adj_factor)
   {
     const double nu = a.nu;
-    const double beta = dt * rka(2, s) * nu, alpha = dt * rka(1, s) * nu, gamma = dt * rka(3, s);
-    fill_rows<BW>(Ag, D0, D2, 1.0 + beta * k2, -beta, 1.0 + beta * k2, -beta, n);
-    labs_lu<BW>(Ag, n);
-    fill_rows<BW>(Vb, D2, D0, 1.0, -k2, 0.0, 1.0, n);  // D2 - k^2 D0, D0 at the walls
-    labs_lu<BW>(Vb, n);
-    // state-independent lines: c2 = Ag^-1 (p0 + i p0) e_1, buf3 = D0 c2, d2h = D2 c2,
-    // ch = V^-1 buf3 (walls zero), hh = D1 ch, hm = D0 ch
-    const DLine c2 = X(5), buf3 = X(6), d2h = X(7), ch = X(8), hh = X(9), hm = X(10);
-    const double p0 = Ag.g(BW + 1, 1);
-    for (int y = 1; y <= n; ++y) c2.st(y, y == 1 ? make_double2(p0, p0) : make_double2(0.0, 0.0));
-    labs_bs<BW>(Ag, c2, n);
-    labs_mat_mul<BW>(D0, c2, buf3, n);
-    labs_mat_mul<BW>(D2, c2, d2h, n);
-    for (int y = 1; y <= n; ++y) ch.st(y, (y == 1 || y == n) ? make_double2(0.0, 0.0) : buf3.ld(y));
-    labs_bs<BW>(Vb, ch, n);
-    labs_mat_mul<BW>(D1, ch, hh, n);
-    labs_mat_mul<BW>(D0, ch, hm, n);
+    const double alpha = dt * rka(1, s) * nu, gamma = dt * rka(3, s);
+    auto C = [&](int i) { return DLine{a.Xc + i * ns + m, nm}; };
+    const DLine buf3 = C(1), d2h = C(2), hh = C(4), hm = C(5);
     const double2 h1 = hh.ld(1), hn = hh.ld(n);
     const double2 den = zsub(zmul(h1, h1), zmul(hn, hn));
     const double q = s != 3 ? 1.0 - dt * rka(1, s + 1) * nu * k2 : 1.0;
@@ -522,7 +554,8 @@ int adjoint_buffers(Handle &h) {
   if ((rc = adj_alloc(h, &A.lmid, 8 * nm))) return rc;
   if ((rc = adj_alloc(h, &A.tmp, 4 * ns))) return rc;
   if ((rc = adj_alloc(h, &A.X, (size_t)kAdjLines * ns))) return rc;
-  if ((rc = adj_alloc(h, &A.B, 3 * band))) return rc;
+  if ((rc = adj_alloc(h, &A.B, 9 * band))) return rc;
+  if ((rc = adj_alloc(h, &A.Xc, 18 * ns))) return rc;
   if ((rc = adj_alloc(h, &A.ml, 3 * 8 * ny))) return rc;
   if ((rc = adj_alloc(h, &A.mb, 3 * (size_t)(2 * h.bw + 1) * ny))) return rc;
   if ((rc = adj_alloc(h, &A.lvw, 2 * (size_t)h.nmodes))) return rc;
@@ -559,15 +592,29 @@ cudaError_t adj_substep_bw(Handle &h, int s, const double2 *sbase, double dt, do
   a.lRK0 = A.lRK0;
   a.lvw = A.lvw;
   a.X = A.X;
-  a.B = A.B;
+  a.B = A.B + (int64_t)(s - 1) * 3 * (2 * h.bw + 1) * h.ns;
+  a.Xc = A.Xc + (int64_t)(s - 1) * 6 * h.ns;
   a.ml = A.ml;
   a.mb = A.mb;
   a.w_tau = w_tau;
   a.w_q = w_q;
+  cudaError_t e;
+  if (!A.cvalid[s - 1] || A.cdt[s - 1] != dt) {
+    k_adj_factor<BW><<<(unsigned)((h.nmodes + 63) / 64), 64, 0, st>>>(a);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    A.cdt[s - 1] = dt;
+    A.cvalid[s - 1] = true;
+  }
+  // the (0,0) lines on the side stream beside the other modes (disjoint entries of every line)
+  if ((e = cudaEventRecord(h.ev_fork, st)) != cudaSuccess) return e;
+  if ((e = cudaStreamWaitEvent(h.side, h.ev_fork, 0)) != cudaSuccess) return e;
+  k_adj_mean<BW><<<1, 32, 0, h.side>>>(a);
+  if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  if ((e = cudaEventRecord(h.ev_join, h.side)) != cudaSuccess) return e;
   // one thread per mode; 64-thread blocks spread the few thousand modes over more SMs
   k_adj_modes<BW><<<(unsigned)((h.nmodes + 63) / 64), 64, 0, st>>>(a);
+  if ((e = cudaStreamWaitEvent(st, h.ev_join, 0)) != cudaSuccess) return e;
   const unsigned blocks = (unsigned)((h.nmodes + 127) / 128);
-  k_adj_mean<BW><<<1, 32, 0, st>>>(a);
   ProbeArgs pa{};
   pa.ny = h.ny;
   pa.nxh = h.nxh;
@@ -583,8 +630,7 @@ cudaError_t adj_substep_bw(Handle &h, int s, const double2 *sbase, double dt, do
   pa.lS0 = A.lS0;
   pa.G = A.G;
   k_adj_probe<<<blocks, 128, 0, st>>>(pa);
-  cudaError_t e = cudaGetLastError();
-  if (e != cudaSuccess) return e;
+  if ((e = cudaGetLastError()) != cudaSuccess) return e;
   // x_to_y^T, products^T at the starting state, y_to_x^T
   if ((e = launch_zinv(h, sbase, h.MID, 4, st)) != cudaSuccess) return e;
   if ((e = launch_zinv(h, A.lP, A.lmid, 8, st)) != cudaSuccess) return e;
@@ -630,7 +676,7 @@ void adjoint_free(Handle &h) {
   if (!h.adj) return;
   Adjoint &A = *h.adj;
   for (double2 *p : A.ck) cudaFree(p);
-  void *ptrs[] = {A.fin, A.sb, A.lS, A.lRK, A.lS0, A.lRK0, A.lP, A.lmid, A.tmp, A.X, A.B, A.ml, A.mb, A.lvw, A.G, A.J};
+  void *ptrs[] = {A.fin, A.sb, A.lS, A.lRK, A.lS0, A.lRK0, A.lP, A.lmid, A.tmp, A.X, A.B, A.Xc, A.ml, A.mb, A.lvw, A.G, A.J};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   delete h.adj;
