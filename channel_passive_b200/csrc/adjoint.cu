@@ -12,7 +12,7 @@
 // applies the transposes of the three substeps in reverse order.
 //
 // The transpose of one substep, with <a, b> = Re sum conj(a) b over the stored coefficients:
-//   wavespace^T   per (kx, kz) mode, one thread each (k_adj_modes): the routines of
+//   wavespace^T   per (kx, kz) mode, three role warps per 32 modes (k_adj_modes): the routines of
 //                 wavespace.f90 in reverse (solve_u_w, solve_t, solve_v_f, solve_g, hvhg), every
 //                 band solve A^{-1} becoming A^{-T} and every band product M becoming M^T, both on
 //                 the packed LU of fixed_bandec (module_labs.f90:3487-3636);
@@ -61,7 +61,7 @@ struct Adjoint {
 
 namespace {
 
-constexpr int kAdjLines = 16;
+constexpr int kAdjLines = 18;
 
 #define ADJ_CUDA(call)                                                                    \
   do {                                                                                    \
@@ -249,11 +249,18 @@ __global__ void __launch_bounds__(64) k_adj_factor(AdjArgs a) {
   labs_mat_mul<BW>(D0, ch, hm, n);
 }
 
-// Per-mode transpose of wavespace (modes other than (0,0)).
+// Per-mode transpose of wavespace (modes other than (0,0)), three warps per 32 modes.  Once the
+// bands are factored (k_adj_factor), solve_t^T (role 0), solve_v_f^T (role 1) and solve_g^T
+// (role 2) are independent; after a block barrier hvhg^T's four D0 solves are spread over the
+// roles, and after a second one each role forms some of the products' lambda.  Each role runs
+// the per-mode arithmetic of the single-thread order, so the results are the same numbers.
+constexpr int kAdjRoles = 3;
+
 template <int BW>
-__global__ void __launch_bounds__(64) k_adj_modes(AdjArgs a) {
-  const int64_t m = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (m == 0 || m >= a.nmodes) return;
+__global__ void __launch_bounds__(32 * kAdjRoles) k_adj_modes(AdjArgs a) {
+  const int role = threadIdx.x / 32;
+  const int64_t m = (int64_t)blockIdx.x * 32 + (threadIdx.x % 32);
+  const bool live = m != 0 && m < a.nmodes;  // every thread reaches the barriers
   const int n = a.ny, s = a.substep;
   const int64_t nm = a.nmodes, ns = a.ns;
   const double dt = a.dt;
@@ -269,101 +276,116 @@ __global__ void __launch_bounds__(64) k_adj_modes(AdjArgs a) {
   const DLine lsg = in(a.lRK, 0), lsp = in(a.lRK, 1), lst = in(a.lRK, 2);
   const DLine og = in(a.lRK0, 0), op = in(a.lRK0, 1), ot = in(a.lRK0, 2);
 
-  // solve_u_w^T: lambda g -> X0, lambda dv -> X1
-  const double kxx = kx / k2, kzz = kz / k2;
-  for (int y = 1; y <= n; ++y) {
-    const double2 u = lu.ld(y), w = lw.ld(y);
-    X(0).st(y, zsub(zi(kzz, u), zi(kxx, w)));
-    X(1).st(y, zsub(zi(-kxx, u), zi(kzz, w)));
-  }
-  // solve_t^T: lambda h_theta -> X2, lambda of the theta store -> ot
-  helm_t<BW>(a, a.nu / a.pr, k2, lth, lst, X(2), ot, At, X(3), X(4));
-
-  // solve_v_f^T (Ag, Vb and the state-independent lines from k_adj_factor)
-  {
-    const double nu = a.nu;
-    const double alpha = dt * rka(1, s) * nu, gamma = dt * rka(3, s);
-    auto C = [&](int i) { return DLine{a.Xc + i * ns + m, nm}; };
-    const DLine buf3 = C(1), d2h = C(2), hh = C(4), hm = C(5);
-    const double2 h1 = hh.ld(1), hn = hh.ld(n);
-    const double2 den = zsub(zmul(h1, h1), zmul(hn, hn));
-    const double q = s != 3 ? 1.0 - dt * rka(1, s + 1) * nu * k2 : 1.0;
-    const double a1 = s != 3 ? dt * rka(1, s + 1) * nu : 0.0;
-    const DLine ldv = X(1);
-    double2 lC1 = make_double2(0.0, 0.0), lC2 = make_double2(0.0, 0.0);
-    for (int y = 1; y <= n; ++y) {
-      const int r = n + 1 - y;
-      const double2 vy = lv.ld(y), py = lsp.ld(y), dy = ldv.ld(y);
-      lC1 = zadd(lC1, zcm(hm.ld(y), vy));
-      lC2 = zadd(lC2, zcm(hm.ld(r), vy));
-      lC1 = zadd(lC1, zcm(zadd(zscale(q, buf3.ld(y)), zscale(a1, d2h.ld(y))), py));
-      lC2 = zadd(lC2, zcm(zadd(zscale(q, buf3.ld(r)), zscale(a1, d2h.ld(r))), py));
-      lC1 = zadd(lC1, zcm(hh.ld(y), dy));
-      lC2 = zsub(lC2, zcm(hh.ld(r), dy));
-    }
-    // dv0 (the particular solution's dv/dy): its wall values set C1 and C2
-    const DLine ldv0 = X(11);
-    for (int y = 1; y <= n; ++y) ldv0.st(y, ldv.ld(y));
-    const double2 hnd = zdiv(hn, den), h1d = zdiv(h1, den);
-    ldv0.st(n, zadd(ldv0.ld(n), zadd(zcm(hnd, lC1), zcm(h1d, lC2))));
-    ldv0.st(1, zsub(ldv0.ld(1), zadd(zcm(h1d, lC1), zcm(hnd, lC2))));
-    // v0 = D0 cv, dv0 = D1 cv, cv = V^-1 r
-    const DLine lr = X(12);
-    mm_t<BW>(D0, lv, lr, n);
-    mm_t<BW>(D1, ldv0, lr, n, 1.0, true);
-    bs_t<BW>(Vb, lr, n);
-    a.lvw[m] = lr.ld(1);
-    a.lvw[nm + m] = lr.ld(n);
-    // part 4: lambda of hv2 (= D0 c1) and of dv_a (= D2 c1)
-    const DLine lhv2 = X(13), lc1 = X(14);
-    for (int y = 1; y <= n; ++y) {
-      const double2 w0 = (y == 1 || y == n) ? make_double2(0.0, 0.0) : lr.ld(y);
-      lhv2.st(y, zadd(w0, zscale(q, lsp.ld(y))));
-    }
-    mm_t<BW>(D0, lhv2, lc1, n);
-    if (s != 3) mm_t<BW>(D2, lsp, lc1, n, a1, true);
-    bs_t<BW>(Ag, lc1, n);
-    zero_walls(lc1, n);  // lambda of the right-hand side of phi
-    // parts 2 and 1
-    const DLine lhv = X(15);
-    const double z1 = s != 3 ? dt * rka(4, s + 1) : 0.0;
-    for (int y = 1; y <= n; ++y) lhv.st(y, zadd(zscale(z1, lsp.ld(y)), zscale(gamma, lc1.ld(y))));
-    if (s == 1) {
-      mm_t<BW>(D2, lc1, X(14 - 1), n);  // X13 is free again
-      bs_t<BW>(D0lu, X(13), n);
-      for (int y = 1; y <= n; ++y) op.st(y, zadd(zscale(1.0 - alpha * k2, lc1.ld(y)), zscale(alpha, X(13).ld(y))));
+  if (live) {
+    // solve_u_w^T: lambda g -> X0 (role 2), lambda dv -> X1 (role 1)
+    const double kxx = kx / k2, kzz = kz / k2;
+    if (role == 0) {
+      // solve_t^T: lambda h_theta -> X2, lambda of the theta store -> ot
+      helm_t<BW>(a, a.nu / a.pr, k2, lth, lst, X(2), ot, At, X(16), X(17));
+    } else if (role == 1) {
+      for (int y = 1; y <= n; ++y) X(1).st(y, zsub(zi(-kxx, lu.ld(y)), zi(kzz, lw.ld(y))));
+      // solve_v_f^T (Ag, Vb and the state-independent lines from k_adj_factor)
+      {
+        const double nu = a.nu;
+        const double alpha = dt * rka(1, s) * nu, gamma = dt * rka(3, s);
+        auto C = [&](int i) { return DLine{a.Xc + i * ns + m, nm}; };
+        const DLine buf3 = C(1), d2h = C(2), hh = C(4), hm = C(5);
+        const double2 h1 = hh.ld(1), hn = hh.ld(n);
+        const double2 den = zsub(zmul(h1, h1), zmul(hn, hn));
+        const double q = s != 3 ? 1.0 - dt * rka(1, s + 1) * nu * k2 : 1.0;
+        const double a1 = s != 3 ? dt * rka(1, s + 1) * nu : 0.0;
+        const DLine ldv = X(1);
+        double2 lC1 = make_double2(0.0, 0.0), lC2 = make_double2(0.0, 0.0);
+        for (int y = 1; y <= n; ++y) {
+          const int r = n + 1 - y;
+          const double2 vy = lv.ld(y), py = lsp.ld(y), dy = ldv.ld(y);
+          lC1 = zadd(lC1, zcm(hm.ld(y), vy));
+          lC2 = zadd(lC2, zcm(hm.ld(r), vy));
+          lC1 = zadd(lC1, zcm(zadd(zscale(q, buf3.ld(y)), zscale(a1, d2h.ld(y))), py));
+          lC2 = zadd(lC2, zcm(zadd(zscale(q, buf3.ld(r)), zscale(a1, d2h.ld(r))), py));
+          lC1 = zadd(lC1, zcm(hh.ld(y), dy));
+          lC2 = zsub(lC2, zcm(hh.ld(r), dy));
+        }
+        // dv0 (the particular solution's dv/dy): its wall values set C1 and C2
+        const DLine ldv0 = X(11);
+        for (int y = 1; y <= n; ++y) ldv0.st(y, ldv.ld(y));
+        const double2 hnd = zdiv(hn, den), h1d = zdiv(h1, den);
+        ldv0.st(n, zadd(ldv0.ld(n), zadd(zcm(hnd, lC1), zcm(h1d, lC2))));
+        ldv0.st(1, zsub(ldv0.ld(1), zadd(zcm(h1d, lC1), zcm(hnd, lC2))));
+        // v0 = D0 cv, dv0 = D1 cv, cv = V^-1 r
+        const DLine lr = X(12);
+        mm_t<BW>(D0, lv, lr, n);
+        mm_t<BW>(D1, ldv0, lr, n, 1.0, true);
+        bs_t<BW>(Vb, lr, n);
+        a.lvw[m] = lr.ld(1);
+        a.lvw[nm + m] = lr.ld(n);
+        // part 4: lambda of hv2 (= D0 c1) and of dv_a (= D2 c1)
+        const DLine lhv2 = X(13), lc1 = X(14);
+        for (int y = 1; y <= n; ++y) {
+          const double2 w0 = (y == 1 || y == n) ? make_double2(0.0, 0.0) : lr.ld(y);
+          lhv2.st(y, zadd(w0, zscale(q, lsp.ld(y))));
+        }
+        mm_t<BW>(D0, lhv2, lc1, n);
+        if (s != 3) mm_t<BW>(D2, lsp, lc1, n, a1, true);
+        bs_t<BW>(Ag, lc1, n);
+        zero_walls(lc1, n);  // lambda of the right-hand side of phi
+        // parts 2 and 1
+        const DLine lhv = X(15);
+        const double z1 = s != 3 ? dt * rka(4, s + 1) : 0.0;
+        for (int y = 1; y <= n; ++y) lhv.st(y, zadd(zscale(z1, lsp.ld(y)), zscale(gamma, lc1.ld(y))));
+        if (s == 1) {
+          mm_t<BW>(D2, lc1, X(14 - 1), n);  // X13 is free again
+          bs_t<BW>(D0lu, X(13), n);
+          for (int y = 1; y <= n; ++y) op.st(y, zadd(zscale(1.0 - alpha * k2, lc1.ld(y)), zscale(alpha, X(13).ld(y))));
+        } else {
+          for (int y = 1; y <= n; ++y) op.st(y, lc1.ld(y));
+        }
+      }
     } else {
-      for (int y = 1; y <= n; ++y) op.st(y, lc1.ld(y));
+      for (int y = 1; y <= n; ++y) X(0).st(y, zsub(zi(kzz, lu.ld(y)), zi(kxx, lw.ld(y))));
+      // solve_g^T: lambda h_g -> X3
+      helm_t<BW>(a, a.nu, k2, X(0), lsg, X(3), og, Ag, X(4), X(5));
     }
   }
-  // solve_g^T: lambda h_g -> X3 (X0 holds lambda g)
-  helm_t<BW>(a, a.nu, k2, X(0), lsg, X(3), og, Ag, X(4), X(5));
+  __syncthreads();
   // hvhg^T with lambda h_g = X3, lambda h_v = X15, lambda h_theta = X2
-  {
-    const DLine lhg = X(3), lhv = X(15), lht = X(2);
-    const DLine e1hg = X(4), e1hv = X(5), e2hv = X(6), e1ht = X(7);
-    mm_t<BW>(D1, lhg, e1hg, n);
-    bs_t<BW>(D0lu, e1hg, n);
-    mm_t<BW>(D1, lhv, e1hv, n);
-    bs_t<BW>(D0lu, e1hv, n);
-    mm_t<BW>(D2, lhv, e2hv, n);
-    bs_t<BW>(D0lu, e2hv, n);
-    mm_t<BW>(D1, lht, e1ht, n);
-    bs_t<BW>(D0lu, e1ht, n);
+  const DLine lhg = X(3), lhv = X(15), lht = X(2);
+  const DLine e1hg = X(4), e1hv = X(5), e2hv = X(6), e1ht = X(7);
+  if (live) {
+    if (role == 0) {
+      mm_t<BW>(D1, lhg, e1hg, n);
+      bs_t<BW>(D0lu, e1hg, n);
+      mm_t<BW>(D1, lht, e1ht, n);
+      bs_t<BW>(D0lu, e1ht, n);
+    } else if (role == 1) {
+      mm_t<BW>(D1, lhv, e1hv, n);
+      bs_t<BW>(D0lu, e1hv, n);
+    } else {
+      mm_t<BW>(D2, lhv, e2hv, n);
+      bs_t<BW>(D0lu, e2hv, n);
+    }
+  }
+  __syncthreads();
+  if (live) {
     const double kx2 = kx * kx, kz2 = kz * kz, kxkz = kx * kz;
     const double c2 = kx * kx * kx + kx * (kz * kz), c4 = (kx * kx) * kz + kz * kz * kz;
     auto P = [&](int i) { return DLine{a.lP + i * ns + m, nm}; };
     for (int y = 1; y <= n; ++y) {
-      const double2 g = lhg.ld(y), v = lhv.ld(y), t = lht.ld(y);
-      const double2 eg = e1hg.ld(y), ev = e1hv.ld(y), e2 = e2hv.ld(y), et = e1ht.ld(y);
-      P(0).st(y, zsub(zscale(kxkz, g), zscale(kx2, ev)));
-      P(2).st(y, zsub(zscale(-kxkz, g), zscale(kz2, ev)));
-      P(4).st(y, zsub(zscale(kz2 - kx2, g), zscale(2.0 * kxkz, ev)));
-      P(1).st(y, zsub(zsub(zi(kz, eg), zi(c2, v)), zi(kx, e2)));
-      P(3).st(y, zsub(zsub(zi(-kx, eg), zi(c4, v)), zi(kz, e2)));
-      P(5).st(y, zi(kx, t));
-      P(7).st(y, zi(kz, t));
-      P(6).st(y, make_double2(-et.x, -et.y));
+      if (role == 0) {
+        const double2 g = lhg.ld(y), ev = e1hv.ld(y);
+        P(0).st(y, zsub(zscale(kxkz, g), zscale(kx2, ev)));
+        P(2).st(y, zsub(zscale(-kxkz, g), zscale(kz2, ev)));
+        P(4).st(y, zsub(zscale(kz2 - kx2, g), zscale(2.0 * kxkz, ev)));
+      } else if (role == 1) {
+        const double2 v = lhv.ld(y), eg = e1hg.ld(y), e2 = e2hv.ld(y);
+        P(1).st(y, zsub(zsub(zi(kz, eg), zi(c2, v)), zi(kx, e2)));
+        P(3).st(y, zsub(zsub(zi(-kx, eg), zi(c4, v)), zi(kz, e2)));
+      } else {
+        const double2 t = lht.ld(y), et = e1ht.ld(y);
+        P(5).st(y, zi(kx, t));
+        P(7).st(y, zi(kz, t));
+        P(6).st(y, make_double2(-et.x, -et.y));
+      }
     }
   }
 }
@@ -611,8 +633,8 @@ cudaError_t adj_substep_bw(Handle &h, int s, const double2 *sbase, double dt, do
   k_adj_mean<BW><<<1, 32, 0, h.side>>>(a);
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
   if ((e = cudaEventRecord(h.ev_join, h.side)) != cudaSuccess) return e;
-  // one thread per mode; 64-thread blocks spread the few thousand modes over more SMs
-  k_adj_modes<BW><<<(unsigned)((h.nmodes + 63) / 64), 64, 0, st>>>(a);
+  // three role warps per 32 modes
+  k_adj_modes<BW><<<(unsigned)((h.nmodes + 31) / 32), 32 * kAdjRoles, 0, st>>>(a);
   if ((e = cudaStreamWaitEvent(st, h.ev_join, 0)) != cudaSuccess) return e;
   const unsigned blocks = (unsigned)((h.nmodes + 127) / 128);
   ProbeArgs pa{};
