@@ -113,26 +113,42 @@ __device__ void mm_t(const B &A, XT x, YT y, int n, double s = 1.0, bool acc = f
 }
 
 // A^T x = b in place, A's packed Crout factors (L with the pivots, unit U): U^T z = b ascending,
-// then L^T x = z descending.
+// then L^T x = z descending.  The last 2BW results of each sweep stay in a register window (the
+// recurrence would otherwise wait on its own stores), taken in the same order of j as a loop over
+// the stored line, so the sums are the same.
 template <int BW, typename B, typename LT>
 __device__ void bs_t(const B &A, LT b, int n) {
+  constexpr int W = 2 * BW;
+  double2 win[W];  // ascending: win[k] = z_{c-W+k}; descending: win[k] = x_{c+1+k}
+#pragma unroll
+  for (int k = 0; k < W; ++k) win[k] = make_double2(0.0, 0.0);
   for (int c = 1; c <= n; ++c) {
     double2 t = b.ld(c);
-    for (int j = (c - 2 * BW > 1 ? c - 2 * BW : 1); j < c; ++j) {
-      if (c > row_hi<BW>(j, n)) continue;
-      t = zsub(t, zscale(ent<BW>(A, j, c, n), b.ld(j)));
+#pragma unroll
+    for (int k = 0; k < W; ++k) {
+      const int j = c - W + k;
+      if (j >= 1 && c <= row_hi<BW>(j, n)) t = zsub(t, zscale(ent<BW>(A, j, c, n), win[k]));
     }
+#pragma unroll
+    for (int k = 0; k < W - 1; ++k) win[k] = win[k + 1];
+    win[W - 1] = t;
     b.st(c, t);
   }
+#pragma unroll
+  for (int k = 0; k < W; ++k) win[k] = make_double2(0.0, 0.0);
   for (int c = n; c >= 1; --c) {
     double2 t = b.ld(c);
-    const int j1 = c + 2 * BW < n ? c + 2 * BW : n;
-    for (int j = c + 1; j <= j1; ++j) {
-      if (c < row_lo<BW>(j, n)) continue;
-      t = zsub(t, zscale(ent<BW>(A, j, c, n), b.ld(j)));
+#pragma unroll
+    for (int k = 0; k < W; ++k) {
+      const int j = c + 1 + k;
+      if (j <= n && c >= row_lo<BW>(j, n)) t = zsub(t, zscale(ent<BW>(A, j, c, n), win[k]));
     }
     const double d = ent<BW>(A, c, c, n);
-    b.st(c, make_double2(t.x / d, t.y / d));
+    t = make_double2(t.x / d, t.y / d);
+#pragma unroll
+    for (int k = W - 1; k >= 1; --k) win[k] = win[k - 1];
+    win[0] = t;
+    b.st(c, t);
   }
 }
 
