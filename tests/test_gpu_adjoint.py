@@ -7,6 +7,8 @@ and the torch.autograd.Function over them).
 * Against central finite differences of the GPU step itself (eps = 1e-4, north_star's check):
   dJ/dA and the gains gradient along a random direction, 1e-4 relative.
 * The state after backward is the state forward left; the configuration checks hold.
+* The per-substep band cache of the backward follows dt: gradients bit-identical to a fresh
+  handle after dt changes between backward calls.
 """
 import numpy as np
 import pytest
@@ -118,3 +120,22 @@ def test_adjoint_configuration_checks():
         with pytest.raises(KmmError) as e:
             ch.adjoint_backward()
         assert e.value.code == _lib.KMM_ERR_ARG
+
+
+def test_adjoint_band_cache_follows_dt():
+    """The backward caches each substep's factored bands for its fixed dt: a second backward at
+    another dt on the same handle rebuilds them, and gives the gradients of a fresh handle at that
+    dt bit for bit (and a third, back at the first dt, those of the first call)."""
+    amp, nsteps = -0.5, 2
+    cfg, p = make_pair(nx=16, ny=33, nz=16, control_amp=amp, precision=0, fixed_dt=1)
+    U = seeded_state(cfg, okmm.make_operators(p).y)
+    gains = _gains(p)
+    fresh = {dt: _gpu_grad(cfg, U, amp, gains, nsteps, 1.0, 0.5, dt=dt) for dt in (0.01, 0.005)}
+    with Channel(cfg) as ch:
+        ch.set_control(amp, gains)
+        for dt in (0.01, 0.005, 0.01):
+            ch.set_initial_data_uvw(U, dt)
+            J = ch.adjoint_forward(nsteps, 1.0, 0.5)
+            dA, dg = ch.adjoint_backward()
+            Jf, dAf, dgf = fresh[dt]
+            assert J == Jf and dA == dAf and np.array_equal(dg, dgf), dt
