@@ -1,7 +1,7 @@
 #!/usr/bin/env python
 """Benchmark: RK3 steps/s of the KMM channel step at Re_tau 180, 192x129x192.
 
-Headline (BASELINE metric): mixed-precision, graph-captured steps/s on one B200, with the
+Headline metric: mixed-precision, graph-captured steps/s on one B200, with the
 plain FP64 GPU path timed beside it and the mixed path's relative L2 error against the FP64
 path after 100 steps.  Workload: Lx = 4 pi, Lz = 4 pi / 3 (LMFx = 2, LMFz = 2/3),
 192 x 129 x 192 modes (288 x 129 x 288 dealiased), order-7 B-splines on the sine map,

@@ -4,7 +4,7 @@ and the torch.autograd.Function over them).
 * Against the FP64 reference gradient of the oracle's own adjoint (oracle/adjoint.py, itself held
   to central finite differences on the CPU): objective, dJ/dA and dJ/dgains of the time-averaged
   wall shear stress and wall scalar flux, 1e-8 relative.
-* Against central finite differences of the GPU step itself (eps = 1e-4, north_star's check):
+* Against central finite differences of the GPU step itself (eps = 1e-4):
   dJ/dA and the gains gradient along a random direction, 1e-4 relative.
 * The state after backward is the state forward left; the configuration checks hold.
 * The per-substep band cache of the backward follows dt: gradients bit-identical to a fresh
