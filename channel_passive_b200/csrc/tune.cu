@@ -355,7 +355,7 @@ int kmm_get_tuning(const kmm_handle *hh, kmm_tuning *out) {
   std::memset(out, 0, sizeof(*out));
   tile_shapes(h, h.tune.z, h.tune.x, &out->z_lines_per_block, &out->x_rows_per_block, &out->x_threads);
   out->modes_per_block = 32 * (h.nsc == 1 ? h.tune.groups : 1);
-  out->helm_modes_per_block = 32 * (h.nsc == 1 ? h.tune.hgroups : 1);
+  out->helm_modes_per_block = 32 * h.tune.hgroups;
   out->helm_tables_shared = h.tune.hstab;
   out->helm_stage_ahead = h.nsc == 1 ? h.tune.stage : 1;
   out->z_tma = h.tune.ztma;
@@ -396,7 +396,7 @@ int kmm_set_tuning(kmm_handle *hh, const kmm_tuning *t) {
                       (t->hvhg_stage_ahead >= 0 && t->hvhg_stage_ahead <= 2) && g != 0 &&
                       hvhg_shape_fits(h, g, t->tables_shared, t->hvhg_stage_ahead);
   const int hg = t->helm_modes_per_block == 32 ? 1 : t->helm_modes_per_block == 64 ? 2
-                 : t->helm_modes_per_block == 128 ? 4 : 0;
+                 : t->helm_modes_per_block == 96 ? 3 : t->helm_modes_per_block == 128 ? 4 : 0;
   const bool helm_ok = hg != 0 && (t->helm_tables_shared == 0 || t->helm_tables_shared == 1) &&
                        (t->helm_stage_ahead == 1 || t->helm_stage_ahead == 2) &&
                        helm_shape_fits(h, hg, t->helm_tables_shared, t->helm_stage_ahead);

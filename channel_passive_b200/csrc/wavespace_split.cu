@@ -703,8 +703,7 @@ constexpr size_t helm_smem() {
 // FC (one scalar): the sweeps read the factor cache that k_helm_factor filled for this dt, and
 // the kernel records that dt as the one the cache holds.
 template <int BW, typename PT, int NS, int SA, bool FC = false>
-__global__ void __launch_bounds__(NS == 1 ? 4 * kLanes * kHelmRoles : kLanes * (kHelmRoles + 1), NS == 1 ? 1 : 3)
-k_helmholtz(SplitArgs a) {
+__global__ void __launch_bounds__(4 * kLanes * kHelmRoles, 1) k_helmholtz(SplitArgs a) {
   extern __shared__ double2 helm_ring[];
   if (a.dsc->err) return;  // a failed dt update leaves the state untouched (uniform over the block)
   if constexpr (FC) {
@@ -1029,7 +1028,7 @@ cudaError_t split_bw(Handle &h, int part, int substep, const double *dt_ptr, cud
   a.vf = h.vf;
   a.vf_l = vop_lband_doubles(h);
   a.groups = h.nsc == 1 ? h.tune.groups : 1;
-  a.hgroups = h.nsc == 1 ? h.tune.hgroups : 1;
+  a.hgroups = h.tune.hgroups;
   a.ulayout = h.tune.ulayout;
   a.stab = h.tune.stab;
   a.hstab = h.tune.hstab;
@@ -1097,9 +1096,12 @@ cudaError_t split_bw(Handle &h, int part, int substep, const double *dt_ptr, cud
   }
   if (part == 1) {
     if (h.nsc == 2) {
-      constexpr int nt = kLanes * (kHelmRoles + 1);
-      if (h.mixed) k_helmholtz<BW, float2, 2, 1><<<blocks, nt, helm_smem<BW, 2>() + htsm, st>>>(a);
-      else k_helmholtz<BW, double2, 2, 1><<<blocks, nt, helm_smem<BW, 2>() + htsm, st>>>(a);
+      const int HG = a.hgroups;
+      const unsigned hb = (unsigned)((h.nmodes + (int64_t)kLanes * HG - 1) / ((int64_t)kLanes * HG));
+      const int nt = kLanes * (kHelmRoles + 1) * HG;
+      const size_t sm = HG * helm_smem<BW, 2>() + htsm;
+      if (h.mixed) k_helmholtz<BW, float2, 2, 1><<<hb, nt, sm, st>>>(a);
+      else k_helmholtz<BW, double2, 2, 1><<<hb, nt, sm, st>>>(a);
     } else {
       const int HG = a.hgroups;
       const unsigned hb = (unsigned)((h.nmodes + (int64_t)kLanes * HG - 1) / ((int64_t)kLanes * HG));
@@ -1206,7 +1208,7 @@ cudaError_t set_solver_smem_limits(const Handle &h) {
 
 size_t helm_ring_bytes(const Handle &h, int hgroups, int stage) {
   const size_t per = sizeof(double2) * (size_t)(stage + 1) * (5 + h.bw) * kLanes;  // kHelmUnits<BW>
-  return per * (h.nsc == 2 ? kHelmRoles + 1 : (size_t)kHelmRoles * hgroups);
+  return per * (size_t)(kHelmRoles + h.nsc - 1) * hgroups;
 }
 
 int device_attr(cudaDeviceAttr attr) {
@@ -1232,7 +1234,9 @@ bool hvhg_shape_fits(const Handle &h, int groups, int stab, int stage) {
 }
 
 bool helm_shape_fits(const Handle &h, int hgroups, int hstab, int stage) {
-  if (h.nsc == 2 && (hgroups != 1 || stage != 1)) return false;
+  // at most 384 threads (the kernel's launch bound); two scalars take one row of look-ahead
+  if (hgroups < 1 || kLanes * (kHelmRoles + h.nsc - 1) * hgroups > 4 * kLanes * kHelmRoles) return false;
+  if (h.nsc == 2 && stage != 1) return false;
   const size_t bytes = helm_ring_bytes(h, hgroups, stage) + (hstab ? solver_tables_bytes(h) : 0);
   return bytes <= (size_t)device_attr(cudaDevAttrMaxSharedMemoryPerBlockOptin);
 }
@@ -1250,14 +1254,29 @@ void default_solver_shapes(Handle &h) {
   h.tune.hstab = 0;
   h.tune.stage = 1;
   h.tune.hvstage = 0;
-  if (h.nsc != 1) return;
-  if (hvhg_shape_fits(h, 1, 0, 2)) h.tune.hvstage = 2;  // k_hvhg: a two-row staging ring
   const int sms = device_attr(cudaDevAttrMultiProcessorCount);
+  // the most 32-mode groups a 384-thread block holds: 4 with one scalar, 3 with two
+  const int hgmax = (4 * kHelmRoles) / (kHelmRoles + h.nsc - 1);
+  const bool full = h.nmodes >= (int64_t)kLanes * hgmax * sms * 9 / 10;
+  if (h.nsc != 1) {
+    // two scalars: the largest blocks with the tables in shared memory where they still put a
+    // block on nearly every SM (one row of look-ahead)
+    if (full && helm_shape_fits(h, hgmax, 1, 1)) {
+      h.tune.hgroups = hgmax;
+      h.tune.hstab = 1;
+    }
+    return;
+  }
+  if (hvhg_shape_fits(h, 1, 0, 2)) h.tune.hvstage = 2;  // k_hvhg: a two-row staging ring
   const size_t per_sm = (size_t)device_attr(cudaDevAttrMaxSharedMemoryPerMultiprocessor);
-  if (h.nmodes >= (int64_t)kLanes * 4 * sms * 9 / 10 && helm_shape_fits(h, 4, 1, 2)) {
+  if (full && helm_shape_fits(h, 4, 1, 2)) {
     h.tune.hgroups = 4;
     h.tune.hstab = 1;
     h.tune.stage = 2;
+  } else if (full && helm_shape_fits(h, 4, 1, 1)) {
+    // a larger ny: the tables and a one-row ring still fit beside each other
+    h.tune.hgroups = 4;
+    h.tune.hstab = 1;
   } else if (2 * (helm_ring_bytes(h, 2, 1) + solver_tables_bytes(h) + 1024) <= per_sm) {
     h.tune.hgroups = 2;
     h.tune.hstab = 1;

@@ -104,7 +104,8 @@ typedef struct kmm_tuning {
   int32_t tuned;              /* 1 once kmm_autotune has run */
   int32_t tables_shared;      /* 1: the hvhg solver copies the B-spline operator tables it reads
                                  into shared memory first */
-  int32_t helm_modes_per_block;  /* systems a block of the Helmholtz solver takes (32, 64, 128) */
+  int32_t helm_modes_per_block;  /* systems a block of the Helmholtz solver takes (32, 64, 128;
+                                    32, 64, 96 with two scalars) */
   int32_t helm_tables_shared;    /* 1: the Helmholtz solver reads the tables from shared memory */
   int32_t helm_stage_ahead;      /* rows its sweeps stage ahead through shared memory (1, 2) */
   int32_t z_tma;              /* 1: the z transforms stage each block's input tile through TMA

@@ -78,3 +78,29 @@ def test_second_scalar_needs_field_11():
         with pytest.raises(KmmError) as e:
             ch.set_initial_data_uvw(U, 0.01)
         assert e.value.code == _lib.KMM_ERR_ARG
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+def test_second_scalar_block_shapes_are_bit_identical(precision):
+    """The two-scalar Helmholtz kernel with 64 or 96 modes per block and the operator tables in
+    shared memory (the shapes a large grid starts with) gives the 32-mode blocks' results bit
+    for bit: the shapes spread the modes over blocks, not the arithmetic."""
+    cfg, p = make_pair(nx=32, ny=33, nz=32, control_amp=-1.0, fixed_dt=1, precision=precision, n_scalar=2,
+                       pr2=0.2, bulk_t2=0.5)
+    U10 = seeded_state(cfg, okmm.make_operators(p).y)
+    U = with_scalar2(U10, 0.5 * U10[6])
+    out = []
+    for shape in (dict(helm_modes_per_block=32, helm_tables_shared=0),
+                  dict(helm_modes_per_block=64, helm_tables_shared=1),
+                  dict(helm_modes_per_block=96, helm_tables_shared=1),
+                  dict(helm_modes_per_block=96, helm_tables_shared=0)):
+        with Channel(cfg) as ch:
+            ch.set_tuning(**shape)
+            assert ch.tuning["helm_modes_per_block"] == shape["helm_modes_per_block"]
+            ch.set_initial_data_uvw(U, 0.01)
+            ch.step(3)
+            out.append(ch.download_state(11))
+    for Ug, RKg in out[1:]:
+        for f in STATE_SLOTS2:
+            assert np.array_equal(Ug[f], out[0][0][f]), f
+        assert np.array_equal(RKg, out[0][1])
