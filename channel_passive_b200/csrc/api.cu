@@ -585,6 +585,10 @@ int kmm_create(const kmm_config *cfg, kmm_handle **out) {
     }
   }
   default_solver_shapes(*h);  // the untuned solver launch shapes
+  // FP64 with two scalars at x lengths of 576 and more: 128 threads a row (x variant 1) instead
+  // of 64, which the six packed output lines' shared memory had held to two warps a block
+  // (384x257x384: x pass 8.54 -> 6.15 ms, 17.0 -> 19.4 steps/s, the tuner's pick there)
+  if (!h->mixed && h->nsc == 2 && h->nx32 >= 576) h->tune.x = 1;
   // with a fixed time step the Helmholtz sweeps read their operators' cached factors
   h->tune.fcache = h->hf ? 1 : 0;
   // the z transforms stage their input tiles through TMA where the grid allows the tile map
